@@ -1,0 +1,206 @@
+/*
+ * pm_stereo.h -- C ABI of the B200 motion-stereo library (libpm_stereo.so).
+ *
+ * Drop-in replacement for the StereoMapper class of HKUST-Aerial-Robotics/probabilistic_mapping
+ * (motion_stereo/stereo_mapper.h:26-63) and for its five C-style launch wrappers
+ * (ad_calc_cost, sgm2, filter_cost, depth_fuse, convert).  Plain pointers and sizes only.
+ *
+ * Conventions
+ *   - Images are W x H, row-major, with an explicit row pitch in BYTES.
+ *   - Cost volumes are plane-innermost float arrays: element ((y*W + x)*D + d), the INDEX()
+ *     layout of motion_stereo/cuda_utils.h:34.
+ *   - Matrices are row-major doubles; poses are camera-to-world (R, T) as in
+ *     StereoMapper::update (stereo_mapper.cpp:73-91).
+ *   - Pointers passed to the mapper-level calls may be host or device memory; the library
+ *     tells them apart with cudaPointerGetAttributes.  Stage-level calls (pm_stage_*) take
+ *     device pointers only and run on the given stream (NULL = legacy default stream).
+ *   - Every call returns a pm_status; pm_last_error() holds the message of the last failure
+ *     on a handle.  Nothing in the library exits or traps (the reference exits on error,
+ *     cuda_utils.h:18-32).
+ *   - A handle owns one CUDA stream; distinct handles may run concurrently; one handle must
+ *     not be used from two threads at once.
+ */
+#ifndef PM_STEREO_H
+#define PM_STEREO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PM_API __attribute__((visibility("default")))
+#else
+#define PM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int pm_status;
+#define PM_OK 0
+#define PM_ERR_INVALID_ARGUMENT 1
+#define PM_ERR_BAD_STATE 2
+#define PM_ERR_CUDA 3
+#define PM_ERR_OUT_OF_MEMORY 4
+#define PM_ERR_UNSUPPORTED 5
+
+#define PM_COST_REFERENCE 0 /* keeps the neighbour quirks of calc_cost.cu:50-51,70-71,106,119 */
+#define PM_COST_CORRECTED 1 /* the intended 3x3 patch absolute difference */
+
+#define PM_PREC_FP32 0 /* plain form: FP32 images, cost volume and aggregation */
+#define PM_PREC_FP16 1 /* FP16 cost volume, FP32 SGM accumulators and fusion */
+
+#define PM_FUSION_GPU 0      /* StereoMapper::outputFusion + depth_fusion.cu kernels */
+#define PM_FUSION_CPU_PATH 1 /* the constants and masks of outputFusionCPU, run on the GPU */
+
+typedef struct pm_config {
+    int width, height;   /* WIDTH, HEIGHT (parameters.h:8-9), runtime here */
+    int num_planes;      /* DEP_CNT (parameters.h:15); a multiple of 32, at most 256 */
+    float rho0;          /* inverse depth of plane 0; 0 in the reference (calc_cost.cu:81) */
+    float rho_step;      /* DEP_SAMPLE; pm_init_intrinsic overwrites it */
+    float intensity_scale; /* image value = uint8 * scale; 1 in the reference (stereo_mapper.cpp:66) */
+    int num_paths;       /* SGM paths: 4 (sgm.cu:119-133) or 8 (adds the four diagonals) */
+    float p1, p2;        /* pi1, pi2 (parameters.cpp:12-13) */
+    float tau_so;        /* parameters.cpp:14 */
+    float q1, q2;        /* sgm_q1, sgm_q2 (parameters.cpp:15-16) */
+    float var_scale;     /* flatness factor (parameters.cpp:18) */
+    float uniqueness_ratio; /* extension: reject when best > ratio * second best; 0 disables */
+    int cost_mode;       /* PM_COST_* */
+    int precision;       /* PM_PREC_* */
+    int fusion_variant;  /* PM_FUSION_* */
+    int tree_compat;     /* 1: reproduce the reduction tree of sgm.cu:24-31 / filter_cost.cu:22-30
+                            (drops planes when D is not a power of two); 0: exact minimum */
+    int max_sources;     /* source frames kept per reference frame (lazy cost evaluation) */
+    int device;          /* CUDA device ordinal */
+} pm_config;
+
+typedef struct pm_mapper pm_mapper;
+
+/* Fills the reference's defaults (parameters.cpp:12-18, DEP_SAMPLE of evaluate.cc:345). */
+PM_API void pm_config_default(pm_config* cfg, int width, int height, int num_planes);
+
+/* StereoMapper::StereoMapper (stereo_mapper.cpp:27-49): allocates every device buffer. */
+PM_API pm_status pm_create(const pm_config* cfg, pm_mapper** out);
+PM_API void pm_destroy(pm_mapper* h);
+
+/* Use the caller's stream instead of the handle's own one (e.g. a torch stream). */
+PM_API pm_status pm_set_stream(pm_mapper* h, void* cuda_stream);
+
+/* StereoMapper::initIntrinsic (stereo_mapper.cpp:51-61).  K row-major 3x3 (fy may be
+ * negative, evaluate.cc:38); bf is unused, as in the reference; dep_sample sets rho_step. */
+PM_API pm_status pm_init_intrinsic(pm_mapper* h, const double K[9], float bf, float dep_sample);
+
+/* StereoMapper::initReference (stereo_mapper.cpp:63-71): uint8 W x H image; resets the
+ * cost volume and the list of source frames. */
+PM_API pm_status pm_init_reference(pm_mapper* h, const uint8_t* img, size_t pitch_bytes);
+
+/* StereoMapper::update (stereo_mapper.cpp:73-91).  Composes H1 = K R_r^T R_l K^-1 and
+ * H2 = K R_r^T (T_l - T_r) in FP64 and queues the source frame; the cost of all queued frames
+ * is evaluated in one pass when the result is requested.  The result equals the reference's
+ * per-call running mean.  A pageable host image may be reused as soon as the call returns;
+ * page-locked host and device images must stay unchanged until the next pm_output* or
+ * pm_synchronize call returns (the upload is asynchronous for them). */
+PM_API pm_status pm_update(pm_mapper* h, const uint8_t* img, size_t pitch_bytes,
+                    const double R_l[9], const double T_l[3],
+                    const double R_r[9], const double T_r[3]);
+
+/* StereoMapper::output (stereo_mapper.cpp:93-109): SGM + winner-take-all/subpixel; writes the
+ * W x H depth (1000 = no overlap, 0 = rejected).  Synchronous for host destinations. */
+PM_API pm_status pm_output(pm_mapper* h, float* depth, size_t pitch_bytes);
+
+/* StereoMapper::outputFusion (stereo_mapper.cpp:111-244) or, with PM_FUSION_CPU_PATH,
+ * outputFusionCPU (stereo_mapper.cpp:625-820).  R, t: current keyframe pose (camera-to-world,
+ * row-major).  Writes the FUSED depth (the reference's GPU path returned the unfused map,
+ * stereo_mapper.cpp:229-230; pm_get_wta_depth gives that one) and, when variance is not NULL,
+ * the per-pixel variance sigma^2 of the fused state.  The first call only initialises the
+ * state and writes zeros, as the reference does (stereo_mapper.cpp:128-146). */
+PM_API pm_status pm_output_fusion(pm_mapper* h, float* depth, size_t depth_pitch, float* variance,
+                           size_t variance_pitch, const double R[9], const double t[3],
+                           float fx, float fy, float cx, float cy);
+
+/* The winner-take-all depth of the last output call (the reference's `dep`). */
+PM_API pm_status pm_get_wta_depth(pm_mapper* h, float* depth, size_t pitch_bytes);
+
+/* The winner-take-all plane index (W*H int32, row-major) of the last output call. */
+PM_API pm_status pm_get_wta_index(pm_mapper* h, int32_t* index);
+
+/* Fusion state of the last fused frame (alpha, beta, mu, sigma^2: W*H floats each; any may
+ * be NULL).  pm_set_state loads a state and pose, e.g. to resume a sequence. */
+PM_API pm_status pm_get_state(pm_mapper* h, float* alpha, float* beta, float* mu, float* sigma);
+PM_API pm_status pm_set_state(pm_mapper* h, const float* alpha, const float* beta, const float* mu,
+                       const float* sigma, const double R[9], const double t[3]);
+
+/* Device pointers of the internal buffers, for inspection and tests.  Valid until pm_destroy. */
+typedef struct pm_buffers {
+    const void* cost;      /* W*H*D: float (FP32) or half (FP16) */
+    const float* sgm;      /* W*H*D float, filled only after pm_debug_store_sgm(h, 1) */
+    const int32_t* wta_index; /* W*H winner-take-all plane index */
+    const float* wta_depth;   /* W*H */
+    const int32_t* table;  /* W*H propagation table of the last fusion step */
+} pm_buffers;
+PM_API pm_status pm_get_buffers(pm_mapper* h, pm_buffers* out);
+PM_API pm_status pm_debug_store_sgm(pm_mapper* h, int enable);
+
+/* Homography of source frame i as passed to the kernels (12 floats: H1 row-major, H2). */
+PM_API pm_status pm_get_homography(pm_mapper* h, int i, float out[12]);
+
+/* Opt-in CUDA-event timers around the stages of pm_output / pm_output_fusion (recorded on the
+ * handle's stream).  pm_get_stage_times synchronises and returns, in milliseconds, the
+ * time of the last call's stages: [0] cost volume, [1] SGM + winner-take-all, [2] fusion,
+ * [3] copy-out.  n is the capacity of ms; returns PM_ERR_BAD_STATE when timing is off. */
+#define PM_NUM_STAGES 4
+PM_API pm_status pm_enable_stage_timing(pm_mapper* h, int enable);
+PM_API pm_status pm_get_stage_times(pm_mapper* h, float* ms, int n);
+
+PM_API pm_status pm_synchronize(pm_mapper* h);
+PM_API const char* pm_last_error(const pm_mapper* h);
+PM_API const char* pm_status_string(pm_status s);
+
+/* ---------------------------------------------------------------------------------------
+ * Stage-level calls: one call per reference launch wrapper.  Device pointers, caller-owned
+ * buffers, asynchronous on `stream`.  Status codes report argument errors and launch errors.
+ * --------------------------------------------------------------------------------------- */
+
+/* uint8 -> scaled float image (the convertTo(CV_32F) + upload of stereo_mapper.cpp:66-67). */
+PM_API pm_status pm_stage_to_float(int W, int H, const uint8_t* src, size_t src_pitch, float* dst,
+                            float scale, void* stream);
+
+/* ad_calc_cost (calc_cost.cu:212-253) for `nsrc` sources at once.  ref: W*H float; srcs: nsrc
+ * consecutive W*H float images; homs: 12*nsrc floats in HOST memory.  cost: W*H*D float.
+ * When cnt is NULL the volume starts from cost=-1, cnt=0 (initReference); otherwise cost and
+ * cnt hold the running state and are updated in place, exactly as repeated ad_calc_cost
+ * calls would.  invalid (optional, W*H bytes) receives 1 where some plane was never measured. */
+PM_API pm_status pm_stage_calc_cost(const pm_config* cfg, const float* ref, const float* srcs, int nsrc,
+                             const float* homs, float* cost, float* cnt, uint8_t* invalid,
+                             void* stream);
+
+/* sgm2 (sgm.cu:115-135): out := sum over cfg->num_paths paths; out needs no clearing. */
+PM_API pm_status pm_stage_sgm(const pm_config* cfg, const float* cost, const float* ref, float* out,
+                       void* stream);
+
+/* filter_cost (filter_cost.cu:57-70): depth with a byte pitch; index (optional) W*H. */
+PM_API pm_status pm_stage_filter(const pm_config* cfg, const float* sgm, float* depth, size_t pitch_bytes,
+                          int32_t* index, void* stream);
+
+/* sgm2 + filter_cost fused: the last path finishes the sum in registers and runs the
+ * winner-take-all; `scratch` holds the partial sum (W*H*D floats). */
+PM_API pm_status pm_stage_sgm_filter(const pm_config* cfg, const float* cost, const float* ref,
+                              float* scratch, float* depth, size_t pitch_bytes, int32_t* index,
+                              void* stream);
+
+/* depth_fuse (depth_fusion.cu:229-280).  pose: R_p2c row-major then t_p2c (floats); cam: fx,
+ * fy, cx, cy.  depth: W*H, in = WTA depth, out = fused depth.  pre/cur: alpha, beta, mu, sigma
+ * (4 pointers each, W*H floats).  ztable: W*H uint64 scratch.  table (optional): W*H int32. */
+PM_API pm_status pm_stage_depth_fuse(int W, int H, const float pose[12], const float cam[4],
+                              float* depth, float* const pre[4], float* const cur[4],
+                              uint64_t* ztable, int32_t* table, void* stream);
+
+/* convert (convert.cu:26-45).  flag != 0: linear -> pitched, else pitched -> linear.  The
+ * pitch is in BYTES (the reference passed a byte step but indexed with it in floats). */
+PM_API pm_status pm_stage_convert(int W, int H, const float* in, float* out, int flag,
+                           size_t pitch_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PM_STEREO_H */

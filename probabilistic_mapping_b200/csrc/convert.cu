@@ -1,0 +1,51 @@
+// convert.cu -- image conversions.
+//   to_float_kernel: uint8 -> scaled float, the convertTo(CV_32F) + upload of
+//                    StereoMapper::initReference / update (stereo_mapper.cpp:65-67,75-77).
+//   convert_kernel:  pitched <-> linear float copy (reference: convert.cu:4-45).  The pitch is
+//                    taken in bytes; the reference received a byte step and indexed with it in
+//                    floats (stereo_mapper.cpp:149-152 vs convert.cu:16-21), which reads past
+//                    the end of the source for every row after the first quarter.
+#include "pm_device.cuh"
+
+namespace pm {
+namespace {
+
+__global__ void __launch_bounds__(256) to_float_kernel(int W, int H, const uint8_t* __restrict__ src,
+                                                       size_t pitch, float* __restrict__ dst, float scale) {
+    const int y = blockIdx.y;
+    const uint8_t* row = src + (size_t)y * pitch;
+    float* out = dst + (size_t)y * W;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < W; x += gridDim.x * blockDim.x)
+        out[x] = __fmul_rn((float)row[x], scale);
+}
+
+__global__ void __launch_bounds__(256) convert_kernel(int W, int H, const float* __restrict__ in,
+                                                      float* __restrict__ out, int flag, size_t pitch) {
+    const int y = blockIdx.y;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < W; x += gridDim.x * blockDim.x) {
+        if (flag) {   // linear -> pitched
+            *reinterpret_cast<float*>(reinterpret_cast<char*>(out) + (size_t)y * pitch + (size_t)x * 4) =
+                in[(size_t)y * W + x];
+        } else {      // pitched -> linear
+            out[(size_t)y * W + x] =
+                *reinterpret_cast<const float*>(reinterpret_cast<const char*>(in) + (size_t)y * pitch + (size_t)x * 4);
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_to_float(int W, int H, const uint8_t* src, size_t src_pitch, float* dst, float scale,
+                            cudaStream_t s) {
+    const dim3 grid((W + 255) / 256, H);
+    to_float_kernel<<<grid, 256, 0, s>>>(W, H, src, src_pitch, dst, scale);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_convert(int W, int H, const float* in, float* out, int flag, size_t pitch, cudaStream_t s) {
+    const dim3 grid((W + 255) / 256, H);
+    convert_kernel<<<grid, 256, 0, s>>>(W, H, in, out, flag, pitch);
+    return cudaGetLastError();
+}
+
+}  // namespace pm

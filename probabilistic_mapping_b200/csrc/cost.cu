@@ -1,0 +1,205 @@
+// cost.cu -- plane-sweep absolute-difference cost volume (reference: calc_cost.cu:11-253).
+//
+// The reference launches one thread per plane and walks D pixels per block, computing all
+// nine projective warps of the 3x3 patch for every voxel and every source frame, with a
+// read-modify-write of cost and count per call.  Here one CTA owns a 32x8 pixel tile and
+// all planes of it:
+//   * for a chunk of 16 planes and one source it warps the tile plus a one-pixel halo once
+//     (340 positions x 16 planes) into shared memory; the nine patch samples of each voxel
+//     are then read from that tile instead of being warped again (the two samples the
+//     reference computes from a corrupted neighbour, calc_cost.cu:50-51 and :70-71, are
+//     per-voxel and stay direct warps in reference mode);
+//   * all source frames queued since initReference are folded in one pass with the
+//     reference's running-mean update kept in registers, so the volume is written once;
+//   * the tile is transposed through shared memory so the volume is stored with 128-byte
+//     coalesced rows in the plane-innermost layout (cuda_utils.h:34).
+// All FP32 arithmetic uses explicit round-to-nearest intrinsics (see pm_device.cuh).
+#include "pm_device.cuh"
+
+namespace pm {
+namespace {
+
+constexpr int TX = 32, TY = 8;          // pixel tile
+constexpr int PC = 16;                  // planes per chunk
+constexpr int HX = TX + 2, HY = TY + 2; // tile + halo
+constexpr int NPOS = HX * HY;           // 340 warped positions
+constexpr int NT = TX * TY;             // 256 threads, one per pixel
+constexpr int SP = PC + 1;              // transpose staging pitch (bank-conflict free)
+
+static_assert(NT * SP <= PC * NPOS, "staging must fit into the warp tile");
+
+__device__ __forceinline__ float ref_at(const float* __restrict__ ref, int W, int H, int x, int y) {
+    return (x < 0 || y < 0 || x >= W || y >= H) ? 0.0f : __ldg(ref + (size_t)y * W + x);
+}
+
+template <bool HALF> __device__ __forceinline__ void store_cost(void* base, size_t i, float v) {
+    if constexpr (HALF) reinterpret_cast<__half*>(base)[i] = __float2half_rn(v);
+    else reinterpret_cast<float*>(base)[i] = v;
+}
+template <bool HALF> __device__ __forceinline__ float load_cost(const void* base, size_t i) {
+    if constexpr (HALF) return __half2float(reinterpret_cast<const __half*>(base)[i]);
+    else return reinterpret_cast<const float*>(base)[i];
+}
+
+// MODE 0: reference sample set (calc_cost.cu:83-199); MODE 1: corrected 3x3 patch.
+template <int MODE, bool HALF>
+__global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
+    __shared__ __align__(16) float wt[PC * NPOS];   // warped source samples [plane][position]
+    __shared__ float hx[NPOS], hy[NPOS], hz[NPOS];  // homogeneous coordinates of the positions
+
+    const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int u = x0 + tx, v = y0 + ty;
+    const int W = a.W, H = a.H, D = a.D;
+    const bool inside = (u < W) && (v < H);
+
+    // reference-image patch (border addressing -> 0, calc_cost.cu:230-231)
+    const float Rc = ref_at(a.ref, W, H, u, v), Ru = ref_at(a.ref, W, H, u, v - 1);
+    const float Rd = ref_at(a.ref, W, H, u, v + 1), Rl = ref_at(a.ref, W, H, u - 1, v);
+    const float Rr = ref_at(a.ref, W, H, u + 1, v), Rul = ref_at(a.ref, W, H, u - 1, v - 1);
+    const float Rdr = ref_at(a.ref, W, H, u + 1, v + 1), Rld = ref_at(a.ref, W, H, u - 1, v + 1);
+    const float Rru = ref_at(a.ref, W, H, u + 1, v - 1);
+
+    bool pix_invalid = false;
+
+    for (int d0 = 0; d0 < D; d0 += PC) {
+        float acc[PC], cn[PC];
+        if (a.incremental) {
+            // running state from memory, transposed through shared memory
+            for (int pass = 0; pass < 2; ++pass) {
+                __syncthreads();
+                for (int i = 0; i < TX; ++i) {
+                    const int pu = x0 + i, pv = y0 + ty;
+                    float val = 0.0f;
+                    if (pu < W && pv < H) {
+                        const size_t e = ((size_t)pv * W + pu) * D + d0 + tx;
+                        val = pass == 0 ? load_cost<HALF>(a.cost, e) : a.cnt[e];
+                    }
+                    wt[(ty * TX + i) * SP + tx] = val;
+                }
+                __syncthreads();
+#pragma unroll
+                for (int k = 0; k < PC; ++k) {
+                    if (pass == 0) acc[k] = wt[tid * SP + k];
+                    else cn[k] = wt[tid * SP + k];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < PC; ++k) { acc[k] = -1.0f; cn[k] = 0.0f; }
+        }
+
+        for (int s = 0; s < a.nsrc; ++s) {
+            const float* __restrict__ src = a.srcs + (size_t)s * W * H;
+            Hom h;
+            h.r11 = a.hom[s][0]; h.r12 = a.hom[s][1]; h.r13 = a.hom[s][2];
+            h.r21 = a.hom[s][3]; h.r22 = a.hom[s][4]; h.r23 = a.hom[s][5];
+            h.r31 = a.hom[s][6]; h.r32 = a.hom[s][7]; h.r33 = a.hom[s][8];
+            h.t1 = a.hom[s][9]; h.t2 = a.hom[s][10]; h.t3 = a.hom[s][11];
+
+            __syncthreads();   // previous consumers of wt / hx are done
+            for (int p = tid; p < NPOS; p += NT) {
+                const int py = p / HX, px = p - py * HX;
+                homog(h, x0 + px - 1, y0 + py - 1, hx[p], hy[p], hz[p]);
+            }
+            __syncthreads();
+            for (int i = tid; i < PC * NPOS; i += NT) {
+                const int k = i / NPOS, p = i - k * NPOS;
+                const float rho = __fmaf_rn((float)(d0 + k), a.drho, a.rho0);   // calc_cost.cu:81
+                wt[i] = warp_fetch(src, W, H, hx[p], hy[p], hz[p], h, rho);
+            }
+            __syncthreads();
+
+            if (inside) {
+                float xc, yc, zc;
+                homog(h, u, v, xc, yc, zc);
+                // corrupted neighbours of the reference (calc_cost.cu:49-51, 69-71)
+                const float xr = __fadd_rn(xc, h.r11), yr = __fadd_rn(xc, h.r21), zr = __fadd_rn(xc, h.r31);
+                const float xru = __fsub_rn(xr, h.r12), yru = __fsub_rn(xr, h.r22), zru = __fsub_rn(xr, h.r32);
+                const float* wc = wt + (ty + 1) * HX + (tx + 1);
+#pragma unroll
+                for (int k = 0; k < PC; ++k) {
+                    const float* w = wc + k * NPOS;
+                    const float W0 = w[0], Wu = w[-HX], Wd = w[HX], Wl = w[-1];
+                    const float Wul = w[-HX - 1], Wdr = w[HX + 1], Wld = w[HX - 1];
+                    float tmp;
+                    if constexpr (MODE == 0) {
+                        const float rho = __fmaf_rn((float)(d0 + k), a.drho, a.rho0);
+                        const float B4 = warp_fetch(src, W, H, xr, yr, zr, h, rho);
+                        const float B8 = warp_fetch(src, W, H, xru, yru, zru, h, rho);
+                        tmp = fabsf(__fsub_rn(Rc, W0));                    // 0  (:93)
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rd, Wu)));    // 1  (:106)
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Ru, Wd)));    // 2  (:119)
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rl, Wl)));    // 3  (:132)
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rr, B4)));    // 4  (:145)
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rul, Wul)));  // 5  (:159)
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rdr, Wdr)));  // 6  (:172)
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rld, Wld)));  // 7  (:185)
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rru, B8)));   // 8  (:198)
+                    } else {
+                        const float Wr = w[1], Wru = w[-HX + 1];
+                        tmp = fabsf(__fsub_rn(Rc, W0));
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Ru, Wu)));
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rd, Wd)));
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rl, Wl)));
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rr, Wr)));
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rul, Wul)));
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rdr, Wdr)));
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rld, Wld)));
+                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rru, Wru)));
+                    }
+                    if (tmp == tmp) {   // a rejected sample skips the voxel (calc_cost.cu:89-91)
+                        const float m = __fdiv_rn(tmp, 9.0f);
+                        if (acc[k] < 0.0f) {                         // first measurement (:200-203)
+                            acc[k] = m;
+                            cn[k] = 1.0f;
+                        } else {                                     // running mean (:205-206)
+                            const float n1 = __fadd_rn(cn[k], 1.0f);
+                            acc[k] = __fdiv_rn(__fmaf_rn(cn[k], acc[k], m), n1);
+                            cn[k] = n1;
+                        }
+                    }
+                }
+            }
+        }
+
+        // transpose through shared memory and store 128-byte rows of the volume
+        for (int pass = 0; pass < (a.cnt ? 2 : 1); ++pass) {
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < PC; ++k) wt[tid * SP + k] = pass == 0 ? acc[k] : cn[k];
+            __syncthreads();
+            for (int i = 0; i < TX; ++i) {
+                const int pu = x0 + i, pv = y0 + ty;
+                if (pu < W && pv < H) {
+                    const size_t e = ((size_t)pv * W + pu) * D + d0 + tx;
+                    const float val = wt[(ty * TX + i) * SP + tx];
+                    if (pass == 0) store_cost<HALF>(a.cost, e, val);
+                    else a.cnt[e] = val;
+                }
+            }
+        }
+        if (inside) {
+#pragma unroll
+            for (int k = 0; k < PC; ++k) pix_invalid |= (cn[k] == 0.0f);
+        }
+    }
+    if (a.invalid && inside) a.invalid[(size_t)v * W + u] = pix_invalid ? 1 : 0;
+}
+
+}  // namespace
+
+cudaError_t launch_cost(const CostLaunch& a, cudaStream_t s) {
+    const dim3 grid((a.W + TX - 1) / TX, (a.H + TY - 1) / TY);
+    const dim3 block(NT);
+    if (a.mode == 0) {
+        if (a.cost_half) cost_kernel<0, true><<<grid, block, 0, s>>>(a);
+        else cost_kernel<0, false><<<grid, block, 0, s>>>(a);
+    } else {
+        if (a.cost_half) cost_kernel<1, true><<<grid, block, 0, s>>>(a);
+        else cost_kernel<1, false><<<grid, block, 0, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace pm

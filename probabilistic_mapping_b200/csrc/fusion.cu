@@ -1,0 +1,146 @@
+// fusion.cu -- Gaussian x uniform Bayesian depth fusion (reference: depth_fusion.cu:3-280).
+//
+// The reference runs four kernels with a device synchronisation after each (transformMap,
+// hole_filling, depth_predict, depthUpdate) and resolves the z-buffer and the hole filling
+// with racy atomicCAS loops, so its output depends on thread timing.  Here:
+//   * fuse_transform_kernel forward-warps the confident previous state and resolves the
+//     z-test with one 64-bit atomicMin on (depth bits << 32 | pixel index): the nearest
+//     surface wins and ties go to the smaller index, independent of scheduling;
+//   * fuse_update_kernel fuses hole filling (a gather over the 3x3 neighbourhood of the
+//     unfilled table: the first occupied interior neighbour in raster order), the state
+//     prediction and the Bayesian update, reading each previous-state entry once.
+// Both rules are one legal outcome of the reference's races.  The double-precision
+// promotions of the reference expressions (0.4, 0.6, 0.05, 0.01 and M_PI literals) are kept.
+#include "pm_device.cuh"
+
+namespace pm {
+namespace {
+
+constexpr unsigned long long kEmpty = ~0ull;
+
+__global__ void __launch_bounds__(256) fuse_transform_kernel(const FuseLaunch a) {
+    const int W = a.W, H = a.H;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= W || y >= H) return;
+    const int index = y * W + x;
+    const float al = a.pre[0][index];
+    if ((double)al < kFloatEps) return;                                    // (:26)
+    const float be = a.pre[1][index];
+    if ((double)__fdiv_rn(al, __fadd_rn(al, be)) < 0.4) return;            // (:30)
+    const float dep = a.pre[2][index];
+    const float fx = a.cam[0], fy = a.cam[1], cx = a.cam[2], cy = a.cam[3];
+    const float px = __fmul_rn(__fdiv_rn(__fsub_rn((float)x, cx), fx), dep);   // (:34)
+    const float py = __fmul_rn(__fdiv_rn(__fsub_rn((float)y, cy), fy), dep);
+    const float pz = dep;
+    const float* p = a.pose;
+    const float px2 = __fmaf_rn(p[0], px, __fmaf_rn(p[1], py, __fmaf_rn(p[2], pz, p[9])));
+    const float py2 = __fmaf_rn(p[3], px, __fmaf_rn(p[4], py, __fmaf_rn(p[5], pz, p[10])));
+    const float pz2 = __fmaf_rn(p[6], px, __fmaf_rn(p[7], py, __fmaf_rn(p[8], pz, p[11])));
+    if ((double)pz2 < kFloatEps) return;                                   // (:40)
+    const int x2 = __double2int_rz(__dadd_rn((double)__fadd_rn(__fmul_rn(__fdiv_rn(px2, pz2), fx), cx), 0.5));
+    const int y2 = __double2int_rz(__dadd_rn((double)__fadd_rn(__fmul_rn(__fdiv_rn(py2, pz2), fy), cy), 0.5));
+    if (x2 < 0 || x2 >= W || y2 < 0 || y2 >= H) return;
+    a.pre[2][index] = pz2;                                                 // (:48)
+    a.pre[3][index] = __double2float_rn(__dadd_rn((double)a.pre[3][index], __dmul_rn((double)pz2, 0.05)));
+    if (index == 0) return;   // index 0 encodes "empty" in the reference's table
+    const unsigned long long key = ((unsigned long long)__float_as_uint(pz2) << 32) | (unsigned)index;
+    atomicMin(a.ztable + (size_t)y2 * W + x2, key);
+}
+
+__device__ __forceinline__ float normpdf(float x, float mu, float sig) {   // (:3-6)
+    const float d = __fsub_rn(x, mu);
+    return __fmul_rn(expf(__fdiv_rn(__fmul_rn(-d, d), __fmul_rn(2.0f, sig))),
+                     rsqrtf(__double2float_rn(__dmul_rn(2.0 * M_PI, (double)sig))));
+}
+
+__global__ void __launch_bounds__(256) fuse_update_kernel(const FuseLaunch a) {
+    const int W = a.W, H = a.H;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= W || y >= H) return;
+    const int e = y * W + x;
+
+    // hole filling (:80-105): an empty cell takes the first occupied interior neighbour
+    const unsigned long long k0 = a.ztable[e];
+    int t = k0 == kEmpty ? 0 : (int)(unsigned)(k0 & 0xffffffffu);
+    if (t == 0) {
+        for (int i = -1; i <= 1 && t == 0; ++i)
+            for (int j = -1; j <= 1; ++j) {
+                const int ny = y + i, nx = x + j;
+                if (nx <= 0 || nx >= W - 1 || ny <= 0 || ny >= H - 1) continue;
+                const unsigned long long kk = a.ztable[ny * W + nx];
+                if (kk != kEmpty) { t = (int)(unsigned)(kk & 0xffffffffu); break; }
+            }
+    }
+    if (a.table) a.table[e] = t;
+
+    // depth_predict (:107-137)
+    float ca, cb = 0.0f, cm = 0.0f, cs = 0.0f;
+    if (t == 0) {
+        ca = -1.0f;
+    } else {
+        ca = a.pre[0][t]; cb = a.pre[1][t]; cm = a.pre[2][t]; cs = a.pre[3][t];
+    }
+
+    // depthUpdate (:139-225)
+    const float d = a.depth[e];
+    const float unc = __double2float_rn(__dmul_rn((double)__fmul_rn(d, d), 0.01));   // (:151)
+    float out_d = d;
+    bool write_all = (t != 0);   // predict copied the whole state
+    if ((double)ca < kFloatEps) {                                           // (:161)
+        if ((double)d < kFloatEps) {
+            out_d = 0.0f;
+        } else {
+            ca = 10.0f; cb = 10.0f; cm = d; cs = 2500.0f;
+            write_all = true;
+        }
+    } else if ((double)d < kFloatEps) {                                     // (:176)
+        out_d = ((double)__fdiv_rn(ca, __fadd_rn(ca, cb)) > 0.6) ? cm : 0.0f;
+    } else {
+        const float aa = ca, bb = cb, miu = cm, sq = cs;
+        const float us = __fadd_rn(unc, sq);
+        const float new_sq = __fdiv_rn(__fmul_rn(unc, sq), us);                           // (:195)
+        const float new_miu = __fdiv_rn(__fmaf_rn(d, sq, __fmul_rn(miu, unc)), us);       // (:196)
+        const float ab = __fadd_rn(aa, bb);
+        float c1 = __fmul_rn(__fdiv_rn(aa, ab), normpdf(d, miu, us));                     // (:197)
+        float c2 = __fdiv_rn(__fmul_rn(__fdiv_rn(bb, ab), 1.0f), 50.0f);                  // (:198)
+        const float norm = __fadd_rn(c1, c2);
+        c1 = __fdiv_rn(c1, norm);
+        c2 = __fdiv_rn(c2, norm);
+        const float a1 = __fadd_rn(aa, 1.0f), a2 = __fadd_rn(aa, 2.0f);
+        const float ab1 = __fadd_rn(ab, 1.0f), ab2 = __fadd_rn(ab, 2.0f);
+        const float f = __fadd_rn(__fmul_rn(c1, __fdiv_rn(a1, ab1)), __fmul_rn(c2, __fdiv_rn(aa, ab1)));
+        const float den = __fmul_rn(ab1, ab2);
+        const float ee = __fadd_rn(__fmul_rn(c1, __fdiv_rn(__fmul_rn(a1, a2), den)),
+                                   __fmul_rn(c2, __fdiv_rn(__fmul_rn(aa, a1), den)));
+        const float mu_p = __fadd_rn(__fmul_rn(c1, new_miu), __fmul_rn(c2, miu));
+        const float sig_p = __fsub_rn(__fadd_rn(__fmul_rn(c1, __fadd_rn(new_sq, __fmul_rn(new_miu, new_miu))),
+                                                __fmul_rn(c2, __fadd_rn(sq, __fmul_rn(miu, miu)))),
+                                      __fmul_rn(mu_p, mu_p));
+        const float a_p = __fdiv_rn(__fsub_rn(ee, f), __fsub_rn(f, __fdiv_rn(ee, f)));
+        const float b_p = __fdiv_rn(__fmul_rn(a_p, __fsub_rn(1.0f, f)), f);
+        ca = a_p; cb = b_p; cm = mu_p; cs = sig_p;
+        write_all = true;
+        out_d = ((double)__fdiv_rn(aa, ab) > 0.6) ? mu_p : 0.0f;             // (:219)
+    }
+    a.cur[0][e] = ca;
+    if (write_all) { a.cur[1][e] = cb; a.cur[2][e] = cm; a.cur[3][e] = cs; }
+    a.depth[e] = out_d;
+    if (a.variance) a.variance[e] = write_all ? cs : a.cur[3][e];
+}
+
+}  // namespace
+
+cudaError_t launch_fuse_gpu(const FuseLaunch& a, cudaStream_t s) {
+    const dim3 block(256), grid((a.W + 255) / 256, a.H);
+    cudaError_t e = cudaMemsetAsync(a.ztable, 0xff, sizeof(unsigned long long) * (size_t)a.W * a.H, s);
+    if (e != cudaSuccess) return e;
+    fuse_transform_kernel<<<grid, block, 0, s>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    fuse_update_kernel<<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace pm

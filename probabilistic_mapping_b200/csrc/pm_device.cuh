@@ -1,0 +1,142 @@
+// pm_device.cuh -- device helpers shared by the motion-stereo kernels (sm_100a).
+//
+// Every FP32 expression that the CPU oracle replays is written with explicit round-to-nearest
+// intrinsics (__fmaf_rn, __fmul_rn, __fdiv_rn, __frcp_rn) and the library is compiled with
+// -fmad=false, so no multiply-add is contracted behind our back: the FP32 results are
+// reproducible bit-for-bit on the CPU.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pm_internal.h"
+
+namespace pm {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ float nan_f() { return __int_as_float(0x7fffffff); }
+__device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
+
+// Homography of one source frame as kernel arguments (the 12 floats of ad_calc_cost,
+// calc_cost.cu:212-219).
+struct Hom {
+    float r11, r12, r13, r21, r22, r23, r31, r32, r33, t1, t2, t3;
+};
+
+__device__ __forceinline__ void homog(const Hom& h, int qu, int qv, float& x, float& y, float& z) {
+    const float fu = (float)qu, fv = (float)qv;
+    x = __fmaf_rn(h.r11, fu, __fmaf_rn(h.r12, fv, h.r13));
+    y = __fmaf_rn(h.r21, fu, __fmaf_rn(h.r22, fv, h.r23));
+    z = __fmaf_rn(h.r31, fu, __fmaf_rn(h.r32, fv, h.r33));
+}
+
+// Bilinear fetch with texel centres at integer coordinates and zero border, the filtering of
+// tex2D(t, u + 0.5f, v + 0.5f) with cudaFilterModeLinear / cudaAddressModeBorder
+// (calc_cost.cu:93,230-237), evaluated with exact weights.  Caller guarantees
+// 0 <= u <= W-1 and 0 <= v <= H-1, so only the +1 texels can fall outside.
+__device__ __forceinline__ float bilinear(const float* __restrict__ img, int W, int H, float u, float v) {
+    const float fu = floorf(u), fv = floorf(v);
+    const int i = (int)fu, j = (int)fv;
+    const float a = __fsub_rn(u, fu), b = __fsub_rn(v, fv);
+    const float* row0 = img + (size_t)j * W;
+    const bool in_i1 = (i + 1) < W, in_j1 = (j + 1) < H;
+    const float t00 = __ldg(row0 + i);
+    const float t10 = in_i1 ? __ldg(row0 + i + 1) : 0.0f;
+    const float t01 = in_j1 ? __ldg(row0 + W + i) : 0.0f;
+    const float t11 = (in_i1 && in_j1) ? __ldg(row0 + W + i + 1) : 0.0f;
+    const float top = __fmaf_rn(a, __fsub_rn(t10, t00), t00);
+    const float bot = __fmaf_rn(a, __fsub_rn(t11, t01), t01);
+    return __fmaf_rn(b, __fsub_rn(bot, top), top);
+}
+
+// One warped sample (calc_cost.cu:85-93): w = z + t3*rho, u = (x + t1*rho)/w, v = (y + t2*rho)/w,
+// computed as one correctly rounded reciprocal and two products.  Rejected samples (w < 0 or
+// (u, v) outside [0, W-1] x [0, H-1], NaN included) return NaN, which then poisons the 9-term sum.
+__device__ __forceinline__ float warp_fetch(const float* __restrict__ img, int W, int H, float x, float y,
+                                            float z, const Hom& h, float rho) {
+    const float w = __fmaf_rn(h.t3, rho, z);
+    const float nx = __fmaf_rn(h.t1, rho, x);
+    const float ny = __fmaf_rn(h.t2, rho, y);
+    const float r = __frcp_rn(w);
+    const float u = __fmul_rn(nx, r), v = __fmul_rn(ny, r);
+    const bool ok = (w >= 0.0f) && (u >= 0.0f) && (u <= (float)(W - 1)) && (v >= 0.0f) &&
+                    (v <= (float)(H - 1));
+    return ok ? bilinear(img, W, H, u, v) : nan_f();
+}
+
+// ---- warp reductions --------------------------------------------------------------------
+__device__ __forceinline__ float warp_min_f32(float x) {
+    float r;
+    asm volatile("redux.sync.min.f32 %0, %1, 0xffffffff;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// ---- cp.async (LDGSTS) helpers: a lane copies its own slice into its own shared slot ------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void cp_async_16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_8(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_4(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Copy BYTES from gmem to smem.  Lane slices start at lane*BYTES, so the piece size is the
+// largest of 16/8/4 dividing BYTES: that keeps every piece naturally aligned on both sides.
+template <int BYTES> __device__ __forceinline__ void cp_async_bytes(void* smem, const void* gmem) {
+    static_assert(BYTES % 4 == 0, "cp.async copies at least 4 aligned bytes");
+    constexpr int PIECE = (BYTES % 16 == 0) ? 16 : ((BYTES % 8 == 0) ? 8 : 4);
+    char* s = (char*)smem;
+    const char* g = (const char*)gmem;
+#pragma unroll
+    for (int off = 0; off < BYTES; off += PIECE) {
+        if constexpr (PIECE == 16) cp_async_16(s + off, g + off);
+        else if constexpr (PIECE == 8) cp_async_8(s + off, g + off);
+        else cp_async_4(s + off, g + off);
+    }
+}
+
+// ---- plane vectors: a lane owns PPL consecutive planes -----------------------------------
+template <int PPL> __device__ __forceinline__ void load_planes(float (&v)[PPL], const float* p) {
+    if constexpr (PPL % 4 == 0) {
+#pragma unroll
+        for (int j = 0; j < PPL; j += 4) {
+            const float4 t = *reinterpret_cast<const float4*>(p + j);
+            v[j] = t.x; v[j + 1] = t.y; v[j + 2] = t.z; v[j + 3] = t.w;
+        }
+    } else if constexpr (PPL % 2 == 0) {
+#pragma unroll
+        for (int j = 0; j < PPL; j += 2) {
+            const float2 t = *reinterpret_cast<const float2*>(p + j);
+            v[j] = t.x; v[j + 1] = t.y;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < PPL; ++j) v[j] = p[j];
+    }
+}
+template <int PPL> __device__ __forceinline__ void store_planes(float* p, const float (&v)[PPL]) {
+    if constexpr (PPL % 4 == 0) {
+#pragma unroll
+        for (int j = 0; j < PPL; j += 4)
+            *reinterpret_cast<float4*>(p + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+    } else if constexpr (PPL % 2 == 0) {
+#pragma unroll
+        for (int j = 0; j < PPL; j += 2) *reinterpret_cast<float2*>(p + j) = make_float2(v[j], v[j + 1]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < PPL; ++j) p[j] = v[j];
+    }
+}
+
+}  // namespace pm

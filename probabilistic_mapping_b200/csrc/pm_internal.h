@@ -1,0 +1,84 @@
+// pm_internal.h -- launch descriptors shared by the kernels and the C-ABI runtime.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace pm {
+
+constexpr int kMaxSources = 32;   // source frames evaluated in one cost pass
+constexpr int kMaxPlanes = 256;   // 32 lanes x up to 8 planes per lane
+constexpr float kDepInf = 1000.0f;   // DEP_INF (parameters.h:29)
+constexpr double kFloatEps = 1e-5;   // FLOAT_EPS (parameters.h:6)
+
+// ---- plane-sweep cost volume (calc_cost.cu) ----------------------------------------------
+struct CostLaunch {
+    const float* ref;      // W*H scaled reference image
+    const float* srcs;     // nsrc consecutive W*H scaled source images
+    int W, H, D, nsrc;
+    float rho0, drho;
+    int mode;              // 0 reference quirks, 1 corrected 3x3 patch
+    float hom[kMaxSources][12];
+    void* cost;            // W*H*D float, or __half when cost_half
+    int cost_half;
+    float* cnt;            // running count (incremental mode) or nullptr
+    uint8_t* invalid;      // W*H, 1 where a plane was never measured (optional)
+    int incremental;       // start from (cost, cnt) in memory instead of (-1, 0)
+};
+cudaError_t launch_cost(const CostLaunch& a, cudaStream_t s);
+
+// ---- SGM aggregation + winner-take-all (sgm.cu, filter_cost.cu) ---------------------------
+struct PlaneOrder {
+    uint32_t incl[32];          // bit j of incl[l]: plane l*PPL+j takes part in the reduction tree
+    uint16_t rank[kMaxPlanes];  // tie-break priority of each plane (0 wins)
+};
+// Priority of the reference reduction tree (filter_cost.cu:22-30); compat=0 keeps all planes.
+void plane_order(int D, int compat, PlaneOrder& out);
+
+struct FilterParams {
+    float var_scale, uniq, rho0, drho;
+};
+
+struct SgmLaunch {
+    const void* cost;      // W*H*D float or __half
+    int cost_half;
+    const float* ref;      // W*H scaled reference image (path gradient D1, sgm.cu:75)
+    float* sum;            // W*H*D partial sum of the paths
+    int W, H, D, num_paths;
+    float p1, p2, tau, q1, q2;
+    FilterParams fp;
+    float* depth;          // W*H with byte pitch depth_pitch (fused filter only)
+    size_t depth_pitch;
+    int32_t* index;        // W*H (optional)
+    int store_sum_last;    // fused filter: also store the complete sum
+    PlaneOrder order;
+};
+// Runs the num_paths direction passes in the reference order; with fuse_filter the last pass
+// completes the sum in registers and writes depth/index instead of the sum.
+cudaError_t launch_sgm(const SgmLaunch& a, bool fuse_filter, cudaStream_t s);
+cudaError_t launch_filter(const float* sum, int W, int H, int D, const FilterParams& fp,
+                          const PlaneOrder& order, float* depth, size_t pitch, int32_t* index,
+                          cudaStream_t s);
+
+// ---- image conversion (convert.cu + the uint8 -> float upload) ----------------------------
+cudaError_t launch_to_float(int W, int H, const uint8_t* src, size_t src_pitch, float* dst,
+                            float scale, cudaStream_t s);
+cudaError_t launch_convert(int W, int H, const float* in, float* out, int flag, size_t pitch_bytes,
+                           cudaStream_t s);
+
+// ---- depth fusion (depth_fusion.cu) --------------------------------------------------------
+struct FuseLaunch {
+    int W, H;
+    float pose[12];        // R_p2c row-major, t_p2c
+    float cam[4];          // fx, fy, cx, cy
+    float* depth;          // in: WTA depth, out: fused depth (W*H)
+    float* pre[4];         // alpha, beta, mu, sigma of the previous keyframe (modified)
+    float* cur[4];         // state of the current keyframe (written)
+    unsigned long long* ztable;  // W*H scratch z-buffer
+    int32_t* table;        // W*H filled propagation table (optional)
+    float* variance;       // W*H sigma^2 of the current state (optional)
+};
+cudaError_t launch_fuse_gpu(const FuseLaunch& a, cudaStream_t s);
+
+}  // namespace pm
