@@ -27,6 +27,8 @@ constexpr int NT = TX * TY;             // 256 threads, one per pixel
 constexpr int SP = PC + 1;              // transpose staging pitch (bank-conflict free)
 
 static_assert(NT * SP <= PC * NPOS, "staging must fit into the warp tile");
+static_assert(TX == 32 && NT == TX * TY, "one warp per tile row, one thread per pixel");
+static_assert((TX * PC) % 32 == 0, "the transposed block is moved in whole warp steps");
 
 __device__ __forceinline__ float ref_at(const float* __restrict__ ref, int W, int H, int x, int y) {
     return (x < 0 || y < 0 || x >= W || y >= H) ? 0.0f : __ldg(ref + (size_t)y * W + x);
@@ -68,14 +70,17 @@ __global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
             // running state from memory, transposed through shared memory
             for (int pass = 0; pass < 2; ++pass) {
                 __syncthreads();
-                for (int i = 0; i < TX; ++i) {
+                // warp ty moves the TX x PC block of its pixel row; lane-linear order keeps the
+                // global accesses contiguous within each pixel's plane run
+                for (int q = tx; q < TX * PC; q += 32) {
+                    const int i = q / PC, k = q - i * PC;
                     const int pu = x0 + i, pv = y0 + ty;
                     float val = 0.0f;
                     if (pu < W && pv < H) {
-                        const size_t e = ((size_t)pv * W + pu) * D + d0 + tx;
+                        const size_t e = ((size_t)pv * W + pu) * D + d0 + k;
                         val = pass == 0 ? load_cost<HALF>(a.cost, e) : a.cnt[e];
                     }
-                    wt[(ty * TX + i) * SP + tx] = val;
+                    wt[(ty * TX + i) * SP + k] = val;
                 }
                 __syncthreads();
 #pragma unroll
@@ -169,11 +174,12 @@ __global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
 #pragma unroll
             for (int k = 0; k < PC; ++k) wt[tid * SP + k] = pass == 0 ? acc[k] : cn[k];
             __syncthreads();
-            for (int i = 0; i < TX; ++i) {
+            for (int q = tx; q < TX * PC; q += 32) {
+                const int i = q / PC, k = q - i * PC;
                 const int pu = x0 + i, pv = y0 + ty;
                 if (pu < W && pv < H) {
-                    const size_t e = ((size_t)pv * W + pu) * D + d0 + tx;
-                    const float val = wt[(ty * TX + i) * SP + tx];
+                    const size_t e = ((size_t)pv * W + pu) * D + d0 + k;
+                    const float val = wt[(ty * TX + i) * SP + k];
                     if (pass == 0) store_cost<HALF>(a.cost, e, val);
                     else a.cnt[e] = val;
                 }
