@@ -174,16 +174,18 @@ PM_API pm_status pm_stage_calc_cost(const pm_config* cfg, const float* ref, cons
                              const float* homs, float* cost, float* cnt, uint8_t* invalid,
                              void* stream);
 
-/* sgm2 (sgm.cu:115-135): out := sum over cfg->num_paths paths; out needs no clearing. */
+/* sgm2 (sgm.cu:115-135): out := sum over cfg->num_paths paths; out needs no clearing.  The
+ * paths run as four groups {g, g+4} with their own partial sums, added as
+ * (S0 + S1) + (S2 + S3); scratch holds the partials of groups 1..3 (3*W*H*D floats). */
 PM_API pm_status pm_stage_sgm(const pm_config* cfg, const float* cost, const float* ref, float* out,
-                       void* stream);
+                       float* scratch, void* stream);
 
 /* filter_cost (filter_cost.cu:57-70): depth with a byte pitch; index (optional) W*H. */
 PM_API pm_status pm_stage_filter(const pm_config* cfg, const float* sgm, float* depth, size_t pitch_bytes,
                           int32_t* index, void* stream);
 
 /* sgm2 + filter_cost fused: the last path finishes the sum in registers and runs the
- * winner-take-all; `scratch` holds the partial sum (W*H*D floats). */
+ * winner-take-all; `scratch` holds the four partial sums (4*W*H*D floats). */
 PM_API pm_status pm_stage_sgm_filter(const pm_config* cfg, const float* cost, const float* ref,
                               float* scratch, float* depth, size_t pitch_bytes, int32_t* index,
                               void* stream);

@@ -35,7 +35,7 @@ class OrcParams(ctypes.Structure):
         ("p1", ctypes.c_double), ("p2", ctypes.c_double), ("tau_so", ctypes.c_double),
         ("q1", ctypes.c_double), ("q2", ctypes.c_double),
         ("var_scale", ctypes.c_double), ("uniqueness", ctypes.c_double),
-        ("tree_compat", ctypes.c_int),
+        ("tree_compat", ctypes.c_int), ("sum_order", ctypes.c_int),
     ]
 
 
@@ -59,12 +59,13 @@ class Params:
     var_scale: float = 1.02
     uniqueness: float = 0.0
     tree_compat: int = 1
+    sum_order: int = 1          # 0 reference path order, 1 grouped order of the B200 kernels
 
     def c(self) -> OrcParams:
         return OrcParams(self.W, self.H, self.D, self.rho0, self.drho, self.intensity_scale,
                          self.cost_mode, self.bilinear_quant, self.num_paths, self.p1, self.p2,
                          self.tau_so, self.q1, self.q2, self.var_scale, self.uniqueness,
-                         self.tree_compat)
+                         self.tree_compat, self.sum_order)
 
 
 def build(force: bool = False) -> str:

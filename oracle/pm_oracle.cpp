@@ -217,15 +217,52 @@ struct Dir { int dx, dy; };
 const Dir kDirs[8] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1}, {-1, 1}, {1, -1}};
 
 // a4 -- sgm.cu:5-113 (one scanline), host order sgm.cu:115-135.
+// sum_order 0 accumulates the paths in the reference's order (L->R, R->L, T->B, B->T, then
+// the diagonals) into one buffer.  sum_order 1 is the order of the B200 kernels, which run the
+// paths as four concurrent groups {r, r+4}: group g accumulates its paths into part[g], and
+// the result is (part0 + part1) + (part2 + part3).  The two differ only in FP rounding.
+template <typename S>
+void sgm_paths(const orc_params* p, const uint8_t* ref8, const S* C, S* out, const int* group_of,
+               std::vector<S*>& parts);
+
 template <typename S>
 void sgm(const orc_params* p, const uint8_t* ref8, const S* C, S* out) {
+    const size_t V = (size_t)p->W * p->H * p->D;
+    int group_of[8];
+    std::vector<std::vector<S>> bufs;
+    std::vector<S*> parts;
+    if (p->sum_order == 0) {
+        for (int r = 0; r < 8; ++r) group_of[r] = 0;
+        parts.push_back(out);
+    } else {
+        for (int r = 0; r < 8; ++r) group_of[r] = r % 4;
+        parts.push_back(out);
+        for (int g = 1; g < 4; ++g) {
+            bufs.emplace_back(V);
+            parts.push_back(bufs.back().data());
+        }
+    }
+    sgm_paths<S>(p, ref8, C, out, group_of, parts);
+    if (p->sum_order != 0) {
+        const S* a = parts[1];
+        const S* b = parts[2];
+        const S* c = parts[3];
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < (long)V; ++i) out[i] = (out[i] + a[i]) + (b[i] + c[i]);
+    }
+}
+
+template <typename S>
+void sgm_paths(const orc_params* p, const uint8_t* ref8, const S* C, S* out, const int* group_of,
+               std::vector<S*>& parts) {
+    (void)out;
     const int W = p->W, H = p->H, D = p->D;
     const size_t N = (size_t)W * H;
     std::vector<S> refv = to_scalar<S>(ref8, (int)N, p->intensity_scale);
     std::vector<int> rank, incl;
     tree_order(D, p->tree_compat, rank, incl);
     const S P1b = (S)p->p1, P2b = (S)p->p2, tau = (S)p->tau_so, q1 = (S)p->q1, q2 = (S)p->q2;
-    std::fill(out, out + N * D, (S)0);   // sgm_cost.setTo(0) (stereo_mapper.cpp:100)
+    for (S* part : parts) std::fill(part, part + N * D, (S)0);   // sgm_cost.setTo(0) (stereo_mapper.cpp:100)
     auto minincl = [&](const S* v) {
         S m = std::numeric_limits<S>::infinity();
         for (int d = 0; d < D; ++d)
@@ -234,6 +271,7 @@ void sgm(const orc_params* p, const uint8_t* ref8, const S* C, S* out) {
     };
     for (int r = 0; r < p->num_paths; ++r) {
         const int dx = kDirs[r].dx, dy = kDirs[r].dy;
+        S* const acc = parts[group_of[r]];
         // chain starts: pixels whose predecessor (x-dx, y-dy) lies outside the image
         std::vector<std::pair<int, int>> starts;
         for (int y = 0; y < H; ++y)
@@ -248,7 +286,7 @@ void sgm(const orc_params* p, const uint8_t* ref8, const S* C, S* out) {
             S mprev = 0;
             for (int k = 0; x >= 0 && y >= 0 && x < W && y < H; ++k, x += dx, y += dy) {
                 const S* c = C + ((size_t)y * W + x) * D;
-                S* o = out + ((size_t)y * W + x) * D;
+                S* o = acc + ((size_t)y * W + x) * D;
                 const bool invalid = minincl(c) < (S)0;   // (:33, :67) COST_INF = 0
                 if (k == 0) {
                     for (int d = 0; d < D; ++d) {

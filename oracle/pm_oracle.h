@@ -39,6 +39,7 @@ typedef struct orc_params {
     double var_scale;     /* parameters.cpp:18 */
     double uniqueness;    /* extension: reject when best > ratio * second best; <=0 or >=1 disables */
     int tree_compat;      /* 1 = reproduce the reduction tree of sgm.cu:24-31 for non power-of-two D */
+    int sum_order;        /* 0 = reference path order, 1 = grouped order of the B200 kernels */
 } orc_params;
 
 /* a1: H1 = K R_r^T R_l K^-1, H2 = K R_r^T (T_l - T_r)  (stereo_mapper.cpp:79-80).

@@ -71,7 +71,7 @@ SIGNATURES = {
     "pm_status_string": (ctypes.c_char_p, [_I]),
     "pm_stage_to_float": (_I, [_I, _I, _VP, _SZ, _VP, _F, _VP]),
     "pm_stage_calc_cost": (_I, [_P(PmConfig), _VP, _VP, _I, _P(ctypes.c_float), _VP, _VP, _VP, _VP]),
-    "pm_stage_sgm": (_I, [_P(PmConfig), _VP, _VP, _VP, _VP]),
+    "pm_stage_sgm": (_I, [_P(PmConfig), _VP, _VP, _VP, _VP, _VP]),
     "pm_stage_filter": (_I, [_P(PmConfig), _VP, _VP, _SZ, _VP, _VP]),
     "pm_stage_sgm_filter": (_I, [_P(PmConfig), _VP, _VP, _VP, _VP, _SZ, _VP, _VP]),
     "pm_stage_depth_fuse": (_I, [_I, _I, _P(ctypes.c_float), _P(ctypes.c_float), _VP, _P(_VP), _P(_VP),

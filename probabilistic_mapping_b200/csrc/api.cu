@@ -27,7 +27,7 @@ struct pm_mapper {
 
     uint8_t* d_u8 = nullptr;    // upload staging, W*H bytes
     float* d_ref = nullptr;     // scaled reference image
-    float* d_src = nullptr;     // max_sources scaled source images
+    float4* d_srcq = nullptr;   // max_sources source frames in the quad layout
     int nsrc = 0;               // queued (not yet folded) sources
     std::vector<float> homs;    // 12 floats per queued source
     std::vector<float> all_homs;  // every source since initReference (inspection)
@@ -37,7 +37,9 @@ struct pm_mapper {
 
     void* d_cost = nullptr;     // W*H*D float or half
     float* d_cnt = nullptr;     // allocated on the first fold
-    float* d_sum = nullptr;     // SGM partial sums
+    float* d_part[4] = {};      // SGM partial sums of the four path groups
+    SgmStreams side{};          // concurrent path groups
+    bool have_side = false;
     float* d_depth = nullptr;   // WTA depth, linear
     int32_t* d_idx = nullptr;   // WTA plane index
     bool store_sgm = false;
@@ -193,18 +195,22 @@ void fill_sgm_launch(const pm_config& c, const PlaneOrder& order, SgmLaunch& a) 
     a.order = order;
 }
 
-pm_status upload_image(pm_mapper* h, const uint8_t* img, size_t pitch, float* dst) {
+// Uploads a uint8 frame (host or device) and converts it to the scaled float image (dst) or,
+// for source frames, to the quad layout the cost kernel samples (dstq).
+pm_status upload_image(pm_mapper* h, const uint8_t* img, size_t pitch, float* dst, float4* dstq) {
     const int W = h->cfg.width, H = h->cfg.height;
     if (!img) return fail(h, PM_ERR_INVALID_ARGUMENT, "image pointer is NULL");
     if (pitch == 0) pitch = (size_t)W;
     if (pitch < (size_t)W) return fail(h, PM_ERR_INVALID_ARGUMENT, "image pitch %zu < width %d", pitch, W);
-    if (is_device_ptr(img)) {
-        PM_CK(h, launch_to_float(W, H, img, pitch, dst, h->cfg.intensity_scale, h->stream));
-    } else {
+    const uint8_t* dev = img;
+    if (!is_device_ptr(img)) {
         PM_CK(h, cudaMemcpy2DAsync(h->d_u8, (size_t)W, img, pitch, (size_t)W, (size_t)H, cudaMemcpyHostToDevice,
                                    h->stream));
-        PM_CK(h, launch_to_float(W, H, h->d_u8, (size_t)W, dst, h->cfg.intensity_scale, h->stream));
+        dev = h->d_u8;
+        pitch = (size_t)W;
     }
+    if (dstq) PM_CK(h, launch_to_quad(W, H, dev, pitch, dstq, h->cfg.intensity_scale, h->stream));
+    else PM_CK(h, launch_to_float(W, H, dev, pitch, dst, h->cfg.intensity_scale, h->stream));
     return PM_OK;
 }
 
@@ -215,7 +221,7 @@ pm_status evaluate_cost(pm_mapper* h, bool into_state) {
     CostLaunch a;
     fill_cost_launch(c, a);
     a.ref = h->d_ref;
-    a.srcs = h->d_src;
+    a.srcq = h->d_srcq;
     a.nsrc = h->nsrc;
     for (int s = 0; s < h->nsrc; ++s)
         for (int i = 0; i < 12; ++i) a.hom[s][i] = h->homs[12 * s + i];
@@ -241,12 +247,12 @@ pm_status run_sgm_filter(pm_mapper* h) {
     fill_sgm_launch(c, h->order, a);
     a.cost = h->d_cost;
     a.ref = h->d_ref;
-    a.sum = h->d_sum;
+    for (int g = 0; g < 4; ++g) a.part[g] = h->d_part[g];
+    a.total = h->store_sgm ? h->d_part[0] : nullptr;   // the final pass reads part[0] before writing
     a.depth = h->d_depth;
     a.depth_pitch = sizeof(float) * (size_t)c.width;
     a.index = h->d_idx;
-    a.store_sum_last = h->store_sgm ? 1 : 0;
-    PM_CK(h, launch_sgm(a, true, h->stream));
+    PM_CK(h, launch_sgm(a, true, h->stream, h->have_side ? &h->side : nullptr));
     return PM_OK;
 }
 
@@ -279,10 +285,10 @@ pm_status copy_out(pm_mapper* h, float* dst, size_t pitch, const float* src) {
 void release(pm_mapper* h) {
     cudaFree(h->d_u8);
     cudaFree(h->d_ref);
-    cudaFree(h->d_src);
+    cudaFree(h->d_srcq);
     cudaFree(h->d_cost);
     cudaFree(h->d_cnt);
-    cudaFree(h->d_sum);
+    for (auto* p : h->d_part) cudaFree(p);
     cudaFree(h->d_depth);
     cudaFree(h->d_idx);
     for (auto& s : h->d_state)
@@ -293,6 +299,11 @@ void release(pm_mapper* h) {
     cudaFree(h->d_var);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
+    for (int g = 0; g < 3; ++g) {
+        if (h->side.stream[g]) cudaStreamDestroy(h->side.stream[g]);
+        if (h->side.join[g]) cudaEventDestroy(h->side.join[g]);
+    }
+    if (h->side.fork) cudaEventDestroy(h->side.fork);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -345,13 +356,21 @@ pm_status pm_create(const pm_config* cfg, pm_mapper** out) {
     bool ok = note(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->own_stream = ok;
     ok = ok && alloc((void**)&h->d_u8, N) && alloc((void**)&h->d_ref, 4 * N) &&
-         alloc((void**)&h->d_src, 4 * N * cfg->max_sources) && alloc(&h->d_cost, esz * V) &&
-         alloc((void**)&h->d_sum, 4 * V) && alloc((void**)&h->d_depth, 4 * N) &&
+         alloc((void**)&h->d_srcq, 16 * N * cfg->max_sources) && alloc(&h->d_cost, esz * V) &&
+         alloc((void**)&h->d_depth, 4 * N) &&
          alloc((void**)&h->d_idx, 4 * N) && alloc((void**)&h->d_ztable, 8 * N) &&
          alloc((void**)&h->d_table, 4 * N) && alloc((void**)&h->d_fused, 4 * N) &&
          alloc((void**)&h->d_var, 4 * N);
+    for (int g4 = 0; g4 < 4 && ok; ++g4) ok = alloc((void**)&h->d_part[g4], 4 * V);
     for (int s = 0; s < 2 && ok; ++s)
         for (int k = 0; k < 4 && ok; ++k) ok = alloc((void**)&h->d_state[s][k], 4 * N);
+    if (ok) {
+        ok = note(cudaEventCreateWithFlags(&h->side.fork, cudaEventDisableTiming));
+        for (int g3 = 0; g3 < 3 && ok; ++g3)
+            ok = note(cudaStreamCreateWithFlags(&h->side.stream[g3], cudaStreamNonBlocking)) &&
+                 note(cudaEventCreateWithFlags(&h->side.join[g3], cudaEventDisableTiming));
+        h->have_side = ok;
+    }
     if (ok) ok = cudaMemsetAsync(h->d_table, 0, 4 * N, h->stream) == cudaSuccess;
     for (int s = 0; s < 2 && ok; ++s)
         for (int k = 0; k < 4 && ok; ++k) ok = cudaMemsetAsync(h->d_state[s][k], 0, 4 * N, h->stream) == cudaSuccess;
@@ -401,7 +420,7 @@ pm_status pm_init_intrinsic(pm_mapper* h, const double K[9], float bf, float dep
 pm_status pm_init_reference(pm_mapper* h, const uint8_t* img, size_t pitch) {
     if (!h) return PM_ERR_INVALID_ARGUMENT;
     DeviceGuard g(h->cfg.device);
-    pm_status st = upload_image(h, img, pitch, h->d_ref);
+    pm_status st = upload_image(h, img, pitch, h->d_ref, nullptr);
     if (st != PM_OK) return st;
     h->have_ref = true;
     h->nsrc = 0;
@@ -427,7 +446,7 @@ pm_status pm_update(pm_mapper* h, const uint8_t* img, size_t pitch, const double
     }
     float hom[12];
     compose_homography(h->K, R_l, T_l, R_r, T_r, hom);
-    pm_status st = upload_image(h, img, pitch, h->d_src + (size_t)h->nsrc * h->cfg.width * h->cfg.height);
+    pm_status st = upload_image(h, img, pitch, nullptr, h->d_srcq + (size_t)h->nsrc * h->cfg.width * h->cfg.height);
     if (st != PM_OK) return st;
     h->homs.insert(h->homs.end(), hom, hom + 12);
     h->all_homs.insert(h->all_homs.end(), hom, hom + 12);
@@ -561,7 +580,7 @@ pm_status pm_set_state(pm_mapper* h, const float* alpha, const float* beta, cons
 pm_status pm_get_buffers(pm_mapper* h, pm_buffers* out) {
     if (!h || !out) return PM_ERR_INVALID_ARGUMENT;
     out->cost = h->d_cost;
-    out->sgm = h->d_sum;
+    out->sgm = h->d_part[0];
     out->wta_index = h->d_idx;
     out->wta_depth = h->d_depth;
     out->table = h->d_table;
@@ -662,8 +681,9 @@ pm_status pm_stage_calc_cost(const pm_config* cfg, const float* ref, const float
     return PM_OK;
 }
 
-pm_status pm_stage_sgm(const pm_config* cfg, const float* cost, const float* ref, float* out, void* stream) {
-    if (check_config(cfg, nullptr) != PM_OK || !cost || !ref || !out) return PM_ERR_INVALID_ARGUMENT;
+pm_status pm_stage_sgm(const pm_config* cfg, const float* cost, const float* ref, float* out, float* scratch,
+                       void* stream) {
+    if (check_config(cfg, nullptr) != PM_OK || !cost || !ref || !out || !scratch) return PM_ERR_INVALID_ARGUMENT;
     if (cfg->precision != PM_PREC_FP32) return PM_ERR_UNSUPPORTED;
     PlaneOrder order;
     plane_order(cfg->num_planes, cfg->tree_compat, order);
@@ -671,8 +691,11 @@ pm_status pm_stage_sgm(const pm_config* cfg, const float* cost, const float* ref
     fill_sgm_launch(*cfg, order, a);
     a.cost = cost;
     a.ref = ref;
-    a.sum = out;
-    return launch_sgm(a, false, (cudaStream_t)stream) == cudaSuccess ? PM_OK : PM_ERR_CUDA;
+    const size_t V = (size_t)cfg->width * cfg->height * cfg->num_planes;
+    a.part[0] = out;   // the final pass reads part[0] before it writes the total there
+    for (int g = 1; g < 4; ++g) a.part[g] = scratch + (g - 1) * V;
+    a.total = out;
+    return launch_sgm(a, false, (cudaStream_t)stream, nullptr) == cudaSuccess ? PM_OK : PM_ERR_CUDA;
 }
 
 pm_status pm_stage_filter(const pm_config* cfg, const float* sgm, float* depth, size_t pitch, int32_t* index,
@@ -701,11 +724,13 @@ pm_status pm_stage_sgm_filter(const pm_config* cfg, const float* cost, const flo
     fill_sgm_launch(*cfg, order, a);
     a.cost = cost;
     a.ref = ref;
-    a.sum = scratch;
+    const size_t V = (size_t)cfg->width * cfg->height * cfg->num_planes;
+    for (int g = 0; g < 4; ++g) a.part[g] = scratch + g * V;
+    a.total = nullptr;
     a.depth = depth;
     a.depth_pitch = pitch;
     a.index = index;
-    return launch_sgm(a, true, (cudaStream_t)stream) == cudaSuccess ? PM_OK : PM_ERR_CUDA;
+    return launch_sgm(a, true, (cudaStream_t)stream, nullptr) == cudaSuccess ? PM_OK : PM_ERR_CUDA;
 }
 
 pm_status pm_stage_depth_fuse(int W, int H, const float pose[12], const float cam[4], float* depth,

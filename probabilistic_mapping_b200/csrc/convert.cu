@@ -19,6 +19,24 @@ __global__ void __launch_bounds__(256) to_float_kernel(int W, int H, const uint8
         out[x] = __fmul_rn((float)row[x], scale);
 }
 
+__global__ void __launch_bounds__(256) to_quad_kernel(int W, int H, const uint8_t* __restrict__ src,
+                                                      size_t pitch, float4* __restrict__ dst, float scale) {
+    const int y = blockIdx.y;
+    const uint8_t* r0 = src + (size_t)y * pitch;
+    const uint8_t* r1 = r0 + pitch;
+    const bool has1 = (y + 1) < H;
+    float4* out = dst + (size_t)y * W;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < W; x += gridDim.x * blockDim.x) {
+        const bool hasx = (x + 1) < W;
+        float4 q;
+        q.x = __fmul_rn((float)r0[x], scale);
+        q.y = hasx ? __fmul_rn((float)r0[x + 1], scale) : 0.0f;
+        q.z = has1 ? __fmul_rn((float)r1[x], scale) : 0.0f;
+        q.w = (has1 && hasx) ? __fmul_rn((float)r1[x + 1], scale) : 0.0f;
+        out[x] = q;
+    }
+}
+
 __global__ void __launch_bounds__(256) convert_kernel(int W, int H, const float* __restrict__ in,
                                                       float* __restrict__ out, int flag, size_t pitch) {
     const int y = blockIdx.y;
@@ -39,6 +57,13 @@ cudaError_t launch_to_float(int W, int H, const uint8_t* src, size_t src_pitch, 
                             cudaStream_t s) {
     const dim3 grid((W + 255) / 256, H);
     to_float_kernel<<<grid, 256, 0, s>>>(W, H, src, src_pitch, dst, scale);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_to_quad(int W, int H, const uint8_t* src, size_t src_pitch, float4* dst, float scale,
+                           cudaStream_t s) {
+    const dim3 grid((W + 255) / 256, H);
+    to_quad_kernel<<<grid, 256, 0, s>>>(W, H, src, src_pitch, dst, scale);
     return cudaGetLastError();
 }
 

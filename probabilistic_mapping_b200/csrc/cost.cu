@@ -9,10 +9,16 @@
 //     are then read from that tile instead of being warped again (the two samples the
 //     reference computes from a corrupted neighbour, calc_cost.cu:50-51 and :70-71, are
 //     per-voxel and stay direct warps in reference mode);
+//   * source frames are stored as "quads": pixel (x, y) holds its 2x2 bilinear footprint
+//     (I(x,y), I(x+1,y), I(x,y+1), I(x+1,y+1)) with the texture border (zero) already applied,
+//     so every bilinear sample is one aligned 16-byte load;
 //   * all source frames queued since initReference are folded in one pass with the
-//     reference's running-mean update kept in registers, so the volume is written once;
-//   * the tile is transposed through shared memory so the volume is stored with 128-byte
-//     coalesced rows in the plane-innermost layout (cuda_utils.h:34).
+//     reference's running-mean update kept in registers, so the volume is written once; the
+//     two divisions of the update use a reciprocal-multiply with one FMA correction step
+//     (Markstein), exhaustively checked to equal the correctly rounded quotient whenever the
+//     quotient is a normal number -- below that the code falls back to IEEE division;
+//   * the tile is transposed through shared memory so the volume is stored with contiguous
+//     plane runs in the plane-innermost layout (cuda_utils.h:34).
 // All FP32 arithmetic uses explicit round-to-nearest intrinsics (see pm_device.cuh).
 #include "pm_device.cuh"
 
@@ -25,10 +31,12 @@ constexpr int HX = TX + 2, HY = TY + 2; // tile + halo
 constexpr int NPOS = HX * HY;           // 340 warped positions
 constexpr int NT = TX * TY;             // 256 threads, one per pixel
 constexpr int SP = PC + 1;              // transpose staging pitch (bank-conflict free)
+constexpr int MAXCNT = kMaxSources + 2; // reciprocal table covers counts 0..kMaxSources+1
 
 static_assert(NT * SP <= PC * NPOS, "staging must fit into the warp tile");
 static_assert(TX == 32 && NT == TX * TY, "one warp per tile row, one thread per pixel");
 static_assert((TX * PC) % 32 == 0, "the transposed block is moved in whole warp steps");
+static_assert(MAXCNT <= NT, "the reciprocal table is filled by one thread per entry");
 
 __device__ __forceinline__ float ref_at(const float* __restrict__ ref, int W, int H, int x, int y) {
     return (x < 0 || y < 0 || x >= W || y >= H) ? 0.0f : __ldg(ref + (size_t)y * W + x);
@@ -43,17 +51,62 @@ template <bool HALF> __device__ __forceinline__ float load_cost(const void* base
     else return reinterpret_cast<const float*>(base)[i];
 }
 
+// Source access: quad layout (one 16-byte load per bilinear sample) or plain float rows.
+template <bool QUAD> struct Src;
+template <> struct Src<true> {
+    const float4* __restrict__ q;
+    int W, H;
+    __device__ __forceinline__ float fetch(float u, float v) const {
+        const float fu = floorf(u), fv = floorf(v);
+        const float4 t = __ldg(q + (size_t)(int)fv * W + (int)fu);
+        const float a = __fsub_rn(u, fu), b = __fsub_rn(v, fv);
+        const float top = __fmaf_rn(a, __fsub_rn(t.y, t.x), t.x);
+        const float bot = __fmaf_rn(a, __fsub_rn(t.w, t.z), t.z);
+        return __fmaf_rn(b, __fsub_rn(bot, top), top);
+    }
+};
+template <> struct Src<false> {
+    const float* __restrict__ p;
+    int W, H;
+    __device__ __forceinline__ float fetch(float u, float v) const { return bilinear(p, W, H, u, v); }
+};
+
+// warp_fetch of pm_device.cuh over either source layout
+template <bool QUAD>
+__device__ __forceinline__ float warp_sample(const Src<QUAD>& src, float x, float y, float z, const Hom& h,
+                                             float rho) {
+    const float w = __fmaf_rn(h.t3, rho, z);
+    const float nx = __fmaf_rn(h.t1, rho, x);
+    const float ny = __fmaf_rn(h.t2, rho, y);
+    const float r = __frcp_rn(w);
+    const float u = __fmul_rn(nx, r), v = __fmul_rn(ny, r);
+    const bool ok = (w >= 0.0f) && (u >= 0.0f) && (u <= (float)(src.W - 1)) && (v >= 0.0f) &&
+                    (v <= (float)(src.H - 1));
+    return ok ? src.fetch(u, v) : nan_f();
+}
+
+// Correctly rounded x / d for x >= 0 and an integer divisor d with r = RN(1/d): q0 = RN(x r),
+// then one Newton correction with the exact residual fma(-q0, d, x).  Exhaustively equal to
+// IEEE division for d in [2, 33] whenever x / d is normal; tiny x takes the IEEE path.
+__device__ __forceinline__ float div_small(float x, float d, float r) {
+    if (x != 0.0f && x < 1e-30f) return __fdiv_rn(x, d);
+    const float q0 = __fmul_rn(x, r);
+    return __fmaf_rn(__fmaf_rn(-q0, d, x), r, q0);
+}
+
 // MODE 0: reference sample set (calc_cost.cu:83-199); MODE 1: corrected 3x3 patch.
-template <int MODE, bool HALF>
+template <int MODE, bool HALF, bool QUAD>
 __global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
     __shared__ __align__(16) float wt[PC * NPOS];   // warped source samples [plane][position]
     __shared__ float hx[NPOS], hy[NPOS], hz[NPOS];  // homogeneous coordinates of the positions
+    __shared__ float rtab[MAXCNT];                  // RN(1/n)
 
     const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int u = x0 + tx, v = y0 + ty;
     const int W = a.W, H = a.H, D = a.D;
     const bool inside = (u < W) && (v < H);
+    if (tid < MAXCNT) rtab[tid] = tid == 0 ? 0.0f : __frcp_rn((float)tid);
 
     // reference-image patch (border addressing -> 0, calc_cost.cu:230-231)
     const float Rc = ref_at(a.ref, W, H, u, v), Ru = ref_at(a.ref, W, H, u, v - 1);
@@ -61,6 +114,7 @@ __global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
     const float Rr = ref_at(a.ref, W, H, u + 1, v), Rul = ref_at(a.ref, W, H, u - 1, v - 1);
     const float Rdr = ref_at(a.ref, W, H, u + 1, v + 1), Rld = ref_at(a.ref, W, H, u - 1, v + 1);
     const float Rru = ref_at(a.ref, W, H, u + 1, v - 1);
+    const float r9 = __frcp_rn(9.0f);
 
     bool pix_invalid = false;
 
@@ -95,7 +149,11 @@ __global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
         }
 
         for (int s = 0; s < a.nsrc; ++s) {
-            const float* __restrict__ src = a.srcs + (size_t)s * W * H;
+            Src<QUAD> src;
+            if constexpr (QUAD) src.q = a.srcq + (size_t)s * W * H;
+            else src.p = a.srcs + (size_t)s * W * H;
+            src.W = W;
+            src.H = H;
             Hom h;
             h.r11 = a.hom[s][0]; h.r12 = a.hom[s][1]; h.r13 = a.hom[s][2];
             h.r21 = a.hom[s][3]; h.r22 = a.hom[s][4]; h.r23 = a.hom[s][5];
@@ -111,7 +169,7 @@ __global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
             for (int i = tid; i < PC * NPOS; i += NT) {
                 const int k = i / NPOS, p = i - k * NPOS;
                 const float rho = __fmaf_rn((float)(d0 + k), a.drho, a.rho0);   // calc_cost.cu:81
-                wt[i] = warp_fetch(src, W, H, hx[p], hy[p], hz[p], h, rho);
+                wt[i] = warp_sample<QUAD>(src, hx[p], hy[p], hz[p], h, rho);
             }
             __syncthreads();
 
@@ -130,8 +188,8 @@ __global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
                     float tmp;
                     if constexpr (MODE == 0) {
                         const float rho = __fmaf_rn((float)(d0 + k), a.drho, a.rho0);
-                        const float B4 = warp_fetch(src, W, H, xr, yr, zr, h, rho);
-                        const float B8 = warp_fetch(src, W, H, xru, yru, zru, h, rho);
+                        const float B4 = warp_sample<QUAD>(src, xr, yr, zr, h, rho);
+                        const float B8 = warp_sample<QUAD>(src, xru, yru, zru, h, rho);
                         tmp = fabsf(__fsub_rn(Rc, W0));                    // 0  (:93)
                         tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rd, Wu)));    // 1  (:106)
                         tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Ru, Wd)));    // 2  (:119)
@@ -154,13 +212,15 @@ __global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
                         tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rru, Wru)));
                     }
                     if (tmp == tmp) {   // a rejected sample skips the voxel (calc_cost.cu:89-91)
-                        const float m = __fdiv_rn(tmp, 9.0f);
+                        const float m = div_small(tmp, 9.0f, r9);     // tmp / 9.0f
                         if (acc[k] < 0.0f) {                         // first measurement (:200-203)
                             acc[k] = m;
                             cn[k] = 1.0f;
                         } else {                                     // running mean (:205-206)
                             const float n1 = __fadd_rn(cn[k], 1.0f);
-                            acc[k] = __fdiv_rn(__fmaf_rn(cn[k], acc[k], m), n1);
+                            const float num = __fmaf_rn(cn[k], acc[k], m);
+                            const int ni = (int)n1;   // counts beyond the table (long running states)
+                            acc[k] = ni < MAXCNT ? div_small(num, n1, rtab[ni]) : __fdiv_rn(num, n1);
                             cn[k] = n1;
                         }
                     }
@@ -168,7 +228,7 @@ __global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
             }
         }
 
-        // transpose through shared memory and store 128-byte rows of the volume
+        // transpose through shared memory and store contiguous plane runs of the volume
         for (int pass = 0; pass < (a.cnt ? 2 : 1); ++pass) {
             __syncthreads();
 #pragma unroll
@@ -193,17 +253,23 @@ __global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
     if (a.invalid && inside) a.invalid[(size_t)v * W + u] = pix_invalid ? 1 : 0;
 }
 
+template <int MODE, bool HALF>
+void launch_q(const CostLaunch& a, dim3 grid, cudaStream_t s) {
+    if (a.srcq) cost_kernel<MODE, HALF, true><<<grid, NT, 0, s>>>(a);
+    else cost_kernel<MODE, HALF, false><<<grid, NT, 0, s>>>(a);
+}
+
 }  // namespace
 
 cudaError_t launch_cost(const CostLaunch& a, cudaStream_t s) {
+    if (a.nsrc > kMaxSources) return cudaErrorInvalidValue;
     const dim3 grid((a.W + TX - 1) / TX, (a.H + TY - 1) / TY);
-    const dim3 block(NT);
     if (a.mode == 0) {
-        if (a.cost_half) cost_kernel<0, true><<<grid, block, 0, s>>>(a);
-        else cost_kernel<0, false><<<grid, block, 0, s>>>(a);
+        if (a.cost_half) launch_q<0, true>(a, grid, s);
+        else launch_q<0, false>(a, grid, s);
     } else {
-        if (a.cost_half) cost_kernel<1, true><<<grid, block, 0, s>>>(a);
-        else cost_kernel<1, false><<<grid, block, 0, s>>>(a);
+        if (a.cost_half) launch_q<1, true>(a, grid, s);
+        else launch_q<1, false>(a, grid, s);
     }
     return cudaGetLastError();
 }

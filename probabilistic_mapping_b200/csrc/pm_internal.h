@@ -15,7 +15,8 @@ constexpr double kFloatEps = 1e-5;   // FLOAT_EPS (parameters.h:6)
 // ---- plane-sweep cost volume (calc_cost.cu) ----------------------------------------------
 struct CostLaunch {
     const float* ref;      // W*H scaled reference image
-    const float* srcs;     // nsrc consecutive W*H scaled source images
+    const float* srcs;     // nsrc consecutive W*H scaled source images (used when srcq is null)
+    const float4* srcq;    // nsrc consecutive W*H quad images (2x2 bilinear footprints)
     int W, H, D, nsrc;
     float rho0, drho;
     int mode;              // 0 reference quirks, 1 corrected 3x3 patch
@@ -44,19 +45,26 @@ struct SgmLaunch {
     const void* cost;      // W*H*D float or __half
     int cost_half;
     const float* ref;      // W*H scaled reference image (path gradient D1, sgm.cu:75)
-    float* sum;            // W*H*D partial sum of the paths
+    float* part[4];        // W*H*D partial sums of the four path groups
+    float* total;          // W*H*D complete sum (may alias part[0]); nullptr: not stored
     int W, H, D, num_paths;
     float p1, p2, tau, q1, q2;
     FilterParams fp;
     float* depth;          // W*H with byte pitch depth_pitch (fused filter only)
     size_t depth_pitch;
     int32_t* index;        // W*H (optional)
-    int store_sum_last;    // fused filter: also store the complete sum
     PlaneOrder order;
 };
-// Runs the num_paths direction passes in the reference order; with fuse_filter the last pass
-// completes the sum in registers and writes depth/index instead of the sum.
-cudaError_t launch_sgm(const SgmLaunch& a, bool fuse_filter, cudaStream_t s);
+// Side streams for the concurrent path groups: groups 0..2 fork from the caller's stream
+// and join back before the final pass.
+struct SgmStreams {
+    cudaStream_t stream[3];
+    cudaEvent_t fork;
+    cudaEvent_t join[3];
+};
+// Runs the path groups {g, g+4}; the final pass adds (S0 + S1) + (S2 + S3) in registers and,
+// with fuse_filter, writes depth/index.  side == nullptr runs every pass on s.
+cudaError_t launch_sgm(const SgmLaunch& a, bool fuse_filter, cudaStream_t s, const SgmStreams* side);
 cudaError_t launch_filter(const float* sum, int W, int H, int D, const FilterParams& fp,
                           const PlaneOrder& order, float* depth, size_t pitch, int32_t* index,
                           cudaStream_t s);
@@ -64,6 +72,10 @@ cudaError_t launch_filter(const float* sum, int W, int H, int D, const FilterPar
 // ---- image conversion (convert.cu + the uint8 -> float upload) ----------------------------
 cudaError_t launch_to_float(int W, int H, const uint8_t* src, size_t src_pitch, float* dst,
                             float scale, cudaStream_t s);
+// uint8 -> scaled quad image: dst[y*W + x] = (I(x,y), I(x+1,y), I(x,y+1), I(x+1,y+1)), zero
+// outside the image (the border addressing of the reference textures, calc_cost.cu:230-237).
+cudaError_t launch_to_quad(int W, int H, const uint8_t* src, size_t src_pitch, float4* dst,
+                           float scale, cudaStream_t s);
 cudaError_t launch_convert(int W, int H, const float* in, float* out, int flag, size_t pitch_bytes,
                            cudaStream_t s);
 

@@ -2,17 +2,20 @@
 // winner-take-all / flatness / subpixel filter (reference: filter_cost.cu:3-70).
 //
 // The reference runs one block per scanline with one thread per plane and finds the two
-// per-pixel minima with shared-memory tree reductions (~2 log2 D barriers per pixel step).
-// Here one WARP owns a scanline: lane l holds planes [l*PPL, (l+1)*PPL), the neighbour planes
-// d-1 / d+1 come from one shuffle each, and the minimum over planes is a single
-// redux.sync.min.f32.  The per-pixel plane vector (D floats, contiguous in the
-// plane-innermost layout) is streamed with cp.async into a per-lane shared-memory ring
-// PF steps ahead, so the sequential recurrence never waits on HBM.
-//
-// Directions are accumulated in the reference order (sgm.cu:119-133, then the diagonals),
-// so the FP32 sum is bit-identical to the reference's: the first pass stores, the middle
-// passes add, and with the fused filter the last pass keeps the complete sum in registers
-// and runs the winner-take-all directly.
+// per-pixel minima with shared-memory tree reductions (~2 log2 D barriers per pixel step),
+// one direction after the other.  Here:
+//   * one WARP owns a scanline: lane l holds planes [l*PPL, (l+1)*PPL), the neighbour planes
+//     d-1 / d+1 come from one shuffle each, and the minimum over planes is a single
+//     redux.sync.min.f32;
+//   * the per-pixel plane vector (contiguous in the plane-innermost layout) is streamed with
+//     cp.async into a per-lane shared-memory ring PF steps ahead of the recurrence;
+//   * the paths run as four concurrent groups {r, r+4} (an axis direction and a diagonal),
+//     each accumulating into its own partial-sum volume, so four times as many scanlines are
+//     in flight as in a one-direction-at-a-time schedule.  The last path of group 3 adds the
+//     four partials as (S0 + S1) + (S2 + S3) in registers and runs the winner-take-all
+//     directly, so the complete sum is never written.  The FP32 result therefore differs from
+//     the reference's sequential path order only by rounding; the CPU oracle replays this
+//     exact order.
 #include <climits>
 #include <vector>
 
@@ -72,6 +75,12 @@ __device__ __forceinline__ Chain chain_start(int c, int dx, int dy, int W, int H
     const int nx = dx > 0 ? W - x : (dx < 0 ? x + 1 : INT_MAX);
     const int ny = dy > 0 ? H - y : (dy < 0 ? y + 1 : INT_MAX);
     return {x, y, nx < ny ? nx : ny};
+}
+
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
 }
 
 // value of plane d (warp-uniform) from the lane that owns it
@@ -142,13 +151,27 @@ template <bool HALF> struct CostElem;
 template <> struct CostElem<false> { using T = float; };
 template <> struct CostElem<true> { using T = __half; };
 
-// MODE 0: first pass (store), 1: middle pass (add), 2: last pass (add + filter).
-template <int PPL, int MODE, bool HALF>
-__global__ void __launch_bounds__(WARPS * 32) sgm_dir_kernel(const SgmLaunch a, int dx, int dy) {
+enum { FIRST = 0, ACC = 1, FINAL = 2 };
+
+// Bytes one lane moves per pixel step, by pass kind: the cost slice, the partial sums it
+// reads (ACC: its own group's; FINAL: its own group's plus the three other groups'), and the
+// reference pixel for the path gradient.
+template <int PPL, int MODE, bool HALF> struct Slots {
+    static constexpr int CB = PPL * (int)sizeof(typename CostElem<HALF>::T);
+    static constexpr int SB = PPL * 4;
+    static constexpr int NS = MODE == FIRST ? 0 : (MODE == ACC ? 1 : 4);
+    static constexpr int LANE_B = CB + NS * SB + 4;
+    static constexpr int STAGE_B = 32 * LANE_B;
+};
+
+// One direction pass.  group: the partial-sum volume this pass accumulates into; own: in a
+// FINAL pass, whether the group already holds an earlier path (8-path mode).
+template <int PPL, int MODE, bool HALF, bool FILTER>
+__global__ void __launch_bounds__(WARPS * 32) sgm_dir_kernel(const SgmLaunch a, int dx, int dy, int group,
+                                                             int own) {
     using CT = typename CostElem<HALF>::T;
-    constexpr int CB = PPL * (int)sizeof(CT);         // cost bytes per lane per step
-    constexpr int SB = (MODE >= 1) ? PPL * 4 : 0;      // partial-sum bytes per lane per step
-    constexpr int LANE_B = CB + SB + 4;                // + reference pixel value
+    using SL = Slots<PPL, MODE, HALF>;
+    constexpr int CB = SL::CB, SB = SL::SB, NS = SL::NS, STAGE_B = SL::STAGE_B;
     extern __shared__ __align__(16) unsigned char ring[];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -157,54 +180,81 @@ __global__ void __launch_bounds__(WARPS * 32) sgm_dir_kernel(const SgmLaunch a, 
     if (c >= num_chains(dx, dy, W, H)) return;        // warp-uniform; no block barriers below
     const Chain ch = chain_start(c, dx, dy, W, H);
 
-    // slots: [warp][stage][part][lane] with parts laid out so each copy is naturally aligned
-    unsigned char* wbase = ring + (size_t)warp * PF * 32 * LANE_B;
-    auto slot_c = [&](int st) { return wbase + (size_t)st * 32 * LANE_B + lane * CB; };
-    auto slot_s = [&](int st) { return wbase + (size_t)st * 32 * LANE_B + 32 * CB + lane * SB; };
-    auto slot_i = [&](int st) { return wbase + (size_t)st * 32 * LANE_B + 32 * (CB + SB) + lane * 4; };
+    // Stage layout: [cost slices of 32 lanes][NS x partial slices of 32 lanes][32 ref values].
+    unsigned char* wbase = ring + (size_t)warp * PF * STAGE_B;
+    const int off_c = lane * CB;
+    const int off_s = 32 * CB + lane * SB;
+    const int off_i = 32 * (CB + NS * SB) + lane * 4;
 
+    // partial-sum sources: [0] = this group's (ACC, FINAL with own), FINAL adds groups 0..2
+    const float* src_s[4];
+    if constexpr (MODE == ACC) {
+        src_s[0] = a.part[group];
+    } else if constexpr (MODE == FINAL) {
+        src_s[0] = a.part[3];
+        src_s[1] = a.part[0];
+        src_s[2] = a.part[1];
+        src_s[3] = a.part[2];
+    }
     const CT* __restrict__ cost = reinterpret_cast<const CT*>(a.cost);
-    auto issue = [&](int k) {
-        if (k < ch.n) {
-            const int x = ch.x + k * dx, y = ch.y + k * dy;
-            const size_t pix = (size_t)y * W + x;
-            const int st = k % PF;
-            cp_async_bytes<CB>(slot_c(st), cost + pix * D + lane * PPL);
-            if constexpr (MODE >= 1) cp_async_bytes<SB>(slot_s(st), a.sum + pix * D + lane * PPL);
-            cp_async_4(slot_i(st), a.ref + pix);
+    const long pstep = (long)dy * W + dx;
+    long pix = (long)ch.y * W + ch.x;
+
+    auto issue = [&](unsigned char* sb, long q) {
+        const size_t e = (size_t)q * D + lane * PPL;
+        cp_async_bytes<CB>(sb + off_c, cost + e);
+#pragma unroll
+        for (int t = 0; t < NS; ++t) {
+            if (MODE == FINAL && t == 0 && !own) continue;
+            cp_async_bytes<SB>(sb + off_s + t * 32 * SB, src_s[t] + e);
         }
-        cp_async_commit();
+        cp_async_4(sb + off_i, a.ref + q);
     };
 #pragma unroll 1
-    for (int k = 0; k < PF; ++k) issue(k);
+    for (int k = 0; k < PF; ++k) {
+        if (k < ch.n) issue(wbase + k * STAGE_B, pix + k * pstep);
+        cp_async_commit();
+    }
 
     const uint32_t incl = a.order.incl[lane];
     uint16_t rk[PPL];
+    if constexpr (FILTER) {
 #pragma unroll
-    for (int j = 0; j < PPL; ++j) rk[j] = a.order.rank[lane * PPL + j];
+        for (int j = 0; j < PPL; ++j) rk[j] = a.order.rank[lane * PPL + j];
+    }
 
     float L[PPL];
 #pragma unroll
     for (int j = 0; j < PPL; ++j) L[j] = 0.0f;
     float mprev = 0.0f, Iprev = 0.0f;
+    int x = ch.x, y = ch.y, st = 0;
+    float* const dst = MODE == FINAL ? a.total : a.part[group];
 
 #pragma unroll 1
     for (int k = 0; k < ch.n; ++k) {
         cp_async_wait<PF - 1>();
-        const int st = k % PF;
+        unsigned char* sb = wbase + st * STAGE_B;
         float cv[PPL];
         if constexpr (HALF) {
-            const __half* hp = reinterpret_cast<const __half*>(slot_c(st));
+            const __half* hp = reinterpret_cast<const __half*>(sb + off_c);
 #pragma unroll
             for (int j = 0; j < PPL; ++j) cv[j] = __half2float(hp[j]);
         } else {
-            load_planes<PPL>(cv, reinterpret_cast<const float*>(slot_c(st)));
+            load_planes<PPL>(cv, reinterpret_cast<const float*>(sb + off_c));
         }
-        float sv[PPL];
-        if constexpr (MODE >= 1) load_planes<PPL>(sv, reinterpret_cast<const float*>(slot_s(st)));
-        const float I = *reinterpret_cast<const float*>(slot_i(st));
+        float sv[NS > 0 ? NS : 1][PPL];
+#pragma unroll
+        for (int t = 0; t < NS; ++t) {
+            if (MODE == FINAL && t == 0 && !own) {
+#pragma unroll
+                for (int j = 0; j < PPL; ++j) sv[t][j] = 0.0f;
+            } else {
+                load_planes<PPL>(sv[t], reinterpret_cast<const float*>(sb + off_s + t * 32 * SB));
+            }
+        }
+        const float I = *reinterpret_cast<const float*>(sb + off_i);
 
-        // any measured-never plane (cost -1) marks the pixel invalid (sgm.cu:33,67)
+        // a plane never measured (cost -1) marks the pixel invalid (sgm.cu:33,67)
         bool neg = false;
 #pragma unroll
         for (int j = 0; j < PPL; ++j) neg |= (((incl >> j) & 1u) && cv[j] < 0.0f);
@@ -224,15 +274,14 @@ __global__ void __launch_bounds__(WARPS * 32) sgm_dir_kernel(const SgmLaunch a, 
             float lp = __shfl_down_sync(kFull, L[0], 1);
             if (lane == 0) lm = inf_f();
             if (lane == 31) lp = inf_f();
+            // min(L[d], minL + P2, L[d-1] + P1, L[d+1] + P1) (sgm.cu:85-92); min(a+P1, b+P1) is
+            // min(a, b) + P1 exactly because rounding is monotonic
 #pragma unroll
             for (int j = 0; j < PPL; ++j) {
                 const float left = (j == 0) ? lm : L[j - 1];
                 const float right = (j == PPL - 1) ? lp : L[j + 1];
-                float vv = fminf(L[j], mP2);                       // (:85)
-                vv = fminf(vv, __fadd_rn(left, P1));                // (:88)
-                vv = fminf(vv, __fadd_rn(right, P1));               // (:92)
-                const float cd = inv ? 0.0f : cv[j];
-                Ln[j] = __fsub_rn(__fadd_rn(cd, vv), mprev);        // (:98)
+                const float vv = min3f(L[j], mP2, __fadd_rn(fminf(left, right), P1));
+                Ln[j] = __fsub_rn(__fadd_rn(inv ? 0.0f : cv[j], vv), mprev);   // (:98)
             }
         }
         Iprev = I;
@@ -244,20 +293,23 @@ __global__ void __launch_bounds__(WARPS * 32) sgm_dir_kernel(const SgmLaunch a, 
         }
         mprev = warp_min_f32(lmin);
 
-        const int x = ch.x + k * dx, y = ch.y + k * dy;
-        const size_t pix = (size_t)y * W + x;
         float o[PPL];
-        if constexpr (MODE == 0) {
+        if constexpr (MODE == FIRST) {
 #pragma unroll
             for (int j = 0; j < PPL; ++j) o[j] = inv ? 0.0f : Ln[j];
-            store_planes<PPL>(a.sum + pix * D + lane * PPL, o);
+            store_planes<PPL>(dst + (size_t)pix * D + lane * PPL, o);
+        } else if constexpr (MODE == ACC) {
+#pragma unroll
+            for (int j = 0; j < PPL; ++j) o[j] = inv ? 0.0f : __fadd_rn(sv[0][j], Ln[j]);   // (:101-108)
+            store_planes<PPL>(dst + (size_t)pix * D + lane * PPL, o);
         } else {
 #pragma unroll
-            for (int j = 0; j < PPL; ++j) o[j] = inv ? 0.0f : __fadd_rn(sv[j], Ln[j]);   // (:101-108)
-            if constexpr (MODE == 1) {
-                store_planes<PPL>(a.sum + pix * D + lane * PPL, o);
-            } else {
-                if (a.store_sum_last) store_planes<PPL>(a.sum + pix * D + lane * PPL, o);
+            for (int j = 0; j < PPL; ++j) {
+                const float t3 = __fadd_rn(sv[0][j], Ln[j]);
+                o[j] = inv ? 0.0f : __fadd_rn(__fadd_rn(sv[1][j], sv[2][j]), __fadd_rn(sv[3][j], t3));
+            }
+            if (dst) store_planes<PPL>(dst + (size_t)pix * D + lane * PPL, o);
+            if constexpr (FILTER) {
                 float depth;
                 int idx;
                 wta_filter<PPL>(o, incl, rk, lane, D, a.fp, depth, idx);
@@ -268,7 +320,13 @@ __global__ void __launch_bounds__(WARPS * 32) sgm_dir_kernel(const SgmLaunch a, 
                 }
             }
         }
-        issue(k + PF);   // slot k % PF has been consumed above
+        // refill this stage (consumed above) with step k + PF
+        if (k + PF < ch.n) issue(sb, pix + PF * pstep);
+        cp_async_commit();
+        pix += pstep;
+        x += dx;
+        y += dy;
+        st = (st + 1 == PF) ? 0 : st + 1;
     }
     cp_async_wait<0>();
 }
@@ -297,31 +355,50 @@ __global__ void __launch_bounds__(128) filter_kernel(const float* __restrict__ s
 
 const int kDirs[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1}, {-1, 1}, {1, -1}};
 
-template <int PPL, int MODE, bool HALF>
-cudaError_t launch_dir(const SgmLaunch& a, int dir, cudaStream_t s) {
-    using CT = typename CostElem<HALF>::T;
-    constexpr int LANE_B = PPL * (int)sizeof(CT) + ((MODE >= 1) ? PPL * 4 : 0) + 4;
-    const size_t smem = (size_t)WARPS * PF * 32 * LANE_B;
-    auto kern = sgm_dir_kernel<PPL, MODE, HALF>;
+template <int PPL, int MODE, bool HALF, bool FILTER>
+cudaError_t launch_dir(const SgmLaunch& a, int dir, int group, int own, cudaStream_t s) {
+    const size_t smem = (size_t)WARPS * PF * Slots<PPL, MODE, HALF>::STAGE_B;
+    auto kern = sgm_dir_kernel<PPL, MODE, HALF, FILTER>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     const int dx = kDirs[dir][0], dy = kDirs[dir][1];
     const int nch = num_chains(dx, dy, a.W, a.H);
-    kern<<<(nch + WARPS - 1) / WARPS, WARPS * 32, smem, s>>>(a, dx, dy);
+    kern<<<(nch + WARPS - 1) / WARPS, WARPS * 32, smem, s>>>(a, dx, dy, group, own);
     return cudaGetLastError();
 }
 
+// Groups g = 0..3 hold paths {g} (4-path mode) or {g, g+4} (8-path mode).  Groups 0..2 run on
+// their own streams when `side` is given; group 3 runs on `s` and its last path waits for them.
 template <int PPL, bool HALF>
-cudaError_t launch_sgm_t(const SgmLaunch& a, bool fuse_filter, cudaStream_t s) {
-    const int P = a.num_paths;
-    cudaError_t e = launch_dir<PPL, 0, HALF>(a, 0, s);
-    for (int r = 1; r < P && e == cudaSuccess; ++r) {
-        if (r == P - 1 && fuse_filter) e = launch_dir<PPL, 2, HALF>(a, r, s);
-        else e = launch_dir<PPL, 1, HALF>(a, r, s);
+cudaError_t launch_sgm_t(const SgmLaunch& a, bool fuse_filter, cudaStream_t s, const SgmStreams* side) {
+    const bool eight = a.num_paths == 8;
+    cudaError_t e = cudaSuccess;
+    auto group_passes = [&](int g, cudaStream_t gs) -> cudaError_t {
+        cudaError_t r = launch_dir<PPL, FIRST, HALF, false>(a, g, g, 0, gs);
+        if (r == cudaSuccess && eight) r = launch_dir<PPL, ACC, HALF, false>(a, g + 4, g, 0, gs);
+        return r;
+    };
+    if (side) {
+        if ((e = cudaEventRecord(side->fork, s)) != cudaSuccess) return e;
+        for (int g = 0; g < 3; ++g) {
+            if ((e = cudaStreamWaitEvent(side->stream[g], side->fork, 0)) != cudaSuccess) return e;
+            if ((e = group_passes(g, side->stream[g])) != cudaSuccess) return e;
+            if ((e = cudaEventRecord(side->join[g], side->stream[g])) != cudaSuccess) return e;
+        }
+    } else {
+        for (int g = 0; g < 3 && e == cudaSuccess; ++g) e = group_passes(g, s);
+        if (e != cudaSuccess) return e;
     }
-    return e;
+    // group 3: its first path (8-path mode), then the final path that combines all partials
+    if (eight && (e = launch_dir<PPL, FIRST, HALF, false>(a, 3, 3, 0, s)) != cudaSuccess) return e;
+    if (side)
+        for (int g = 0; g < 3; ++g)
+            if ((e = cudaStreamWaitEvent(s, side->join[g], 0)) != cudaSuccess) return e;
+    const int last = eight ? 7 : 3;
+    return fuse_filter ? launch_dir<PPL, FINAL, HALF, true>(a, last, 3, eight ? 1 : 0, s)
+                       : launch_dir<PPL, FINAL, HALF, false>(a, last, 3, eight ? 1 : 0, s);
 }
 
 template <int PPL>
@@ -335,19 +412,23 @@ cudaError_t launch_filter_t(const float* sum, int W, int H, int D, const FilterP
 
 }  // namespace
 
-cudaError_t launch_sgm(const SgmLaunch& a, bool fuse_filter, cudaStream_t s) {
+cudaError_t launch_sgm(const SgmLaunch& a, bool fuse_filter, cudaStream_t s, const SgmStreams* side) {
     const int ppl = a.D / 32;
     // FP16 volumes need an even number of planes per lane (4-byte cp.async pieces)
     if (a.cost_half && (ppl % 2)) return cudaErrorInvalidValue;
     switch (ppl) {
-        case 1: return launch_sgm_t<1, false>(a, fuse_filter, s);
-        case 2: return a.cost_half ? launch_sgm_t<2, true>(a, fuse_filter, s) : launch_sgm_t<2, false>(a, fuse_filter, s);
-        case 3: return launch_sgm_t<3, false>(a, fuse_filter, s);
-        case 4: return a.cost_half ? launch_sgm_t<4, true>(a, fuse_filter, s) : launch_sgm_t<4, false>(a, fuse_filter, s);
-        case 5: return launch_sgm_t<5, false>(a, fuse_filter, s);
-        case 6: return a.cost_half ? launch_sgm_t<6, true>(a, fuse_filter, s) : launch_sgm_t<6, false>(a, fuse_filter, s);
-        case 7: return launch_sgm_t<7, false>(a, fuse_filter, s);
-        case 8: return a.cost_half ? launch_sgm_t<8, true>(a, fuse_filter, s) : launch_sgm_t<8, false>(a, fuse_filter, s);
+        case 1: return launch_sgm_t<1, false>(a, fuse_filter, s, side);
+        case 2: return a.cost_half ? launch_sgm_t<2, true>(a, fuse_filter, s, side)
+                                   : launch_sgm_t<2, false>(a, fuse_filter, s, side);
+        case 3: return launch_sgm_t<3, false>(a, fuse_filter, s, side);
+        case 4: return a.cost_half ? launch_sgm_t<4, true>(a, fuse_filter, s, side)
+                                   : launch_sgm_t<4, false>(a, fuse_filter, s, side);
+        case 5: return launch_sgm_t<5, false>(a, fuse_filter, s, side);
+        case 6: return a.cost_half ? launch_sgm_t<6, true>(a, fuse_filter, s, side)
+                                   : launch_sgm_t<6, false>(a, fuse_filter, s, side);
+        case 7: return launch_sgm_t<7, false>(a, fuse_filter, s, side);
+        case 8: return a.cost_half ? launch_sgm_t<8, true>(a, fuse_filter, s, side)
+                                   : launch_sgm_t<8, false>(a, fuse_filter, s, side);
         default: return cudaErrorInvalidValue;
     }
 }

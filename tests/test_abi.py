@@ -65,7 +65,7 @@ def test_stage_calls_validate_arguments(pm_lib):
     from probabilistic_mapping_b200 import _lib
     c = _lib.default_config(64, 48, 64)
     null = ctypes.c_void_p(0)
-    assert pm_lib.pm_stage_sgm(ctypes.byref(c), null, null, null, null) == _lib.PM_ERR_INVALID_ARGUMENT
+    assert pm_lib.pm_stage_sgm(ctypes.byref(c), null, null, null, null, null) == _lib.PM_ERR_INVALID_ARGUMENT
     assert pm_lib.pm_stage_filter(ctypes.byref(c), null, null, 0, null, null) == _lib.PM_ERR_INVALID_ARGUMENT
     assert pm_lib.pm_stage_convert(64, 48, null, null, 1, 4, null) == _lib.PM_ERR_INVALID_ARGUMENT
     assert pm_lib.pm_stage_to_float(0, 48, null, 64, null, 1.0, null) == _lib.PM_ERR_INVALID_ARGUMENT

@@ -107,8 +107,9 @@ def test_sgm_and_filter_bit_exact(pm_lib, D, paths, compat, uniq):
     rf, _ = upload_images(pm_lib, fs, p.intensity_scale)
     dcost = torch.from_numpy(cost).cuda()
     out = torch.empty_like(dcost)
+    part = torch.empty((3,) + tuple(dcost.shape), dtype=torch.float32, device="cuda")
     cfg = config(p)
-    assert pm_lib.pm_stage_sgm(ctypes.byref(cfg), vp(dcost), vp(rf), vp(out), None) == 0
+    assert pm_lib.pm_stage_sgm(ctypes.byref(cfg), vp(dcost), vp(rf), vp(out), vp(part), None) == 0
     depth = torch.empty((p.H, p.W), dtype=torch.float32, device="cuda")
     idx = torch.empty((p.H, p.W), dtype=torch.int32, device="cuda")
     assert pm_lib.pm_stage_filter(ctypes.byref(cfg), vp(out), vp(depth), 4 * p.W, vp(idx), None) == 0
@@ -117,8 +118,13 @@ def test_sgm_and_filter_bit_exact(pm_lib, D, paths, compat, uniq):
     assert (bits(got) == bits(want_sum)).all(), np.abs(got - want_sum).max()
     assert (idx.cpu().numpy() == want_idx).all()
     assert (bits(depth.cpu().numpy()) == bits(want_depth)).all()
+    # the reference's sequential path order differs only by rounding
+    p.sum_order = 0
+    seq_sum = oracle.sgm(p, fs.ref, cost, "f32")
+    p.sum_order = 1
+    np.testing.assert_allclose(seq_sum, want_sum, rtol=2e-6, atol=1e-6)
     # fused last path + filter gives the same depth and index
-    scratch = torch.empty_like(dcost)
+    scratch = torch.empty((4,) + tuple(dcost.shape), dtype=torch.float32, device="cuda")
     depth2 = torch.zeros((p.H, p.W + 3), dtype=torch.float32, device="cuda")   # pitched output
     idx2 = torch.empty((p.H, p.W), dtype=torch.int32, device="cuda")
     assert pm_lib.pm_stage_sgm_filter(ctypes.byref(cfg), vp(dcost), vp(rf), vp(scratch), vp(depth2),
