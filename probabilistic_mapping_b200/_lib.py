@@ -67,6 +67,7 @@ SIGNATURES = {
     "pm_enable_stage_timing": (_I, [_VP, _I]),
     "pm_get_stage_times": (_I, [_VP, _P(ctypes.c_float), _I]),
     "pm_synchronize": (_I, [_VP]),
+    "pm_debug_check_arith": (_I, [_P(ctypes.c_uint64), _VP]),
     "pm_last_error": (ctypes.c_char_p, [_VP]),
     "pm_status_string": (ctypes.c_char_p, [_I]),
     "pm_stage_to_float": (_I, [_I, _I, _VP, _SZ, _VP, _F, _VP]),

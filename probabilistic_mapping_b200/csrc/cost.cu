@@ -3,22 +3,27 @@
 // The reference launches one thread per plane and walks D pixels per block, computing all
 // nine projective warps of the 3x3 patch for every voxel and every source frame, with a
 // read-modify-write of cost and count per call.  Here one CTA owns a 32x8 pixel tile and
-// all planes of it:
-//   * for a chunk of 16 planes and one source it warps the tile plus a one-pixel halo once
-//     (340 positions x 16 planes) into shared memory; the nine patch samples of each voxel
-//     are then read from that tile instead of being warped again (the two samples the
-//     reference computes from a corrupted neighbour, calc_cost.cu:50-51 and :70-71, are
-//     per-voxel and stay direct warps in reference mode);
+// all planes of it, and for every chunk of 16 planes and every source frame runs three
+// phases over shared memory:
+//   A  warp the tile plus a one-pixel halo once (340 positions x 16 planes); the nine patch
+//      samples of a voxel are read from this tile instead of being warped again;
+//   A2 (reference mode) the two samples the reference computes from a corrupted neighbour
+//      (calc_cost.cu:50-51 and :70-71) depend on the pixel itself, so each thread warps them
+//      for its own pixel and stores the two absolute differences;
+//   B  each thread sums the nine terms of its pixel in the reference's order and applies the
+//      running-mean update in registers.
+// All source frames queued since initReference are folded in one pass, so the volume is
+// written once.  Further choices:
 //   * source frames are stored as "quads": pixel (x, y) holds its 2x2 bilinear footprint
-//     (I(x,y), I(x+1,y), I(x,y+1), I(x+1,y+1)) with the texture border (zero) already applied,
-//     so every bilinear sample is one aligned 16-byte load;
-//   * all source frames queued since initReference are folded in one pass with the
-//     reference's running-mean update kept in registers, so the volume is written once; the
-//     two divisions of the update use a reciprocal-multiply with one FMA correction step
+//     (I(x,y), I(x+1,y), I(x,y+1), I(x+1,y+1)) with the texture border (zero) applied, so a
+//     bilinear sample is one aligned 16-byte load;
+//   * floor() for addressing adds 1.5 * 2^23 with round-toward-minus-infinity, which leaves
+//     the integer part in the mantissa, instead of float->int conversions;
+//   * the divisions of the running mean use a reciprocal-multiply with one FMA correction
 //     (Markstein), exhaustively checked to equal the correctly rounded quotient whenever the
-//     quotient is a normal number -- below that the code falls back to IEEE division;
-//   * the tile is transposed through shared memory so the volume is stored with contiguous
-//     plane runs in the plane-innermost layout (cuda_utils.h:34).
+//     quotient is a normal number; below that the code takes IEEE division;
+//   * the tile is transposed through shared memory so the volume is stored in contiguous
+//     plane runs of the plane-innermost layout (cuda_utils.h:34).
 // All FP32 arithmetic uses explicit round-to-nearest intrinsics (see pm_device.cuh).
 #include "pm_device.cuh"
 
@@ -36,7 +41,21 @@ constexpr int MAXCNT = kMaxSources + 2; // reciprocal table covers counts 0..kMa
 static_assert(NT * SP <= PC * NPOS, "staging must fit into the warp tile");
 static_assert(TX == 32 && NT == TX * TY, "one warp per tile row, one thread per pixel");
 static_assert((TX * PC) % 32 == 0, "the transposed block is moved in whole warp steps");
-static_assert(MAXCNT <= NT, "the reciprocal table is filled by one thread per entry");
+static_assert(MAXCNT <= NT && PC <= NT, "tables are filled by one thread per entry");
+
+// shared-memory layout (floats)
+template <int MODE> struct Smem {
+    static constexpr int WT = 0;                       // [PC][NPOS] warped samples
+    static constexpr int BUG = WT + PC * NPOS;         // [PC][2][NT] |R - B4|, |R - B8|
+    static constexpr int HXo = BUG + (MODE == 0 ? PC * 2 * NT : 0);
+    static constexpr int HYo = HXo + NPOS;
+    static constexpr int HZo = HYo + NPOS;
+    static constexpr int RHO = HZo + NPOS;             // [PC] plane inverse depths of the chunk
+    static constexpr int RTAB = RHO + PC;              // [MAXCNT] RN(1/n)
+    static constexpr int REF = RTAB + MAXCNT;          // [NPOS] reference image tile + halo
+    static constexpr int TOTAL = REF + NPOS;
+    static constexpr size_t BYTES = sizeof(float) * TOTAL;
+};
 
 __device__ __forceinline__ float ref_at(const float* __restrict__ ref, int W, int H, int x, int y) {
     return (x < 0 || y < 0 || x >= W || y >= H) ? 0.0f : __ldg(ref + (size_t)y * W + x);
@@ -56,10 +75,14 @@ template <bool QUAD> struct Src;
 template <> struct Src<true> {
     const float4* __restrict__ q;
     int W, H;
+    // 0 <= u <= W-1 and 0 <= v <= H-1 (< 2^22): floor by the 1.5 * 2^23 round-down add
     __device__ __forceinline__ float fetch(float u, float v) const {
-        const float fu = floorf(u), fv = floorf(v);
-        const float4 t = __ldg(q + (size_t)(int)fv * W + (int)fu);
+        float fu, fv;
+        int i, j;
+        floor_split(u, fu, i);
+        floor_split(v, fv, j);
         const float a = __fsub_rn(u, fu), b = __fsub_rn(v, fv);
+        const float4 t = __ldg(q + (size_t)j * W + i);
         const float top = __fmaf_rn(a, __fsub_rn(t.y, t.x), t.x);
         const float bot = __fmaf_rn(a, __fsub_rn(t.w, t.z), t.z);
         return __fmaf_rn(b, __fsub_rn(bot, top), top);
@@ -78,28 +101,34 @@ __device__ __forceinline__ float warp_sample(const Src<QUAD>& src, float x, floa
     const float w = __fmaf_rn(h.t3, rho, z);
     const float nx = __fmaf_rn(h.t1, rho, x);
     const float ny = __fmaf_rn(h.t2, rho, y);
-    const float r = __frcp_rn(w);
+    const float r = rcp_rn(w);
     const float u = __fmul_rn(nx, r), v = __fmul_rn(ny, r);
     const bool ok = (w >= 0.0f) && (u >= 0.0f) && (u <= (float)(src.W - 1)) && (v >= 0.0f) &&
                     (v <= (float)(src.H - 1));
     return ok ? src.fetch(u, v) : nan_f();
 }
 
-// Correctly rounded x / d for x >= 0 and an integer divisor d with r = RN(1/d): q0 = RN(x r),
-// then one Newton correction with the exact residual fma(-q0, d, x).  Exhaustively equal to
-// IEEE division for d in [2, 33] whenever x / d is normal; tiny x takes the IEEE path.
-__device__ __forceinline__ float div_small(float x, float d, float r) {
-    if (x != 0.0f && x < 1e-30f) return __fdiv_rn(x, d);
-    const float q0 = __fmul_rn(x, r);
-    return __fmaf_rn(__fmaf_rn(-q0, d, x), r, q0);
+__device__ __forceinline__ Hom load_hom(const CostLaunch& a, int s) {
+    Hom h;
+    h.r11 = a.hom[s][0]; h.r12 = a.hom[s][1]; h.r13 = a.hom[s][2];
+    h.r21 = a.hom[s][3]; h.r22 = a.hom[s][4]; h.r23 = a.hom[s][5];
+    h.r31 = a.hom[s][6]; h.r32 = a.hom[s][7]; h.r33 = a.hom[s][8];
+    h.t1 = a.hom[s][9]; h.t2 = a.hom[s][10]; h.t3 = a.hom[s][11];
+    return h;
 }
 
 // MODE 0: reference sample set (calc_cost.cu:83-199); MODE 1: corrected 3x3 patch.
 template <int MODE, bool HALF, bool QUAD>
-__global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
-    __shared__ __align__(16) float wt[PC * NPOS];   // warped source samples [plane][position]
-    __shared__ float hx[NPOS], hy[NPOS], hz[NPOS];  // homogeneous coordinates of the positions
-    __shared__ float rtab[MAXCNT];                  // RN(1/n)
+__global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
+    using SM = Smem<MODE>;
+    extern __shared__ __align__(16) float smem[];
+    float* const wt = smem + SM::WT;
+    float* const bug = smem + SM::BUG;
+    float* const hx = smem + SM::HXo;
+    float* const hy = smem + SM::HYo;
+    float* const hz = smem + SM::HZo;
+    float* const rho_s = smem + SM::RHO;
+    float* const rtab = smem + SM::RTAB;
 
     const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
@@ -108,18 +137,22 @@ __global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
     const bool inside = (u < W) && (v < H);
     if (tid < MAXCNT) rtab[tid] = tid == 0 ? 0.0f : __frcp_rn((float)tid);
 
-    // reference-image patch (border addressing -> 0, calc_cost.cu:230-231)
-    const float Rc = ref_at(a.ref, W, H, u, v), Ru = ref_at(a.ref, W, H, u, v - 1);
-    const float Rd = ref_at(a.ref, W, H, u, v + 1), Rl = ref_at(a.ref, W, H, u - 1, v);
-    const float Rr = ref_at(a.ref, W, H, u + 1, v), Rul = ref_at(a.ref, W, H, u - 1, v - 1);
-    const float Rdr = ref_at(a.ref, W, H, u + 1, v + 1), Rld = ref_at(a.ref, W, H, u - 1, v + 1);
-    const float Rru = ref_at(a.ref, W, H, u + 1, v - 1);
+    // reference-image tile with halo (border addressing -> 0, calc_cost.cu:230-231); read per
+    // phase from shared memory so it does not occupy registers across the phases
+    float* const rt = smem + SM::REF;
+    for (int p = tid; p < NPOS; p += NT) {
+        const int py = p / HX, px = p - py * HX;
+        rt[p] = ref_at(a.ref, W, H, x0 + px - 1, y0 + py - 1);
+    }
+    const float* const rc = rt + (ty + 1) * HX + (tx + 1);   // this pixel's centre
     const float r9 = __frcp_rn(9.0f);
 
     bool pix_invalid = false;
 
     for (int d0 = 0; d0 < D; d0 += PC) {
         float acc[PC], cn[PC];
+        __syncthreads();   // previous chunk's staging reads are done
+        if (tid < PC) rho_s[tid] = __fmaf_rn((float)(d0 + tid), a.drho, a.rho0);   // calc_cost.cu:81
         if (a.incremental) {
             // running state from memory, transposed through shared memory
             for (int pass = 0; pass < 2; ++pass) {
@@ -154,32 +187,43 @@ __global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
             else src.p = a.srcs + (size_t)s * W * H;
             src.W = W;
             src.H = H;
-            Hom h;
-            h.r11 = a.hom[s][0]; h.r12 = a.hom[s][1]; h.r13 = a.hom[s][2];
-            h.r21 = a.hom[s][3]; h.r22 = a.hom[s][4]; h.r23 = a.hom[s][5];
-            h.r31 = a.hom[s][6]; h.r32 = a.hom[s][7]; h.r33 = a.hom[s][8];
-            h.t1 = a.hom[s][9]; h.t2 = a.hom[s][10]; h.t3 = a.hom[s][11];
+            const Hom h = load_hom(a, s);
 
-            __syncthreads();   // previous consumers of wt / hx are done
+            __syncthreads();   // previous consumers of wt / hx / bug are done
             for (int p = tid; p < NPOS; p += NT) {
                 const int py = p / HX, px = p - py * HX;
                 homog(h, x0 + px - 1, y0 + py - 1, hx[p], hy[p], hz[p]);
             }
             __syncthreads();
+            // A: warped tile
+#pragma unroll 2
             for (int i = tid; i < PC * NPOS; i += NT) {
                 const int k = i / NPOS, p = i - k * NPOS;
-                const float rho = __fmaf_rn((float)(d0 + k), a.drho, a.rho0);   // calc_cost.cu:81
-                wt[i] = warp_sample<QUAD>(src, hx[p], hy[p], hz[p], h, rho);
+                wt[i] = warp_sample<QUAD>(src, hx[p], hy[p], hz[p], h, rho_s[k]);
+            }
+            // A2: per-pixel samples of the corrupted neighbours (calc_cost.cu:49-51, 69-71)
+            if (MODE == 0 && inside) {
+                float xc, yc, zc;
+                homog(h, u, v, xc, yc, zc);
+                const float xr = __fadd_rn(xc, h.r11), yr = __fadd_rn(xc, h.r21), zr = __fadd_rn(xc, h.r31);
+                const float xru = __fsub_rn(xr, h.r12), yru = __fsub_rn(xr, h.r22), zru = __fsub_rn(xr, h.r32);
+                const float Rr = rc[1], Rru = rc[1 - HX];
+#pragma unroll 2
+                for (int k = 0; k < PC; ++k) {
+                    const float rho = rho_s[k];
+                    const float B4 = warp_sample<QUAD>(src, xr, yr, zr, h, rho);
+                    const float B8 = warp_sample<QUAD>(src, xru, yru, zru, h, rho);
+                    bug[(2 * k) * NT + tid] = fabsf(__fsub_rn(Rr, B4));       // term 4 (:145)
+                    bug[(2 * k + 1) * NT + tid] = fabsf(__fsub_rn(Rru, B8));  // term 8 (:198)
+                }
             }
             __syncthreads();
 
+            // B: nine-term sum in the reference order and the running mean
             if (inside) {
-                float xc, yc, zc;
-                homog(h, u, v, xc, yc, zc);
-                // corrupted neighbours of the reference (calc_cost.cu:49-51, 69-71)
-                const float xr = __fadd_rn(xc, h.r11), yr = __fadd_rn(xc, h.r21), zr = __fadd_rn(xc, h.r31);
-                const float xru = __fsub_rn(xr, h.r12), yru = __fsub_rn(xr, h.r22), zru = __fsub_rn(xr, h.r32);
                 const float* wc = wt + (ty + 1) * HX + (tx + 1);
+                const float Rc = rc[0], Ru = rc[-HX], Rd = rc[HX], Rl = rc[-1], Rr = rc[1];
+                const float Rul = rc[-HX - 1], Rdr = rc[HX + 1], Rld = rc[HX - 1], Rru = rc[1 - HX];
 #pragma unroll
                 for (int k = 0; k < PC; ++k) {
                     const float* w = wc + k * NPOS;
@@ -187,18 +231,16 @@ __global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
                     const float Wul = w[-HX - 1], Wdr = w[HX + 1], Wld = w[HX - 1];
                     float tmp;
                     if constexpr (MODE == 0) {
-                        const float rho = __fmaf_rn((float)(d0 + k), a.drho, a.rho0);
-                        const float B4 = warp_sample<QUAD>(src, xr, yr, zr, h, rho);
-                        const float B8 = warp_sample<QUAD>(src, xru, yru, zru, h, rho);
+                        const float t4 = bug[(2 * k) * NT + tid], t8 = bug[(2 * k + 1) * NT + tid];
                         tmp = fabsf(__fsub_rn(Rc, W0));                    // 0  (:93)
                         tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rd, Wu)));    // 1  (:106)
                         tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Ru, Wd)));    // 2  (:119)
                         tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rl, Wl)));    // 3  (:132)
-                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rr, B4)));    // 4  (:145)
+                        tmp = __fadd_rn(tmp, t4);                          // 4  (:145)
                         tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rul, Wul)));  // 5  (:159)
                         tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rdr, Wdr)));  // 6  (:172)
                         tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rld, Wld)));  // 7  (:185)
-                        tmp = __fadd_rn(tmp, fabsf(__fsub_rn(Rru, B8)));   // 8  (:198)
+                        tmp = __fadd_rn(tmp, t8);                          // 8  (:198)
                     } else {
                         const float Wr = w[1], Wru = w[-HX + 1];
                         tmp = fabsf(__fsub_rn(Rc, W0));
@@ -253,10 +295,21 @@ __global__ void __launch_bounds__(NT, 2) cost_kernel(const CostLaunch a) {
     if (a.invalid && inside) a.invalid[(size_t)v * W + u] = pix_invalid ? 1 : 0;
 }
 
+template <int MODE, bool HALF, bool QUAD>
+cudaError_t launch_t(const CostLaunch& a, dim3 grid, cudaStream_t s) {
+    auto kern = cost_kernel<MODE, HALF, QUAD>;
+    constexpr size_t bytes = Smem<MODE>::BYTES;
+    if (bytes > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) return e;
+    }
+    kern<<<grid, NT, bytes, s>>>(a);
+    return cudaGetLastError();
+}
+
 template <int MODE, bool HALF>
-void launch_q(const CostLaunch& a, dim3 grid, cudaStream_t s) {
-    if (a.srcq) cost_kernel<MODE, HALF, true><<<grid, NT, 0, s>>>(a);
-    else cost_kernel<MODE, HALF, false><<<grid, NT, 0, s>>>(a);
+cudaError_t launch_q(const CostLaunch& a, dim3 grid, cudaStream_t s) {
+    return a.srcq ? launch_t<MODE, HALF, true>(a, grid, s) : launch_t<MODE, HALF, false>(a, grid, s);
 }
 
 }  // namespace
@@ -264,14 +317,8 @@ void launch_q(const CostLaunch& a, dim3 grid, cudaStream_t s) {
 cudaError_t launch_cost(const CostLaunch& a, cudaStream_t s) {
     if (a.nsrc > kMaxSources) return cudaErrorInvalidValue;
     const dim3 grid((a.W + TX - 1) / TX, (a.H + TY - 1) / TY);
-    if (a.mode == 0) {
-        if (a.cost_half) launch_q<0, true>(a, grid, s);
-        else launch_q<0, false>(a, grid, s);
-    } else {
-        if (a.cost_half) launch_q<1, true>(a, grid, s);
-        else launch_q<1, false>(a, grid, s);
-    }
-    return cudaGetLastError();
+    if (a.mode == 0) return a.cost_half ? launch_q<0, true>(a, grid, s) : launch_q<0, false>(a, grid, s);
+    return a.cost_half ? launch_q<1, true>(a, grid, s) : launch_q<1, false>(a, grid, s);
 }
 
 }  // namespace pm

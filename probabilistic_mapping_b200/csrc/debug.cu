@@ -1,0 +1,55 @@
+// debug.cu -- exhaustive self-check of the arithmetic shortcuts the FP32 kernels rely on for
+// bit-exactness with IEEE operations:
+//   [0] rcp_rn(w) == __frcp_rn(w)               for every positive finite float w
+//   [1] floor_split(u) == floorf(u)              for every float u in [0, 2^22)
+//   [2] div_small(x, d, RN(1/d)) == x / d (IEEE) for every non-negative finite float x and
+//       every integer divisor d in [2, 33]
+#include "pm_device.cuh"
+#include "pm_stereo.h"
+
+namespace pm {
+namespace {
+
+__global__ void __launch_bounds__(256) check_arith_kernel(uint32_t base, unsigned long long* bad) {
+    const uint32_t bits = base + blockIdx.x * blockDim.x + threadIdx.x;
+    if (bits >= 0x7f800000u) return;   // positive finite floats and zero only
+    const float x = __uint_as_float(bits);
+    unsigned long long nb[3] = {0, 0, 0};
+    if (bits != 0 && __float_as_uint(rcp_rn(x)) != __float_as_uint(__frcp_rn(x))) nb[0]++;
+    if (x < 4194304.0f) {
+        float fu;
+        int i;
+        floor_split(x, fu, i);
+        if (fu != floorf(x) || i != (int)floorf(x)) nb[1]++;
+    }
+    for (int d = 2; d <= 33; ++d) {
+        const float df = (float)d;
+        if (__float_as_uint(div_small(x, df, __frcp_rn(df))) != __float_as_uint(__fdiv_rn(x, df))) nb[2]++;
+    }
+    for (int k = 0; k < 3; ++k)
+        if (nb[k]) atomicAdd(bad + k, nb[k]);
+}
+
+}  // namespace
+}  // namespace pm
+
+extern "C" pm_status pm_debug_check_arith(uint64_t out[3], void* stream) {
+    if (!out) return PM_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned long long* bad = nullptr;
+    if (cudaMalloc(&bad, 3 * sizeof(unsigned long long)) != cudaSuccess) return PM_ERR_OUT_OF_MEMORY;
+    pm_status st = PM_OK;
+    if (cudaMemsetAsync(bad, 0, 3 * sizeof(unsigned long long), s) != cudaSuccess) st = PM_ERR_CUDA;
+    const uint32_t per = 1u << 26;
+    for (uint32_t base = 0; st == PM_OK && base < 0x80000000u; base += per) {
+        pm::check_arith_kernel<<<per / 256, 256, 0, s>>>(base, bad);
+        if (cudaGetLastError() != cudaSuccess) st = PM_ERR_CUDA;
+    }
+    unsigned long long host[3] = {0, 0, 0};
+    if (st == PM_OK && (cudaMemcpyAsync(host, bad, sizeof host, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                        cudaStreamSynchronize(s) != cudaSuccess))
+        st = PM_ERR_CUDA;
+    cudaFree(bad);
+    for (int k = 0; k < 3; ++k) out[k] = host[k];
+    return st;
+}

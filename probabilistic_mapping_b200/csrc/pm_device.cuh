@@ -25,6 +25,36 @@ struct Hom {
     float r11, r12, r13, r21, r22, r23, r31, r32, r33, t1, t2, t3;
 };
 
+// Correctly rounded 1/w.  For w in [2^-126, 2^126) one Newton-Raphson step from the hardware
+// reciprocal estimate (r1 = r0 + r0 (1 - w r0)) gives exactly RN(1/w); this was checked for
+// every float in that range against __frcp_rn (pm_debug_check_arith re-runs the check).
+// Outside that range the estimate flushes to zero or infinity, so IEEE reciprocal is used.
+__device__ __forceinline__ float rcp_rn(float w) {
+    if (w >= 1.17549435e-38f && w < 8.50705917e37f) {
+        float r0;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(w));
+        return __fmaf_rn(r0, __fmaf_rn(-w, r0, 1.0f), r0);
+    }
+    return __frcp_rn(w);
+}
+
+// floor(u) for 0 <= u < 2^22 as (float, int) without a conversion instruction: adding
+// 1.5 * 2^23 with rounding toward minus infinity leaves floor(u) in the low mantissa bits.
+__device__ __forceinline__ void floor_split(float u, float& fu, int& i) {
+    const float t = __fadd_rd(u, 12582912.0f);
+    i = __float_as_int(t) - 0x4B400000;
+    fu = __fsub_rn(t, 12582912.0f);
+}
+
+// Correctly rounded x / d for x >= 0 and an integer divisor d in [2, 33] with r = RN(1/d):
+// q0 = RN(x r), then one correction with the exact residual fma(-q0, d, x) (Markstein).  Equal
+// to IEEE division whenever x / d is a normal number; smaller x takes the IEEE path.
+__device__ __forceinline__ float div_small(float x, float d, float r) {
+    if (x != 0.0f && x < 1e-30f) return __fdiv_rn(x, d);
+    const float q0 = __fmul_rn(x, r);
+    return __fmaf_rn(__fmaf_rn(-q0, d, x), r, q0);
+}
+
 __device__ __forceinline__ void homog(const Hom& h, int qu, int qv, float& x, float& y, float& z) {
     const float fu = (float)qu, fv = (float)qv;
     x = __fmaf_rn(h.r11, fu, __fmaf_rn(h.r12, fv, h.r13));
@@ -59,7 +89,7 @@ __device__ __forceinline__ float warp_fetch(const float* __restrict__ img, int W
     const float w = __fmaf_rn(h.t3, rho, z);
     const float nx = __fmaf_rn(h.t1, rho, x);
     const float ny = __fmaf_rn(h.t2, rho, y);
-    const float r = __frcp_rn(w);
+    const float r = rcp_rn(w);
     const float u = __fmul_rn(nx, r), v = __fmul_rn(ny, r);
     const bool ok = (w >= 0.0f) && (u >= 0.0f) && (u <= (float)(W - 1)) && (v >= 0.0f) &&
                     (v <= (float)(H - 1));

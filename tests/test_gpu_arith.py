@@ -1,0 +1,14 @@
+"""The FP32 kernels replace three IEEE operations by cheaper sequences that must give the same
+bits (a Newton step from the hardware reciprocal, an add-based floor, a reciprocal-multiply
+division by a small integer).  This re-runs the exhaustive device-side comparison."""
+import ctypes
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_exact_arithmetic_shortcuts(pm_lib):
+    out = (ctypes.c_uint64 * 3)()
+    assert pm_lib.pm_debug_check_arith(out, None) == 0
+    assert list(out) == [0, 0, 0], f"mismatches: rcp={out[0]} floor={out[1]} div={out[2]}"
