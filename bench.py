@@ -110,12 +110,12 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
-def make_mapper(precision: int, device: int):
+def make_mapper(precision: int, device: int, cost_mode: int = 0):
     from probabilistic_mapping_b200 import scene
     from probabilistic_mapping_b200.mapper import StereoMapper
     rho0, drho = scene.plane_range(D)
     m = StereoMapper(W, H, D, rho0=rho0, intensity_scale=1 / 255, num_paths=PATHS, p1=P1, p2=P2, tau_so=TAU,
-                     uniqueness_ratio=UNIQ, cost_mode=0, precision=precision, device=device)
+                     uniqueness_ratio=UNIQ, cost_mode=cost_mode, precision=precision, device=device)
     return m, drho
 
 
@@ -139,7 +139,7 @@ def run_ours(args, rank, world):
     K = seq[0].K
     fx, fy, cx, cy = K[0, 0], K[1, 1], K[0, 2], K[1, 2]
     prec = 1 if args.precision == "fp16" else 0
-    m, drho = make_mapper(prec, dev)
+    m, drho = make_mapper(prec, dev, 1 if args.cost_mode == "corrected" else 0)
     m.initIntrinsic(K, 0.0, drho)
     stream = torch.cuda.Stream(device=dev)
     m.set_stream(stream.cuda_stream)
@@ -238,6 +238,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp32", "fp16"], default="fp32")
+    ap.add_argument("--cost-mode", choices=["reference", "corrected"], default="reference")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
@@ -287,7 +288,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": t_dev / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if e == 4 else "f16", "data": "synthetic",
             "config": {"workload": f"{W}x{H}, {D} planes, {S} sources, {PATHS}-path SGM, uniqueness {UNIQ}, "
-                                   f"fusion step; plain {args.precision} form, reference-compatible cost",
+                                   f"fusion step; {args.precision} form, {args.cost_mode} cost samples",
                        "global_batch": world, "seq_len": 0, "parallelism": f"replicas x{world}",
                        "l2": "per-map working set (cost + partial-sum volumes, 315 MB FP32) exceeds the 126 MB L2"},
             "roofline": {"bound": "hbm", "kernel": "sgm direction passes + fused winner-take-all",
