@@ -248,7 +248,7 @@ pm_status run_sgm_filter(pm_mapper* h) {
     a.cost = h->d_cost;
     a.ref = h->d_ref;
     for (int g = 0; g < 4; ++g) a.part[g] = h->d_part[g];
-    a.total = h->store_sgm ? h->d_part[0] : nullptr;   // the final pass reads part[0] before writing
+    a.total = h->store_sgm ? h->d_part[0] : nullptr;   // combine reads part[0] of a pixel before writing it
     a.depth = h->d_depth;
     a.depth_pitch = sizeof(float) * (size_t)c.width;
     a.index = h->d_idx;
@@ -692,7 +692,7 @@ pm_status pm_stage_sgm(const pm_config* cfg, const float* cost, const float* ref
     a.cost = cost;
     a.ref = ref;
     const size_t V = (size_t)cfg->width * cfg->height * cfg->num_planes;
-    a.part[0] = out;   // the final pass reads part[0] before it writes the total there
+    a.part[0] = out;   // the combine kernel reads part[0] of a pixel before it writes the total there
     for (int g = 1; g < 4; ++g) a.part[g] = scratch + (g - 1) * V;
     a.total = out;
     return launch_sgm(a, false, (cudaStream_t)stream, nullptr) == cudaSuccess ? PM_OK : PM_ERR_CUDA;

@@ -11,11 +11,11 @@
 //     cp.async into a per-lane shared-memory ring PF steps ahead of the recurrence;
 //   * the paths run as four concurrent groups {r, r+4} (an axis direction and a diagonal),
 //     each accumulating into its own partial-sum volume, so four times as many scanlines are
-//     in flight as in a one-direction-at-a-time schedule.  The last path of group 3 adds the
-//     four partials as (S0 + S1) + (S2 + S3) in registers and runs the winner-take-all
-//     directly, so the complete sum is never written.  The FP32 result therefore differs from
-//     the reference's sequential path order only by rounding; the CPU oracle replays this
-//     exact order.
+//     in flight as in a one-direction-at-a-time schedule;
+//   * a pixel-parallel combine kernel (one warp per pixel, full occupancy) adds the partials
+//     as (S0 + S1) + (S2 + S3) in registers and runs the winner-take-all directly, so the
+//     complete sum is never written.  The FP32 result therefore differs from the reference's
+//     sequential path order only by rounding; the CPU oracle replays this exact order.
 #include <climits>
 #include <vector>
 
@@ -151,27 +151,23 @@ template <bool HALF> struct CostElem;
 template <> struct CostElem<false> { using T = float; };
 template <> struct CostElem<true> { using T = __half; };
 
-enum { FIRST = 0, ACC = 1, FINAL = 2 };
+enum { FIRST = 0, ACC = 1 };
 
-// Bytes one lane moves per pixel step, by pass kind: the cost slice, the partial sums it
-// reads (ACC: its own group's; FINAL: its own group's plus the three other groups'), and the
+// Bytes one lane moves per pixel step: the cost slice, the group's partial sum (ACC), and the
 // reference pixel for the path gradient.
 template <int PPL, int MODE, bool HALF> struct Slots {
     static constexpr int CB = PPL * (int)sizeof(typename CostElem<HALF>::T);
-    static constexpr int SB = PPL * 4;
-    static constexpr int NS = MODE == FIRST ? 0 : (MODE == ACC ? 1 : 4);
-    static constexpr int LANE_B = CB + NS * SB + 4;
+    static constexpr int SB = MODE == ACC ? PPL * 4 : 0;
+    static constexpr int LANE_B = CB + SB + 4;
     static constexpr int STAGE_B = 32 * LANE_B;
 };
 
-// One direction pass.  group: the partial-sum volume this pass accumulates into; own: in a
-// FINAL pass, whether the group already holds an earlier path (8-path mode).
-template <int PPL, int MODE, bool HALF, bool FILTER>
-__global__ void __launch_bounds__(WARPS * 32) sgm_dir_kernel(const SgmLaunch a, int dx, int dy, int group,
-                                                             int own) {
+// One direction pass accumulating into the partial-sum volume of its group.
+template <int PPL, int MODE, bool HALF>
+__global__ void __launch_bounds__(WARPS * 32) sgm_dir_kernel(const SgmLaunch a, int dx, int dy, int group) {
     using CT = typename CostElem<HALF>::T;
     using SL = Slots<PPL, MODE, HALF>;
-    constexpr int CB = SL::CB, SB = SL::SB, NS = SL::NS, STAGE_B = SL::STAGE_B;
+    constexpr int CB = SL::CB, SB = SL::SB, STAGE_B = SL::STAGE_B;
     extern __shared__ __align__(16) unsigned char ring[];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -180,22 +176,13 @@ __global__ void __launch_bounds__(WARPS * 32) sgm_dir_kernel(const SgmLaunch a, 
     if (c >= num_chains(dx, dy, W, H)) return;        // warp-uniform; no block barriers below
     const Chain ch = chain_start(c, dx, dy, W, H);
 
-    // Stage layout: [cost slices of 32 lanes][NS x partial slices of 32 lanes][32 ref values].
+    // stage layout: [cost slices of 32 lanes][partial slices of 32 lanes][32 ref values]
     unsigned char* wbase = ring + (size_t)warp * PF * STAGE_B;
     const int off_c = lane * CB;
     const int off_s = 32 * CB + lane * SB;
-    const int off_i = 32 * (CB + NS * SB) + lane * 4;
+    const int off_i = 32 * (CB + SB) + lane * 4;
 
-    // partial-sum sources: [0] = this group's (ACC, FINAL with own), FINAL adds groups 0..2
-    const float* src_s[4];
-    if constexpr (MODE == ACC) {
-        src_s[0] = a.part[group];
-    } else if constexpr (MODE == FINAL) {
-        src_s[0] = a.part[3];
-        src_s[1] = a.part[0];
-        src_s[2] = a.part[1];
-        src_s[3] = a.part[2];
-    }
+    float* const part = a.part[group];
     const CT* __restrict__ cost = reinterpret_cast<const CT*>(a.cost);
     const long pstep = (long)dy * W + dx;
     long pix = (long)ch.y * W + ch.x;
@@ -203,11 +190,7 @@ __global__ void __launch_bounds__(WARPS * 32) sgm_dir_kernel(const SgmLaunch a, 
     auto issue = [&](unsigned char* sb, long q) {
         const size_t e = (size_t)q * D + lane * PPL;
         cp_async_bytes<CB>(sb + off_c, cost + e);
-#pragma unroll
-        for (int t = 0; t < NS; ++t) {
-            if (MODE == FINAL && t == 0 && !own) continue;
-            cp_async_bytes<SB>(sb + off_s + t * 32 * SB, src_s[t] + e);
-        }
+        if constexpr (MODE == ACC) cp_async_bytes<SB>(sb + off_s, part + e);
         cp_async_4(sb + off_i, a.ref + q);
     };
 #pragma unroll 1
@@ -217,18 +200,11 @@ __global__ void __launch_bounds__(WARPS * 32) sgm_dir_kernel(const SgmLaunch a, 
     }
 
     const uint32_t incl = a.order.incl[lane];
-    uint16_t rk[PPL];
-    if constexpr (FILTER) {
-#pragma unroll
-        for (int j = 0; j < PPL; ++j) rk[j] = a.order.rank[lane * PPL + j];
-    }
-
     float L[PPL];
 #pragma unroll
     for (int j = 0; j < PPL; ++j) L[j] = 0.0f;
     float mprev = 0.0f, Iprev = 0.0f;
-    int x = ch.x, y = ch.y, st = 0;
-    float* const dst = MODE == FINAL ? a.total : a.part[group];
+    int st = 0;
 
 #pragma unroll 1
     for (int k = 0; k < ch.n; ++k) {
@@ -242,16 +218,8 @@ __global__ void __launch_bounds__(WARPS * 32) sgm_dir_kernel(const SgmLaunch a, 
         } else {
             load_planes<PPL>(cv, reinterpret_cast<const float*>(sb + off_c));
         }
-        float sv[NS > 0 ? NS : 1][PPL];
-#pragma unroll
-        for (int t = 0; t < NS; ++t) {
-            if (MODE == FINAL && t == 0 && !own) {
-#pragma unroll
-                for (int j = 0; j < PPL; ++j) sv[t][j] = 0.0f;
-            } else {
-                load_planes<PPL>(sv[t], reinterpret_cast<const float*>(sb + off_s + t * 32 * SB));
-            }
-        }
+        float sv[PPL];
+        if constexpr (MODE == ACC) load_planes<PPL>(sv, reinterpret_cast<const float*>(sb + off_s));
         const float I = *reinterpret_cast<const float*>(sb + off_i);
 
         // a plane never measured (cost -1) marks the pixel invalid (sgm.cu:33,67)
@@ -293,42 +261,68 @@ __global__ void __launch_bounds__(WARPS * 32) sgm_dir_kernel(const SgmLaunch a, 
         }
         mprev = warp_min_f32(lmin);
 
+        // the output is set to COST_INF = 0 at an invalid pixel, else accumulated (:101-108)
         float o[PPL];
         if constexpr (MODE == FIRST) {
 #pragma unroll
             for (int j = 0; j < PPL; ++j) o[j] = inv ? 0.0f : Ln[j];
-            store_planes<PPL>(dst + (size_t)pix * D + lane * PPL, o);
-        } else if constexpr (MODE == ACC) {
-#pragma unroll
-            for (int j = 0; j < PPL; ++j) o[j] = inv ? 0.0f : __fadd_rn(sv[0][j], Ln[j]);   // (:101-108)
-            store_planes<PPL>(dst + (size_t)pix * D + lane * PPL, o);
         } else {
 #pragma unroll
-            for (int j = 0; j < PPL; ++j) {
-                const float t3 = __fadd_rn(sv[0][j], Ln[j]);
-                o[j] = inv ? 0.0f : __fadd_rn(__fadd_rn(sv[1][j], sv[2][j]), __fadd_rn(sv[3][j], t3));
-            }
-            if (dst) store_planes<PPL>(dst + (size_t)pix * D + lane * PPL, o);
-            if constexpr (FILTER) {
-                float depth;
-                int idx;
-                wta_filter<PPL>(o, incl, rk, lane, D, a.fp, depth, idx);
-                if (lane == 0) {
-                    *reinterpret_cast<float*>(reinterpret_cast<char*>(a.depth) + (size_t)y * a.depth_pitch +
-                                              (size_t)x * 4) = depth;
-                    if (a.index) a.index[pix] = idx;
-                }
-            }
+            for (int j = 0; j < PPL; ++j) o[j] = inv ? 0.0f : __fadd_rn(sv[j], Ln[j]);
         }
+        store_planes<PPL>(part + (size_t)pix * D + lane * PPL, o);
         // refill this stage (consumed above) with step k + PF
         if (k + PF < ch.n) issue(sb, pix + PF * pstep);
         cp_async_commit();
         pix += pstep;
-        x += dx;
-        y += dy;
         st = (st + 1 == PF) ? 0 : st + 1;
     }
     cp_async_wait<0>();
+}
+
+// Sum of the four group partials, (S0 + S1) + (S2 + S3), then (FILTER) the winner-take-all or
+// (!FILTER) a store of the sum.  One warp per pixel, grid-stride; the next pixel's partials are
+// loaded before the current one is reduced.
+template <int PPL, bool FILTER>
+__global__ void __launch_bounds__(256) combine_kernel(const SgmLaunch a) {
+    const int lane = threadIdx.x & 31;
+    const long nw = (long)gridDim.x * (blockDim.x >> 5);
+    const long npix = (long)a.W * a.H;
+    const int D = a.D;
+    const uint32_t incl = a.order.incl[lane];
+    uint16_t rk[PPL];
+#pragma unroll
+    for (int j = 0; j < PPL; ++j) rk[j] = a.order.rank[lane * PPL + j];
+    auto load4 = [&](long pix, float (&s)[4][PPL]) {
+        const size_t e = (size_t)pix * D + lane * PPL;
+#pragma unroll
+        for (int g = 0; g < 4; ++g) load_planes<PPL>(s[g], a.part[g] + e);
+    };
+    long pix = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    float cur[4][PPL], nxt[4][PPL];
+    if (pix < npix) load4(pix, cur);
+    for (; pix < npix; pix += nw) {
+        if (pix + nw < npix) load4(pix + nw, nxt);
+        float o[PPL];
+#pragma unroll
+        for (int j = 0; j < PPL; ++j) o[j] = __fadd_rn(__fadd_rn(cur[0][j], cur[1][j]), __fadd_rn(cur[2][j], cur[3][j]));
+        if (a.total) store_planes<PPL>(a.total + (size_t)pix * D + lane * PPL, o);
+        if constexpr (FILTER) {
+            float depth;
+            int idx;
+            wta_filter<PPL>(o, incl, rk, lane, D, a.fp, depth, idx);
+            if (lane == 0) {
+                const int y = (int)(pix / a.W), x = (int)(pix - (long)y * a.W);
+                *reinterpret_cast<float*>(reinterpret_cast<char*>(a.depth) + (size_t)y * a.depth_pitch +
+                                          (size_t)x * 4) = depth;
+                if (a.index) a.index[pix] = idx;
+            }
+        }
+#pragma unroll
+        for (int g = 0; g < 4; ++g)
+#pragma unroll
+            for (int j = 0; j < PPL; ++j) cur[g][j] = nxt[g][j];
+    }
 }
 
 template <int PPL>
@@ -355,29 +349,43 @@ __global__ void __launch_bounds__(128) filter_kernel(const float* __restrict__ s
 
 const int kDirs[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1}, {-1, 1}, {1, -1}};
 
-template <int PPL, int MODE, bool HALF, bool FILTER>
-cudaError_t launch_dir(const SgmLaunch& a, int dir, int group, int own, cudaStream_t s) {
+template <int PPL, int MODE, bool HALF>
+cudaError_t launch_dir(const SgmLaunch& a, int dir, int group, cudaStream_t s) {
     const size_t smem = (size_t)WARPS * PF * Slots<PPL, MODE, HALF>::STAGE_B;
-    auto kern = sgm_dir_kernel<PPL, MODE, HALF, FILTER>;
+    auto kern = sgm_dir_kernel<PPL, MODE, HALF>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     const int dx = kDirs[dir][0], dy = kDirs[dir][1];
     const int nch = num_chains(dx, dy, a.W, a.H);
-    kern<<<(nch + WARPS - 1) / WARPS, WARPS * 32, smem, s>>>(a, dx, dy, group, own);
+    kern<<<(nch + WARPS - 1) / WARPS, WARPS * 32, smem, s>>>(a, dx, dy, group);
+    return cudaGetLastError();
+}
+
+template <int PPL>
+cudaError_t launch_combine(const SgmLaunch& a, bool fuse_filter, cudaStream_t s) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long npix = (long)a.W * a.H;
+    const long blocks_needed = (npix + 7) / 8;   // 8 warps per block
+    const int blocks = (int)(blocks_needed < (long)sms * 8 ? blocks_needed : (long)sms * 8);
+    if (fuse_filter) combine_kernel<PPL, true><<<blocks, 256, 0, s>>>(a);
+    else combine_kernel<PPL, false><<<blocks, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 
 // Groups g = 0..3 hold paths {g} (4-path mode) or {g, g+4} (8-path mode).  Groups 0..2 run on
-// their own streams when `side` is given; group 3 runs on `s` and its last path waits for them.
+// their own streams when `side` is given; group 3 runs on `s`, which then joins the others and
+// runs the combine / winner-take-all kernel.
 template <int PPL, bool HALF>
 cudaError_t launch_sgm_t(const SgmLaunch& a, bool fuse_filter, cudaStream_t s, const SgmStreams* side) {
     const bool eight = a.num_paths == 8;
     cudaError_t e = cudaSuccess;
     auto group_passes = [&](int g, cudaStream_t gs) -> cudaError_t {
-        cudaError_t r = launch_dir<PPL, FIRST, HALF, false>(a, g, g, 0, gs);
-        if (r == cudaSuccess && eight) r = launch_dir<PPL, ACC, HALF, false>(a, g + 4, g, 0, gs);
+        cudaError_t r = launch_dir<PPL, FIRST, HALF>(a, g, g, gs);
+        if (r == cudaSuccess && eight) r = launch_dir<PPL, ACC, HALF>(a, g + 4, g, gs);
         return r;
     };
     if (side) {
@@ -391,14 +399,11 @@ cudaError_t launch_sgm_t(const SgmLaunch& a, bool fuse_filter, cudaStream_t s, c
         for (int g = 0; g < 3 && e == cudaSuccess; ++g) e = group_passes(g, s);
         if (e != cudaSuccess) return e;
     }
-    // group 3: its first path (8-path mode), then the final path that combines all partials
-    if (eight && (e = launch_dir<PPL, FIRST, HALF, false>(a, 3, 3, 0, s)) != cudaSuccess) return e;
+    if ((e = group_passes(3, s)) != cudaSuccess) return e;
     if (side)
         for (int g = 0; g < 3; ++g)
             if ((e = cudaStreamWaitEvent(s, side->join[g], 0)) != cudaSuccess) return e;
-    const int last = eight ? 7 : 3;
-    return fuse_filter ? launch_dir<PPL, FINAL, HALF, true>(a, last, 3, eight ? 1 : 0, s)
-                       : launch_dir<PPL, FINAL, HALF, false>(a, last, 3, eight ? 1 : 0, s);
+    return launch_combine<PPL>(a, fuse_filter, s);
 }
 
 template <int PPL>
