@@ -204,6 +204,18 @@ PM_API pm_status pm_stage_depth_fuse(int W, int H, const float pose[12], const f
                               float* depth, float* const pre[4], float* const cur[4],
                               uint64_t* ztable, int32_t* table, void* stream);
 
+/* pm_stage_depth_fuse without the ztable argument, for callers that must not allocate device
+ * memory at run time (a flight-control loop, a host framework that owns all device buffers,
+ * work recorded into a CUDA graph).  No counterpart in the reference.  The z-buffer is a
+ * library-owned __device__ array of 2^19 pixels (4 MiB, held by every GPU that loads the
+ * library until exit); W*H above that returns PM_ERR_INVALID_ARGUMENT.  The array is cleared
+ * at the start of each call and shared by all calls, so calls that overlap on the GPU race.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress);
+ * make that first call before any stream capture. */
+PM_API pm_status pm_stage_depth_fuse_noalloc(int W, int H, const float pose[12], const float cam[4],
+                                             float* depth, float* const pre[4], float* const cur[4],
+                                             int32_t* table, void* stream);
+
 /* convert (convert.cu:26-45).  flag != 0: linear -> pitched, else pitched -> linear.  The
  * pitch is in BYTES (the reference passed a byte step but indexed with it in floats). */
 PM_API pm_status pm_stage_convert(int W, int H, const float* in, float* out, int flag,

@@ -78,6 +78,8 @@ SIGNATURES = {
     "pm_stage_depth_fuse": (_I, [_I, _I, _P(ctypes.c_float), _P(ctypes.c_float), _VP, _P(_VP), _P(_VP),
                                  _VP, _VP, _VP]),
     "pm_stage_convert": (_I, [_I, _I, _VP, _VP, _I, _SZ, _VP]),
+    "pm_stage_depth_fuse_noalloc": (_I, [_I, _I, _P(ctypes.c_float), _P(ctypes.c_float), _VP, _P(_VP),
+                                         _P(_VP), _VP, _VP]),
 }
 
 _lib = None
