@@ -392,12 +392,14 @@ void fuse_gpu(int W, int H, const float pose[12], const float cam[4], S* depth, 
             const S px = ((S)x - cx) / fx * dep;                     // (:34)
             const S py = ((S)y - cy) / fy * dep;
             const S pz = dep;
-            const S px2 = fmaT(r11, px, fmaT(r12, py, fmaT(r13, pz, t1)));
-            const S py2 = fmaT(r21, px, fmaT(r22, py, fmaT(r23, pz, t2)));
-            const S pz2 = fmaT(r31, px, fmaT(r32, py, fmaT(r33, pz, t3)));
+            // r11*px+r12*py+r13*pz + t1 (:37-39) with the multiply-add contraction the reference's
+            // nvcc build performs (matched against its outputs, tests/golden/)
+            const S px2 = fmaT(r13, pz, fmaT(r12, py, r11 * px)) + t1;
+            const S py2 = fmaT(r23, pz, fmaT(r22, py, r21 * px)) + t2;
+            const S pz2 = fmaT(r33, pz, fmaT(r32, py, r31 * px)) + t3;
             if ((double)pz2 < kFloatEps) continue;                  // (:40)
-            const int x2 = (int)((double)(px2 / pz2 * fx + cx) + 0.5);   // (:43), truncation
-            const int y2 = (int)((double)(py2 / pz2 * fy + cy) + 0.5);
+            const int x2 = (int)((double)fmaT(px2 / pz2, fx, cx) + 0.5);   // (:43), truncation
+            const int y2 = (int)((double)fmaT(py2 / pz2, fy, cy) + 0.5);
             if (x2 < 0 || x2 >= W || y2 < 0 || y2 >= H) continue;
             pm[index] = pz2;                                         // (:48)
             ps[index] = (S)((double)ps[index] + (double)pz2 * 0.05); // (:49)
@@ -408,14 +410,16 @@ void fuse_gpu(int W, int H, const float pose[12], const float cam[4], S* depth, 
                 bestd[cell] = pz2;
             }
         }
-    // hole_filling (:80-105): empty cells take the first occupied interior neighbour
+    // hole_filling (:80-105): empty cells take the last occupied interior neighbour in raster
+    // order -- the writer whose own 3x3 loop (:96-103) reaches the cell first, which is the
+    // outcome when the writers run in lockstep
     std::vector<int32_t> filled(table);
     for (int y = 0; y < H; ++y)
         for (int x = 0; x < W; ++x) {
             const int e = y * W + x;
             if (table[e] != 0) continue;
-            for (int i = -1; i <= 1 && filled[e] == 0; ++i)
-                for (int j = -1; j <= 1; ++j) {
+            for (int i = 1; i >= -1 && filled[e] == 0; --i)
+                for (int j = 1; j >= -1; --j) {
                     const int ny = y + i, nx = x + j;
                     if (nx <= 0 || nx >= W - 1 || ny <= 0 || ny >= H - 1) continue;
                     const int t = table[ny * W + nx];
@@ -451,17 +455,19 @@ void fuse_gpu(int W, int H, const float pose[12], const float cam[4], S* depth, 
         }
         const S a = ca[e], b = cb[e], miu = cm[e], sq = cs[e];
         const S new_sq = unc * sq / (unc + sq);                               // (:195)
-        const S new_miu = fmaT(d, sq, miu * unc) / (unc + sq);                // (:196)
+        const S new_miu = fmaT(miu, unc, d * sq) / (unc + sq);                // (:196)
         S c1 = (a / (a + b)) * normpdf(d, miu, unc + sq);                     // (:197)
         S c2 = (b / (a + b)) * (S)1 / (S)50;                                  // (:198)
         const S norm = c1 + c2;
         c1 = c1 / norm;
         c2 = c2 / norm;
-        const S f = c1 * ((a + (S)1) / (a + b + (S)1)) + c2 * (a / (a + b + (S)1));
-        const S ee = c1 * (((a + (S)1) * (a + (S)2)) / ((a + b + (S)1) * (a + b + (S)2))) +
-                     c2 * (a * (a + (S)1) / ((a + b + (S)1) * (a + b + (S)2)));
-        const S mu_p = c1 * new_miu + c2 * miu;
-        const S sig_p = c1 * (new_sq + new_miu * new_miu) + c2 * (sq + miu * miu) - mu_p * mu_p;
+        // u*v + x*y contracts to fma(u, v, x*y) and X - u*v to fma(-u, v, X), as in the
+        // reference's nvcc build
+        const S f = fmaT(c1, (a + (S)1) / (a + b + (S)1), c2 * (a / (a + b + (S)1)));
+        const S ee = fmaT(c1, ((a + (S)1) * (a + (S)2)) / ((a + b + (S)1) * (a + b + (S)2)),
+                          c2 * (a * (a + (S)1) / ((a + b + (S)1) * (a + b + (S)2))));
+        const S mu_p = fmaT(c1, new_miu, c2 * miu);
+        const S sig_p = fmaT(-mu_p, mu_p, fmaT(c1, fmaT(new_miu, new_miu, new_sq), c2 * fmaT(miu, miu, sq)));
         const S a_p = (ee - f) / (f - ee / f);
         const S b_p = a_p * ((S)1 - f) / f;
         ca[e] = a_p; cb[e] = b_p; cm[e] = mu_p; cs[e] = sig_p;

@@ -12,9 +12,12 @@
  *   *_f32  -- the same algorithm in FP32 with the op order of the B200 kernels, so that
  *             the GPU result can be compared bit-for-bit.
  *
- * Parity status: pinned against the reference's own CUDA where oracle/_ref was built and
- * run (tests/golden/ref_*.npz, generated by tests/golden/make_ref_golden.py); otherwise the
- * restatement is checked only by analytic known-answer tests.
+ * Parity status: pinned against the reference's own CUDA (built unmodified through
+ * oracle/ref_shim.h, run on a B200; outputs in tests/golden/ref_40x32x32.npz, generated by
+ * tests/golden/make_ref_golden.py, checked by tests/test_golden.py): SGM, filter and convert
+ * bit-exact, cost counts/validity exact and values within the texture-unit bilinear rounding,
+ * fusion transform and z-buffer exact.  The CPU fusion variant (host C++ needing OpenCV and
+ * Eigen) is checked by analytic known-answer tests only.
  *
  * Layouts: images are W*H row-major uint8; cost volumes are plane-innermost
  * ((y*W + x)*D + d), as INDEX() in motion_stereo/cuda_utils.h:34.

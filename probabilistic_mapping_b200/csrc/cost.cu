@@ -108,6 +108,57 @@ __device__ __forceinline__ float warp_sample(const Src<QUAD>& src, float x, floa
     return ok ? src.fetch(u, v) : nan_f();
 }
 
+// ---- two samples at once on the packed FP32x2 pipe ----------------------------------------
+// Each element follows exactly the scalar operation sequence above (every packed instruction
+// rounds each element like its scalar counterpart), so the results are bit-identical; the pair
+// only halves the instruction count.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
+__device__ __forceinline__ float2 rcp_rn2(float2 w) {
+    const bool in0 = w.x >= 1.17549435e-38f && w.x < 8.50705917e37f;
+    const bool in1 = w.y >= 1.17549435e-38f && w.y < 8.50705917e37f;
+    if (in0 && in1) {
+        float2 r0;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0.x) : "f"(w.x));
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0.y) : "f"(w.y));
+        return __ffma2_rn(r0, __ffma2_rn(neg2(w), r0, f2(1.0f, 1.0f)), r0);
+    }
+    return f2(rcp_rn(w.x), rcp_rn(w.y));
+}
+
+// bilinear from the quad layout for two in-range sample positions
+__device__ __forceinline__ float2 fetch2(const float4* __restrict__ q, int W, float2 u, float2 v) {
+    const float2 M = f2(12582912.0f, 12582912.0f);
+    const float2 tu = __fadd2_rd(u, M), tv = __fadd2_rd(v, M);
+    const int i0 = __float_as_int(tu.x) - 0x4B400000, i1 = __float_as_int(tu.y) - 0x4B400000;
+    const int j0 = __float_as_int(tv.x) - 0x4B400000, j1 = __float_as_int(tv.y) - 0x4B400000;
+    const float2 a = __fadd2_rn(u, neg2(__fadd2_rn(tu, neg2(M))));   // u - floor(u)
+    const float2 b = __fadd2_rn(v, neg2(__fadd2_rn(tv, neg2(M))));
+    const float4 t0 = __ldg(q + (size_t)j0 * W + i0);
+    const float4 t1 = __ldg(q + (size_t)j1 * W + i1);
+    // (top, bot) of each sample as one pair: fma(a, (t.y - t.x, t.w - t.z), (t.x, t.z))
+    const float2 tb0 = __ffma2_rn(f2(a.x, a.x), __fadd2_rn(f2(t0.y, t0.w), neg2(f2(t0.x, t0.z))), f2(t0.x, t0.z));
+    const float2 tb1 = __ffma2_rn(f2(a.y, a.y), __fadd2_rn(f2(t1.y, t1.w), neg2(f2(t1.x, t1.z))), f2(t1.x, t1.z));
+    return __ffma2_rn(b, __fadd2_rn(f2(tb0.y, tb1.y), neg2(f2(tb0.x, tb1.x))), f2(tb0.x, tb1.x));
+}
+
+// warp_sample for two (x, y, z, rho) at once; a rejected element is NaN.
+__device__ __forceinline__ float2 warp_sample2(const Src<true>& src, float2 x, float2 y, float2 z, const Hom& h,
+                                               float2 rho) {
+    const float2 w = __ffma2_rn(f2(h.t3, h.t3), rho, z);
+    const float2 nx = __ffma2_rn(f2(h.t1, h.t1), rho, x);
+    const float2 ny = __ffma2_rn(f2(h.t2, h.t2), rho, y);
+    const float2 r = rcp_rn2(w);
+    const float2 u = __fmul2_rn(nx, r), v = __fmul2_rn(ny, r);
+    const float W1 = (float)(src.W - 1), H1 = (float)(src.H - 1);
+    const bool ok0 = (w.x >= 0.0f) && (u.x >= 0.0f) && (u.x <= W1) && (v.x >= 0.0f) && (v.x <= H1);
+    const bool ok1 = (w.y >= 0.0f) && (u.y >= 0.0f) && (u.y <= W1) && (v.y >= 0.0f) && (v.y <= H1);
+    // positions of rejected elements are replaced by 0 so the fetch stays inside the image
+    const float2 s = fetch2(src.q, src.W, f2(ok0 ? u.x : 0.0f, ok1 ? u.y : 0.0f), f2(ok0 ? v.x : 0.0f, ok1 ? v.y : 0.0f));
+    return f2(ok0 ? s.x : nan_f(), ok1 ? s.y : nan_f());
+}
+
 __device__ __forceinline__ Hom load_hom(const CostLaunch& a, int s) {
     Hom h;
     h.r11 = a.hom[s][0]; h.r12 = a.hom[s][1]; h.r13 = a.hom[s][2];
@@ -195,11 +246,24 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
                 homog(h, x0 + px - 1, y0 + py - 1, hx[p], hy[p], hz[p]);
             }
             __syncthreads();
-            // A: warped tile
+            // A: warped tile (quad sources: planes k and k + PC/2 of a position as one pair)
+            if constexpr (QUAD) {
+                constexpr int HALF_PC = PC / 2;
 #pragma unroll 2
-            for (int i = tid; i < PC * NPOS; i += NT) {
-                const int k = i / NPOS, p = i - k * NPOS;
-                wt[i] = warp_sample<QUAD>(src, hx[p], hy[p], hz[p], h, rho_s[k]);
+                for (int i = tid; i < HALF_PC * NPOS; i += NT) {
+                    const int k = i / NPOS, p = i - k * NPOS;
+                    const float x = hx[p], y = hy[p], z = hz[p];
+                    const float2 s2 = warp_sample2(src, f2(x, x), f2(y, y), f2(z, z), h,
+                                                   f2(rho_s[k], rho_s[k + HALF_PC]));
+                    wt[i] = s2.x;
+                    wt[i + HALF_PC * NPOS] = s2.y;
+                }
+            } else {
+#pragma unroll 2
+                for (int i = tid; i < PC * NPOS; i += NT) {
+                    const int k = i / NPOS, p = i - k * NPOS;
+                    wt[i] = warp_sample<QUAD>(src, hx[p], hy[p], hz[p], h, rho_s[k]);
+                }
             }
             // A2: per-pixel samples of the corrupted neighbours (calc_cost.cu:49-51, 69-71)
             if (MODE == 0 && inside) {
@@ -211,8 +275,15 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
 #pragma unroll 2
                 for (int k = 0; k < PC; ++k) {
                     const float rho = rho_s[k];
-                    const float B4 = warp_sample<QUAD>(src, xr, yr, zr, h, rho);
-                    const float B8 = warp_sample<QUAD>(src, xru, yru, zru, h, rho);
+                    float B4, B8;
+                    if constexpr (QUAD) {
+                        const float2 b = warp_sample2(src, f2(xr, xru), f2(yr, yru), f2(zr, zru), h, f2(rho, rho));
+                        B4 = b.x;
+                        B8 = b.y;
+                    } else {
+                        B4 = warp_sample<QUAD>(src, xr, yr, zr, h, rho);
+                        B8 = warp_sample<QUAD>(src, xru, yru, zru, h, rho);
+                    }
                     bug[(2 * k) * NT + tid] = fabsf(__fsub_rn(Rr, B4));       // term 4 (:145)
                     bug[(2 * k + 1) * NT + tid] = fabsf(__fsub_rn(Rru, B8));  // term 8 (:198)
                 }

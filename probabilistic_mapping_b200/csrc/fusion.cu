@@ -7,7 +7,7 @@
 //     z-test with one 64-bit atomicMin on (depth bits << 32 | pixel index): the nearest
 //     surface wins and ties go to the smaller index, independent of scheduling;
 //   * fuse_update_kernel fuses hole filling (a gather over the 3x3 neighbourhood of the
-//     unfilled table: the first occupied interior neighbour in raster order), the state
+//     unfilled table: the last occupied interior neighbour in raster order), the state
 //     prediction and the Bayesian update, reading each previous-state entry once.
 // Both rules are one legal outcome of the reference's races.  The double-precision
 // promotions of the reference expressions (0.4, 0.6, 0.05, 0.01 and M_PI literals) are kept.
@@ -34,12 +34,14 @@ __global__ void __launch_bounds__(256) fuse_transform_kernel(const FuseLaunch a)
     const float py = __fmul_rn(__fdiv_rn(__fsub_rn((float)y, cy), fy), dep);
     const float pz = dep;
     const float* p = a.pose;
-    const float px2 = __fmaf_rn(p[0], px, __fmaf_rn(p[1], py, __fmaf_rn(p[2], pz, p[9])));
-    const float py2 = __fmaf_rn(p[3], px, __fmaf_rn(p[4], py, __fmaf_rn(p[5], pz, p[10])));
-    const float pz2 = __fmaf_rn(p[6], px, __fmaf_rn(p[7], py, __fmaf_rn(p[8], pz, p[11])));
+    // r11*px+r12*py+r13*pz + t1 (:37-39) with the multiply-add contraction of the reference's
+    // nvcc build, so the transformed depth and the target pixel agree with it bit for bit
+    const float px2 = __fadd_rn(__fmaf_rn(p[2], pz, __fmaf_rn(p[1], py, __fmul_rn(p[0], px))), p[9]);
+    const float py2 = __fadd_rn(__fmaf_rn(p[5], pz, __fmaf_rn(p[4], py, __fmul_rn(p[3], px))), p[10]);
+    const float pz2 = __fadd_rn(__fmaf_rn(p[8], pz, __fmaf_rn(p[7], py, __fmul_rn(p[6], px))), p[11]);
     if ((double)pz2 < kFloatEps) return;                                   // (:40)
-    const int x2 = __double2int_rz(__dadd_rn((double)__fadd_rn(__fmul_rn(__fdiv_rn(px2, pz2), fx), cx), 0.5));
-    const int y2 = __double2int_rz(__dadd_rn((double)__fadd_rn(__fmul_rn(__fdiv_rn(py2, pz2), fy), cy), 0.5));
+    const int x2 = __double2int_rz(__dadd_rn((double)__fmaf_rn(__fdiv_rn(px2, pz2), fx, cx), 0.5));   // (:43)
+    const int y2 = __double2int_rz(__dadd_rn((double)__fmaf_rn(__fdiv_rn(py2, pz2), fy, cy), 0.5));
     if (x2 < 0 || x2 >= W || y2 < 0 || y2 >= H) return;
     a.pre[2][index] = pz2;                                                 // (:48)
     a.pre[3][index] = __double2float_rn(__dadd_rn((double)a.pre[3][index], __dmul_rn((double)pz2, 0.05)));
@@ -61,12 +63,13 @@ __global__ void __launch_bounds__(256) fuse_update_kernel(const FuseLaunch a) {
     if (x >= W || y >= H) return;
     const int e = y * W + x;
 
-    // hole filling (:80-105): an empty cell takes the first occupied interior neighbour
+    // hole filling (:80-105): an empty cell takes the last occupied interior neighbour in
+    // raster order, the writer whose own 3x3 loop (:96-103) reaches it first
     const unsigned long long k0 = a.ztable[e];
     int t = k0 == kEmpty ? 0 : (int)(unsigned)(k0 & 0xffffffffu);
     if (t == 0) {
-        for (int i = -1; i <= 1 && t == 0; ++i)
-            for (int j = -1; j <= 1; ++j) {
+        for (int i = 1; i >= -1 && t == 0; --i)
+            for (int j = 1; j >= -1; --j) {
                 const int ny = y + i, nx = x + j;
                 if (nx <= 0 || nx >= W - 1 || ny <= 0 || ny >= H - 1) continue;
                 const unsigned long long kk = a.ztable[ny * W + nx];
@@ -101,7 +104,7 @@ __global__ void __launch_bounds__(256) fuse_update_kernel(const FuseLaunch a) {
         const float aa = ca, bb = cb, miu = cm, sq = cs;
         const float us = __fadd_rn(unc, sq);
         const float new_sq = __fdiv_rn(__fmul_rn(unc, sq), us);                           // (:195)
-        const float new_miu = __fdiv_rn(__fmaf_rn(d, sq, __fmul_rn(miu, unc)), us);       // (:196)
+        const float new_miu = __fdiv_rn(__fmaf_rn(miu, unc, __fmul_rn(d, sq)), us);       // (:196)
         const float ab = __fadd_rn(aa, bb);
         float c1 = __fmul_rn(__fdiv_rn(aa, ab), normpdf(d, miu, us));                     // (:197)
         float c2 = __fdiv_rn(__fmul_rn(__fdiv_rn(bb, ab), 1.0f), 50.0f);                  // (:198)
@@ -110,14 +113,16 @@ __global__ void __launch_bounds__(256) fuse_update_kernel(const FuseLaunch a) {
         c2 = __fdiv_rn(c2, norm);
         const float a1 = __fadd_rn(aa, 1.0f), a2 = __fadd_rn(aa, 2.0f);
         const float ab1 = __fadd_rn(ab, 1.0f), ab2 = __fadd_rn(ab, 2.0f);
-        const float f = __fadd_rn(__fmul_rn(c1, __fdiv_rn(a1, ab1)), __fmul_rn(c2, __fdiv_rn(aa, ab1)));
+        // u*v + x*y -> fma(u, v, x*y) and X - u*v -> fma(-u, v, X): the contraction of the
+        // reference's nvcc build (:203-208)
+        const float f = __fmaf_rn(c1, __fdiv_rn(a1, ab1), __fmul_rn(c2, __fdiv_rn(aa, ab1)));
         const float den = __fmul_rn(ab1, ab2);
-        const float ee = __fadd_rn(__fmul_rn(c1, __fdiv_rn(__fmul_rn(a1, a2), den)),
+        const float ee = __fmaf_rn(c1, __fdiv_rn(__fmul_rn(a1, a2), den),
                                    __fmul_rn(c2, __fdiv_rn(__fmul_rn(aa, a1), den)));
-        const float mu_p = __fadd_rn(__fmul_rn(c1, new_miu), __fmul_rn(c2, miu));
-        const float sig_p = __fsub_rn(__fadd_rn(__fmul_rn(c1, __fadd_rn(new_sq, __fmul_rn(new_miu, new_miu))),
-                                                __fmul_rn(c2, __fadd_rn(sq, __fmul_rn(miu, miu)))),
-                                      __fmul_rn(mu_p, mu_p));
+        const float mu_p = __fmaf_rn(c1, new_miu, __fmul_rn(c2, miu));
+        const float sig_p = __fmaf_rn(-mu_p, mu_p,
+                                      __fmaf_rn(c1, __fmaf_rn(new_miu, new_miu, new_sq),
+                                                __fmul_rn(c2, __fmaf_rn(miu, miu, sq))));
         const float a_p = __fdiv_rn(__fsub_rn(ee, f), __fsub_rn(f, __fdiv_rn(ee, f)));
         const float b_p = __fdiv_rn(__fmul_rn(a_p, __fsub_rn(1.0f, f)), f);
         ca = a_p; cb = b_p; cm = mu_p; cs = sig_p;
