@@ -158,8 +158,10 @@ PM_API pm_status pm_synchronize(pm_mapper* h);
  * reference): out[0] = floats w > 0 where the Newton reciprocal differs from the correctly
  * rounded 1/w, out[1] = floats u in [0, 2^22) where the add-based floor differs from floorf,
  * out[2] = (x, d) pairs, d in [2, 33], where the reciprocal-multiply division differs from IEEE
- * x / d.  All three are 0 on a correct device.  Allocates 24 bytes of device memory. */
-PM_API pm_status pm_debug_check_arith(uint64_t out[3], void* stream);
+ * x / d, out[3] = floats w where the branch-free reciprocal of the warps differs from its
+ * definition (RN(1/w) for 2^-126 <= |w| <= 2^126, NaN for zero, subnormal, infinite or NaN w,
+ * +-0 above).  All four are 0 on a correct device.  Allocates 32 bytes of device memory. */
+PM_API pm_status pm_debug_check_arith(uint64_t out[4], void* stream);
 PM_API const char* pm_last_error(const pm_mapper* h);
 PM_API const char* pm_status_string(pm_status s);
 

@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -73,6 +74,18 @@ template <typename S> struct Hom {
           r31((S)h[6]), r32((S)h[7]), r33((S)h[8]), t1((S)h[9]), t2((S)h[10]), t3((S)h[11]) {}
 };
 
+// Reciprocal of a warp.  S = double: 1/w.  S = float: the kernels' branch-free reciprocal,
+// RN(1/w) for 2^-126 <= |w| <= 2^126, NaN (sample rejected) for zero, subnormal, infinite or NaN
+// w, +-0 for larger finite |w| -- outside the first range only for homogeneous coordinates no
+// image-sized scene produces.
+template <typename S> inline S rcp_warp(S w) { return (S)1 / w; }
+template <> inline float rcp_warp<float>(float w) {
+    const float a = std::fabs(w);
+    if (!(a >= 1.17549435e-38f) || std::isinf(w)) return std::numeric_limits<float>::quiet_NaN();
+    if (a > 8.50705917e37f) return std::copysign(0.0f, w);
+    return 1.0f / w;
+}
+
 // One warped source sample (calc_cost.cu:85-93): w = z + t3*rho, u = (x + t1*rho)/w,
 // v = (y + t2*rho)/w, rejected when w < 0 or (u, v) outside [0, W-1] x [0, H-1].
 // Returns NaN for a rejected sample so that the 9-term sum carries the rejection.
@@ -81,7 +94,7 @@ inline S warp_fetch(const Plane<S>& src, S x, S y, S z, const Hom<S>& h, S rho, 
     S w = fmaT(h.t3, rho, z);
     S nx = fmaT(h.t1, rho, x);
     S ny = fmaT(h.t2, rho, y);
-    S r = (S)1 / w;
+    S r = rcp_warp(w);
     S u = nx * r, v = ny * r;
     bool ok = (w >= (S)0) && (u >= (S)0) && (u <= (S)(src.W - 1)) && (v >= (S)0) &&
               (v <= (S)(src.H - 1));

@@ -29,10 +29,10 @@ __global__ void __launch_bounds__(256) to_quad_kernel(int W, int H, const uint8_
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < W; x += gridDim.x * blockDim.x) {
         const bool hasx = (x + 1) < W;
         float4 q;
-        q.x = __fmul_rn((float)r0[x], scale);
-        q.y = hasx ? __fmul_rn((float)r0[x + 1], scale) : 0.0f;
-        q.z = has1 ? __fmul_rn((float)r1[x], scale) : 0.0f;
-        q.w = (has1 && hasx) ? __fmul_rn((float)r1[x + 1], scale) : 0.0f;
+        q.x = __fmul_rn((float)r0[x], scale);                                   // I(x, y)
+        q.y = has1 ? __fmul_rn((float)r1[x], scale) : 0.0f;                     // I(x, y+1)
+        q.z = hasx ? __fmul_rn((float)r0[x + 1], scale) : 0.0f;                 // I(x+1, y)
+        q.w = (has1 && hasx) ? __fmul_rn((float)r1[x + 1], scale) : 0.0f;       // I(x+1, y+1)
         out[x] = q;
     }
 }

@@ -38,6 +38,17 @@ __device__ __forceinline__ float rcp_rn(float w) {
     return __frcp_rn(w);
 }
 
+// The warps' reciprocal, without a branch: rcp.approx.ftz plus the same Newton step.  Equal
+// to RN(1/w) for 2^-126 <= |w| <= 2^126 (as rcp_rn); NaN for w = +-0, subnormal, infinite or NaN
+// w (a warped sample from such a w is rejected); +-0 for larger finite |w|.  The FP32 oracle
+// implements exactly this rule; pm_debug_check_arith checks it for every float.
+__device__ __forceinline__ float2 rcp_warp2(float2 w) {
+    float2 r0;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0.x) : "f"(w.x));
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0.y) : "f"(w.y));
+    return __ffma2_rn(r0, __ffma2_rn(make_float2(-w.x, -w.y), r0, make_float2(1.0f, 1.0f)), r0);
+}
+
 // floor(u) for 0 <= u < 2^22 as (float, int) without a conversion instruction: adding
 // 1.5 * 2^23 with rounding toward minus infinity leaves floor(u) in the low mantissa bits.
 __device__ __forceinline__ void floor_split(float u, float& fu, int& i) {

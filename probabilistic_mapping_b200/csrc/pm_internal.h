@@ -72,7 +72,7 @@ cudaError_t launch_filter(const float* sum, int W, int H, int D, const FilterPar
 // ---- image conversion (convert.cu + the uint8 -> float upload) ----------------------------
 cudaError_t launch_to_float(int W, int H, const uint8_t* src, size_t src_pitch, float* dst,
                             float scale, cudaStream_t s);
-// uint8 -> scaled quad image: dst[y*W + x] = (I(x,y), I(x+1,y), I(x,y+1), I(x+1,y+1)), zero
+// uint8 -> scaled quad image: dst[y*W + x] = (I(x,y), I(x,y+1), I(x+1,y), I(x+1,y+1)), zero
 // outside the image (the border addressing of the reference textures, calc_cost.cu:230-237).
 cudaError_t launch_to_quad(int W, int H, const uint8_t* src, size_t src_pitch, float4* dst,
                            float scale, cudaStream_t s);

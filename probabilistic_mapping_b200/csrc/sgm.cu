@@ -92,6 +92,21 @@ template <int PPL> __device__ __forceinline__ float plane_value(const float (&s)
     return __shfl_sync(kFull, v, d / PPL);
 }
 
+// This lane's entries of the plane-order table, through shared memory.  Read straight from the
+// kernel parameters with a lane-dependent index they become indexed constant-cache loads, which
+// serialise per distinct address and which the compiler re-issues inside the pixel loop.
+template <int PPL>
+__device__ __forceinline__ void lane_order(const PlaneOrder& o, int lane, uint32_t& incl, uint16_t (&rk)[PPL]) {
+    __shared__ uint32_t s_incl[32];
+    __shared__ uint16_t s_rank[kMaxPlanes];
+    for (int i = threadIdx.x; i < kMaxPlanes; i += blockDim.x) s_rank[i] = o.rank[i];
+    if (threadIdx.x < 32) s_incl[threadIdx.x] = o.incl[threadIdx.x];
+    __syncthreads();
+    incl = s_incl[lane];
+#pragma unroll
+    for (int j = 0; j < PPL; ++j) rk[j] = s_rank[lane * PPL + j];
+}
+
 // Winner-take-all with the reference tree's tie-break, then the three rejection rules and
 // the parabola subpixel refinement (filter_cost.cu:22-52), plus the optional uniqueness test.
 template <int PPL>
@@ -289,10 +304,9 @@ __global__ void __launch_bounds__(256) combine_kernel(const SgmLaunch a) {
     const long nw = (long)gridDim.x * (blockDim.x >> 5);
     const long npix = (long)a.W * a.H;
     const int D = a.D;
-    const uint32_t incl = a.order.incl[lane];
+    uint32_t incl;
     uint16_t rk[PPL];
-#pragma unroll
-    for (int j = 0; j < PPL; ++j) rk[j] = a.order.rank[lane * PPL + j];
+    lane_order<PPL>(a.order, lane, incl, rk);
     auto load4 = [&](long pix, float (&s)[4][PPL]) {
         const size_t e = (size_t)pix * D + lane * PPL;
 #pragma unroll
@@ -331,15 +345,15 @@ __global__ void __launch_bounds__(128) filter_kernel(const float* __restrict__ s
                                                      float* depth, size_t pitch, int32_t* index) {
     const int lane = threadIdx.x & 31;
     const long pix = (long)blockIdx.x * 4 + (threadIdx.x >> 5);
+    uint32_t incl;
+    uint16_t rk[PPL];
+    lane_order<PPL>(order, lane, incl, rk);
     if (pix >= (long)W * H) return;
     float s[PPL];
     load_planes<PPL>(s, sum + (size_t)pix * D + lane * PPL);
-    uint16_t rk[PPL];
-#pragma unroll
-    for (int j = 0; j < PPL; ++j) rk[j] = order.rank[lane * PPL + j];
     float dep;
     int idx;
-    wta_filter<PPL>(s, order.incl[lane], rk, lane, D, fp, dep, idx);
+    wta_filter<PPL>(s, incl, rk, lane, D, fp, dep, idx);
     if (lane == 0) {
         const int y = (int)(pix / W), x = (int)(pix - (long)y * W);
         *reinterpret_cast<float*>(reinterpret_cast<char*>(depth) + (size_t)y * pitch + (size_t)x * 4) = dep;
