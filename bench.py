@@ -38,12 +38,28 @@ N_KEYFRAMES = 4
 
 
 def peaks():
+    """HBM copy bandwidth (GB/s) and the SM clock the FP32 SIMT peak is derived from."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
+        return float(d["hbm_gbs"]), float(d.get("sm_max_mhz", 1965.0)), "measured"
     except Exception:
-        return 6650.0, "fallback"
+        return 6650.0, 1965.0, "fallback"
+
+
+def fp32_peak_tflops(sm_mhz: float) -> float:
+    """Non-tensor FP32 peak: 148 SMs x 128 FP32 lanes x 2 flop (FMA) per clock."""
+    return 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+
+
+def ncu_traffic(kernel: str):
+    """DRAM bytes (read + write) per launch of `kernel` at this workload, from the committed ncu
+    summary profiles/traffic.json (written from a capture of this same bench command)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)["kernels"][kernel]["dram_bytes_per_launch"]
+    except Exception:
+        return None
 
 
 class ClockSampler:
@@ -128,6 +144,19 @@ def algorithmic_bytes(e: int):
     b_alg = (S + 1) * N + 3 * e * V + 8 * V + 60 * N
     sgm_pass = PATHS * e * V + (1 + 2 * (PATHS - 2) + 1) * 4 * V + PATHS * 4 * N + 4 * N
     return b_alg, sgm_pass
+
+
+# Cost construction: 9 projective warps + 9 bilinear samples + 9 absolute differences per voxel
+# and source, 144 FP32 flop counting a division as one.
+FLOP_PER_VOXEL_SOURCE = 144
+
+
+def cost_kernel_work(e: int):
+    """Algorithmic flop and bytes of one cost-kernel launch (all S sources folded at once): the
+    volume written once (e V), the reference image and the S source quads read once."""
+    N = W * H
+    V = N * D
+    return FLOP_PER_VOXEL_SOURCE * V * S, e * V + 4 * N + 16 * N * S
 
 
 def run_ours(args, rank, world):
@@ -278,10 +307,17 @@ def main():
     e2e = world * args.steps / (t_e2e / 1000.0)
     e = 2 if args.precision == "fp16" else 4
     b_alg, sgm_bytes = algorithmic_bytes(e)
-    peak, peak_kind = peaks()
-    sgm_ms = float(stage_ms[1])
-    achieved = sgm_bytes / (sgm_ms / 1000.0) / 1e9 if sgm_ms > 0 else None
-    launches_per_step = 1 + S + 1 + PATHS + 2   # to_float x (1+S), cost, SGM passes, fusion
+    peak_hbm, sm_mhz, peak_kind = peaks()
+    peak_fp32 = fp32_peak_tflops(sm_mhz)
+    cost_ms, sgm_ms = float(stage_ms[0]), float(stage_ms[1])
+    cost_flop, cost_bytes = cost_kernel_work(e)
+    cost_tflops = cost_flop / (cost_ms / 1000.0) / 1e12 if cost_ms > 0 else None
+    cost_gbs = cost_bytes / (cost_ms / 1000.0) / 1e9 if cost_ms > 0 else None
+    sgm_gbs = sgm_bytes / (sgm_ms / 1000.0) / 1e9 if sgm_ms > 0 else None
+    map_s = t_dev / args.steps / 1000.0
+    # to_float (reference) + to_quad (S sources), cost, 2 passes x 4 path groups (8 paths) or
+    # 1 x 4, combine + winner-take-all, fusion transform + update
+    launches_per_step = 1 + S + 1 + PATHS + 1 + 2
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "depth maps/s", "n_gpus": world, "steps": args.steps,
@@ -291,13 +327,21 @@ def main():
                                    f"fusion step; {args.precision} form, {args.cost_mode} cost samples",
                        "global_batch": world, "seq_len": 0, "parallelism": f"replicas x{world}",
                        "l2": "per-map working set (cost + partial-sum volumes, 315 MB FP32) exceeds the 126 MB L2"},
-            "roofline": {"bound": "hbm", "kernel": "sgm direction passes + fused winner-take-all",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None, "traffic": None,
-                         "algorithmic_bytes_per_map": sgm_bytes, "peak_kind": peak_kind},
-            "map_roofline": {"b_alg_bytes": b_alg, "ms": t_dev / args.steps,
-                             "frac_of_hbm": b_alg / (t_dev / args.steps / 1000.0) / 1e9 / peak},
-            "stage_ms": {"cost": float(stage_ms[0]), "sgm_wta": sgm_ms, "fusion": float(stage_ms[2]),
+            # the dominant kernel (cost_kernel, ~2/3 of the map) is FP32-ALU-bound, not HBM-bound
+            "roofline": {"bound": "fp32", "kernel": "cost_kernel", "achieved": cost_tflops, "peak": peak_fp32,
+                         "unit": "TFLOP/s", "frac": (cost_tflops / peak_fp32) if cost_tflops else None,
+                         "traffic": ncu_traffic("cost_kernel"), "ms_per_launch": cost_ms,
+                         "algorithmic_flop_per_launch": cost_flop, "algorithmic_bytes_per_launch": cost_bytes,
+                         "hbm_achieved_gbs": cost_gbs, "hbm_frac": (cost_gbs / peak_hbm) if cost_gbs else None,
+                         "peak_kind": f"derived: 148 SM x 128 lanes x 2 flop x {sm_mhz:.0f} MHz ({peak_kind} clock)"},
+            "roofline_sgm": {"bound": "hbm", "kernel": "sgm direction passes + combine/winner-take-all",
+                             "achieved": sgm_gbs, "peak": peak_hbm, "unit": "GB/s",
+                             "frac": (sgm_gbs / peak_hbm) if sgm_gbs else None,
+                             "algorithmic_bytes_per_map": sgm_bytes, "ms": sgm_ms, "peak_kind": peak_kind},
+            "map_roofline": {"b_alg_bytes": b_alg, "f_alg_flop": cost_flop, "ms": t_dev / args.steps,
+                             "frac_of_hbm": b_alg / map_s / 1e9 / peak_hbm,
+                             "frac_of_fp32": cost_flop / map_s / 1e12 / peak_fp32},
+            "stage_ms": {"cost": cost_ms, "sgm_wta": sgm_ms, "fusion": float(stage_ms[2]),
                          "copy_out": float(stage_ms[3])},
             "e2e": {"value": e2e, "unit": "depth maps/s", "h2d_bytes_per_step": (S + 1) * W * H,
                     "d2h_bytes_per_step": 2 * 4 * W * H},
