@@ -50,6 +50,11 @@ typedef int pm_status;
 #define PM_PREC_FP32 0 /* plain form: FP32 images, cost volume and aggregation */
 #define PM_PREC_FP16 1 /* FP16 cost volume, FP32 SGM accumulators and fusion */
 
+/* How the FP16 form samples source frames (the FP32 form always uses exact bilinear weights). */
+#define PM_SAMPLER_EXACT 0   /* FP16 images, bilinear weights and interpolation in FP32 */
+#define PM_SAMPLER_TEXTURE 1 /* FP16 images filtered by the texture unit (8-bit weights, as the
+                                reference's own textures, calc_cost.cu:226-237) */
+
 #define PM_FUSION_GPU 0      /* StereoMapper::outputFusion + depth_fusion.cu kernels */
 #define PM_FUSION_CPU_PATH 1 /* the constants and masks of outputFusionCPU, run on the GPU */
 
@@ -72,6 +77,7 @@ typedef struct pm_config {
                             (drops planes when D is not a power of two); 0: exact minimum */
     int max_sources;     /* source frames kept per reference frame (lazy cost evaluation) */
     int device;          /* CUDA device ordinal */
+    int sampler;         /* PM_SAMPLER_*, FP16 form only */
 } pm_config;
 
 typedef struct pm_mapper pm_mapper;

@@ -22,6 +22,8 @@ PM_COST_REFERENCE = 0
 PM_COST_CORRECTED = 1
 PM_PREC_FP32 = 0
 PM_PREC_FP16 = 1
+PM_SAMPLER_EXACT = 0
+PM_SAMPLER_TEXTURE = 1
 PM_FUSION_GPU = 0
 PM_FUSION_CPU_PATH = 1
 
@@ -36,6 +38,7 @@ class PmConfig(ctypes.Structure):
         ("uniqueness_ratio", ctypes.c_float),
         ("cost_mode", ctypes.c_int), ("precision", ctypes.c_int), ("fusion_variant", ctypes.c_int),
         ("tree_compat", ctypes.c_int), ("max_sources", ctypes.c_int), ("device", ctypes.c_int),
+        ("sampler", ctypes.c_int),
     ]
 
 

@@ -13,6 +13,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda_fp16.h>
+
 #include "pm_internal.h"
 #include "pm_stereo.h"
 
@@ -27,7 +29,11 @@ struct pm_mapper {
 
     uint8_t* d_u8 = nullptr;    // upload staging, W*H bytes
     float* d_ref = nullptr;     // scaled reference image
-    float4* d_srcq = nullptr;   // max_sources source frames in the quad layout
+    float4* d_srcq = nullptr;   // FP32: max_sources source frames in the quad layout
+    void* d_srcq16 = nullptr;                     // FP16 form, exact sampler: FP16 quads
+    void* d_srch[kMaxSources] = {};               // FP16 form, texture sampler: pitched FP16 frames
+    size_t srch_pitch = 0;
+    cudaTextureObject_t tex[kMaxSources] = {};    // FP16 form: one texture object per slot
     int nsrc = 0;               // queued (not yet folded) sources
     std::vector<float> homs;    // 12 floats per queued source
     std::vector<float> all_homs;  // every source since initReference (inspection)
@@ -116,6 +122,10 @@ pm_status check_config(const pm_config* c, pm_mapper* h) {
         return fail(h, PM_ERR_INVALID_ARGUMENT, "unknown precision %d", c->precision);
     if (c->precision == PM_PREC_FP16 && c->num_planes % 64)
         return fail(h, PM_ERR_INVALID_ARGUMENT, "FP16 volumes need num_planes to be a multiple of 64");
+    if (c->sampler != PM_SAMPLER_EXACT && c->sampler != PM_SAMPLER_TEXTURE)
+        return fail(h, PM_ERR_INVALID_ARGUMENT, "unknown sampler %d", c->sampler);
+    if (c->sampler == PM_SAMPLER_TEXTURE && c->precision != PM_PREC_FP16)
+        return fail(h, PM_ERR_INVALID_ARGUMENT, "the texture sampler belongs to the FP16 form");
     if (c->fusion_variant != PM_FUSION_GPU && c->fusion_variant != PM_FUSION_CPU_PATH)
         return fail(h, PM_ERR_INVALID_ARGUMENT, "unknown fusion_variant %d", c->fusion_variant);
     if (c->max_sources < 1 || c->max_sources > kMaxSources)
@@ -196,8 +206,9 @@ void fill_sgm_launch(const pm_config& c, const PlaneOrder& order, SgmLaunch& a) 
 }
 
 // Uploads a uint8 frame (host or device) and converts it to the scaled float image (dst) or,
-// for source frames, to the quad layout the cost kernel samples (dstq).
-pm_status upload_image(pm_mapper* h, const uint8_t* img, size_t pitch, float* dst, float4* dstq) {
+// for source frame `slot` (>= 0), to the layout the cost kernel samples: quads (FP32) or the
+// slot's FP16 texture storage (FP16 form).  The FP16 form also rounds the reference to FP16.
+pm_status upload_image(pm_mapper* h, const uint8_t* img, size_t pitch, float* dst, int slot) {
     const int W = h->cfg.width, H = h->cfg.height;
     if (!img) return fail(h, PM_ERR_INVALID_ARGUMENT, "image pointer is NULL");
     if (pitch == 0) pitch = (size_t)W;
@@ -209,8 +220,19 @@ pm_status upload_image(pm_mapper* h, const uint8_t* img, size_t pitch, float* ds
         dev = h->d_u8;
         pitch = (size_t)W;
     }
-    if (dstq) PM_CK(h, launch_to_quad(W, H, dev, pitch, dstq, h->cfg.intensity_scale, h->stream));
-    else PM_CK(h, launch_to_float(W, H, dev, pitch, dst, h->cfg.intensity_scale, h->stream));
+    const float sc = h->cfg.intensity_scale;
+    const bool half = h->cfg.precision == PM_PREC_FP16;
+    if (slot >= 0 && half && h->cfg.sampler == PM_SAMPLER_TEXTURE)
+        PM_CK(h, launch_to_half(W, H, dev, pitch, h->d_srch[slot], h->srch_pitch, sc, h->stream));
+    else if (slot >= 0 && half)
+        PM_CK(h, launch_to_quad_half(W, H, dev, pitch, (char*)h->d_srcq16 + (size_t)slot * 8 * W * H, sc,
+                                     h->stream));
+    else if (slot >= 0)
+        PM_CK(h, launch_to_quad(W, H, dev, pitch, h->d_srcq + (size_t)slot * W * H, sc, h->stream));
+    else if (half)
+        PM_CK(h, launch_to_float_h(W, H, dev, pitch, dst, sc, h->stream));
+    else
+        PM_CK(h, launch_to_float(W, H, dev, pitch, dst, sc, h->stream));
     return PM_OK;
 }
 
@@ -223,6 +245,12 @@ pm_status evaluate_cost(pm_mapper* h, bool into_state) {
     a.ref = h->d_ref;
     a.srcq = h->d_srcq;
     a.nsrc = h->nsrc;
+    if (c.precision == PM_PREC_FP16 && c.sampler == PM_SAMPLER_TEXTURE) {
+        a.use_tex = 1;
+        for (int s = 0; s < h->nsrc; ++s) a.tex[s] = h->tex[s];
+    } else if (c.precision == PM_PREC_FP16) {
+        a.srcq16 = h->d_srcq16;
+    }
     for (int s = 0; s < h->nsrc; ++s)
         for (int i = 0; i < 12; ++i) a.hom[s][i] = h->homs[12 * s + i];
     a.cost = h->d_cost;
@@ -286,6 +314,11 @@ void release(pm_mapper* h) {
     cudaFree(h->d_u8);
     cudaFree(h->d_ref);
     cudaFree(h->d_srcq);
+    cudaFree(h->d_srcq16);
+    for (int s = 0; s < kMaxSources; ++s) {
+        if (h->tex[s]) cudaDestroyTextureObject(h->tex[s]);
+        cudaFree(h->d_srch[s]);
+    }
     cudaFree(h->d_cost);
     cudaFree(h->d_cnt);
     for (auto* p : h->d_part) cudaFree(p);
@@ -355,12 +388,36 @@ pm_status pm_create(const pm_config* cfg, pm_mapper** out) {
     auto alloc = [&](void** p, size_t bytes) { return note(cudaMalloc(p, bytes)); };
     bool ok = note(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->own_stream = ok;
+    const bool half = cfg->precision == PM_PREC_FP16;
     ok = ok && alloc((void**)&h->d_u8, N) && alloc((void**)&h->d_ref, 4 * N) &&
-         alloc((void**)&h->d_srcq, 16 * N * cfg->max_sources) && alloc(&h->d_cost, esz * V) &&
+         (half || alloc((void**)&h->d_srcq, 16 * N * cfg->max_sources)) &&
+         (!half || cfg->sampler == PM_SAMPLER_TEXTURE || alloc(&h->d_srcq16, 8 * N * cfg->max_sources)) &&
+         alloc(&h->d_cost, esz * V) &&
          alloc((void**)&h->d_depth, 4 * N) &&
          alloc((void**)&h->d_idx, 4 * N) && alloc((void**)&h->d_ztable, 8 * N) &&
          alloc((void**)&h->d_table, 4 * N) && alloc((void**)&h->d_fused, 4 * N) &&
          alloc((void**)&h->d_var, 4 * N);
+    // FP16 form: per-slot pitched FP16 images sampled through texture objects (linear filter,
+    // zero border, unnormalised coordinates: the reference's texture setup, calc_cost.cu:226-237)
+    for (int s = 0; half && cfg->sampler == PM_SAMPLER_TEXTURE && s < cfg->max_sources && ok; ++s) {
+        ok = note(cudaMallocPitch(&h->d_srch[s], &h->srch_pitch, sizeof(__half) * cfg->width, cfg->height));
+        if (!ok) break;
+        cudaResourceDesc rd;
+        std::memset(&rd, 0, sizeof rd);
+        rd.resType = cudaResourceTypePitch2D;
+        rd.res.pitch2D.devPtr = h->d_srch[s];
+        rd.res.pitch2D.desc = cudaCreateChannelDescHalf();
+        rd.res.pitch2D.width = cfg->width;
+        rd.res.pitch2D.height = cfg->height;
+        rd.res.pitch2D.pitchInBytes = h->srch_pitch;
+        cudaTextureDesc td;
+        std::memset(&td, 0, sizeof td);
+        td.addressMode[0] = td.addressMode[1] = cudaAddressModeBorder;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 0;
+        ok = note(cudaCreateTextureObject(&h->tex[s], &rd, &td, nullptr));
+    }
     for (int g4 = 0; g4 < 4 && ok; ++g4) ok = alloc((void**)&h->d_part[g4], 4 * V);
     for (int s = 0; s < 2 && ok; ++s)
         for (int k = 0; k < 4 && ok; ++k) ok = alloc((void**)&h->d_state[s][k], 4 * N);
@@ -420,7 +477,7 @@ pm_status pm_init_intrinsic(pm_mapper* h, const double K[9], float bf, float dep
 pm_status pm_init_reference(pm_mapper* h, const uint8_t* img, size_t pitch) {
     if (!h) return PM_ERR_INVALID_ARGUMENT;
     DeviceGuard g(h->cfg.device);
-    pm_status st = upload_image(h, img, pitch, h->d_ref, nullptr);
+    pm_status st = upload_image(h, img, pitch, h->d_ref, -1);
     if (st != PM_OK) return st;
     h->have_ref = true;
     h->nsrc = 0;
@@ -446,7 +503,7 @@ pm_status pm_update(pm_mapper* h, const uint8_t* img, size_t pitch, const double
     }
     float hom[12];
     compose_homography(h->K, R_l, T_l, R_r, T_r, hom);
-    pm_status st = upload_image(h, img, pitch, nullptr, h->d_srcq + (size_t)h->nsrc * h->cfg.width * h->cfg.height);
+    pm_status st = upload_image(h, img, pitch, nullptr, h->nsrc);
     if (st != PM_OK) return st;
     h->homs.insert(h->homs.end(), hom, hom + 12);
     h->all_homs.insert(h->all_homs.end(), hom, hom + 12);

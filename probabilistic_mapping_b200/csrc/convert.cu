@@ -1,6 +1,8 @@
 // convert.cu -- image conversions.
 //   to_float_kernel: uint8 -> scaled float, the convertTo(CV_32F) + upload of
 //                    StereoMapper::initReference / update (stereo_mapper.cpp:65-67,75-77).
+//   to_half_kernel:  uint8 -> scaled FP16 (pitched texture storage of the FP16 form), or the
+//                    same values widened to float (its reference image).
 //   convert_kernel:  pitched <-> linear float copy (reference: convert.cu:4-45).  The pitch is
 //                    taken in bytes; the reference received a byte step and indexed with it in
 //                    floats (stereo_mapper.cpp:149-152 vs convert.cu:16-21), which reads past
@@ -37,6 +39,37 @@ __global__ void __launch_bounds__(256) to_quad_kernel(int W, int H, const uint8_
     }
 }
 
+__global__ void __launch_bounds__(256) to_half_kernel(int W, int H, const uint8_t* __restrict__ src, size_t pitch,
+                                                      __half* __restrict__ dst, size_t dst_pitch, float scale,
+                                                      int as_float) {
+    const int y = blockIdx.y;
+    const uint8_t* row = src + (size_t)y * pitch;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < W; x += gridDim.x * blockDim.x) {
+        const __half v = __float2half_rn(__fmul_rn((float)row[x], scale));
+        if (as_float) reinterpret_cast<float*>(dst)[(size_t)y * W + x] = __half2float(v);
+        else reinterpret_cast<__half*>(reinterpret_cast<char*>(dst) + (size_t)y * dst_pitch)[x] = v;
+    }
+}
+
+// FP16 quads for the FP16 form's exact sampler: the layout of to_quad_kernel in halves.
+__global__ void __launch_bounds__(256) to_quad_half_kernel(int W, int H, const uint8_t* __restrict__ src,
+                                                           size_t pitch, uint2* __restrict__ dst, float scale) {
+    const int y = blockIdx.y;
+    const uint8_t* r0 = src + (size_t)y * pitch;
+    const uint8_t* r1 = r0 + pitch;
+    const bool has1 = (y + 1) < H;
+    uint2* out = dst + (size_t)y * W;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < W; x += gridDim.x * blockDim.x) {
+        const bool hasx = (x + 1) < W;
+        const float a = __fmul_rn((float)r0[x], scale);                             // I(x, y)
+        const float b = has1 ? __fmul_rn((float)r1[x], scale) : 0.0f;               // I(x, y+1)
+        const float c = hasx ? __fmul_rn((float)r0[x + 1], scale) : 0.0f;           // I(x+1, y)
+        const float d = (has1 && hasx) ? __fmul_rn((float)r1[x + 1], scale) : 0.0f; // I(x+1, y+1)
+        const __half2 lo = __floats2half2_rn(a, b), hi = __floats2half2_rn(c, d);
+        out[x] = make_uint2(*reinterpret_cast<const unsigned*>(&lo), *reinterpret_cast<const unsigned*>(&hi));
+    }
+}
+
 __global__ void __launch_bounds__(256) convert_kernel(int W, int H, const float* __restrict__ in,
                                                       float* __restrict__ out, int flag, size_t pitch) {
     const int y = blockIdx.y;
@@ -64,6 +97,27 @@ cudaError_t launch_to_quad(int W, int H, const uint8_t* src, size_t src_pitch, f
                            cudaStream_t s) {
     const dim3 grid((W + 255) / 256, H);
     to_quad_kernel<<<grid, 256, 0, s>>>(W, H, src, src_pitch, dst, scale);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_to_half(int W, int H, const uint8_t* src, size_t src_pitch, void* dst, size_t dst_pitch,
+                           float scale, cudaStream_t s) {
+    const dim3 grid((W + 255) / 256, H);
+    to_half_kernel<<<grid, 256, 0, s>>>(W, H, src, src_pitch, reinterpret_cast<__half*>(dst), dst_pitch, scale, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_to_float_h(int W, int H, const uint8_t* src, size_t src_pitch, float* dst, float scale,
+                              cudaStream_t s) {
+    const dim3 grid((W + 255) / 256, H);
+    to_half_kernel<<<grid, 256, 0, s>>>(W, H, src, src_pitch, reinterpret_cast<__half*>(dst), 0, scale, 1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_to_quad_half(int W, int H, const uint8_t* src, size_t src_pitch, void* dst, float scale,
+                                cudaStream_t s) {
+    const dim3 grid((W + 255) / 256, H);
+    to_quad_half_kernel<<<grid, 256, 0, s>>>(W, H, src, src_pitch, reinterpret_cast<uint2*>(dst), scale);
     return cudaGetLastError();
 }
 

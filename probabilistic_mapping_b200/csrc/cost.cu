@@ -72,16 +72,27 @@ __device__ __forceinline__ float2 shfl_down2(float2 v) {
     return f2(__shfl_down_sync(kFull, v.x, 1), __shfl_down_sync(kFull, v.y, 1));
 }
 
-// Source access: quad layout (one 16-byte load per bilinear sample) or plain float rows.
-template <bool QUAD> struct Src;
-template <> struct Src<true> {
+// Source access: plain float rows, the quad layout (one 16-byte load per bilinear sample), or
+// (FP16 form) a texture object over an FP16 image, filtered by the texture unit.
+enum { kPlain = 0, kQuad = 1, kTex = 2, kQuadH = 3 };
+template <int SAMP> struct Src;
+template <> struct Src<kPlain> {
+    const float* __restrict__ p;
+    int W, H;
+};
+template <> struct Src<kQuad> {
     const float4* __restrict__ q;
     int W, H;
     unsigned off;   // (1.5 * 2^23 bit pattern) * (W + 1), folded out of the quad index
 };
-template <> struct Src<false> {
-    const float* __restrict__ p;
+template <> struct Src<kTex> {
+    cudaTextureObject_t t;
     int W, H;
+};
+template <> struct Src<kQuadH> {   // FP16 quads: (I(x,y), I(x,y+1)) and (I(x+1,y), I(x+1,y+1)) as half2
+    const uint2* __restrict__ q;
+    int W, H;
+    unsigned off;
 };
 
 // Per-source constants of the warps, as packed pairs.
@@ -91,19 +102,31 @@ struct WarpConst {
 };
 
 // The warped sample of one position (x, y, z) at two planes (calc_cost.cu:85-93):
-// w = z + t3*rho, u = (x + t1*rho) * r, v = (y + t2*rho) * r with r = rcp_warp2(w); rejected (NaN)
-// when w < 0 or (u, v) lies outside [0, W-1] x [0, H-1] (NaN coordinates included).
-template <bool QUAD>
-__device__ __forceinline__ float2 sample2(const Src<QUAD>& src, const WarpConst& c, float x, float y, float z,
+// w = z + t3*rho, u = (x + t1*rho) * r, v = (y + t2*rho) * r with r = rcp_warp2(w) (FP16 form:
+// the hardware reciprocal estimate); rejected (NaN) when w < 0 or (u, v) lies outside
+// [0, W-1] x [0, H-1] (NaN coordinates included).
+template <int SAMP>
+__device__ __forceinline__ float2 sample2(const Src<SAMP>& src, const WarpConst& c, float x, float y, float z,
                                           float2 rho) {
     const float2 w = __ffma2_rn(c.t3, rho, f2(z, z));
     const float2 nx = __ffma2_rn(c.t1, rho, f2(x, x));
     const float2 ny = __ffma2_rn(c.t2, rho, f2(y, y));
-    const float2 r = rcp_warp2(w);
+    float2 r;
+    if constexpr (SAMP == kTex || SAMP == kQuadH) {
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r.x) : "f"(w.x));
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r.y) : "f"(w.y));
+    } else {
+        r = rcp_warp2(w);
+    }
     const float2 u = __fmul2_rn(nx, r), v = __fmul2_rn(ny, r);
     const bool ok0 = (w.x >= 0.0f) && (u.x >= 0.0f) && (u.x <= c.W1) && (v.x >= 0.0f) && (v.x <= c.H1);
     const bool ok1 = (w.y >= 0.0f) && (u.y >= 0.0f) && (u.y <= c.W1) && (v.y >= 0.0f) && (v.y <= c.H1);
-    if constexpr (QUAD) {
+    if constexpr (SAMP == kTex) {
+        // texel centres at +0.5, as the reference's tex2D(t, u + 0.5f, v + 0.5f) (calc_cost.cu:93)
+        const float s0 = tex2D<float>(src.t, u.x + 0.5f, v.x + 0.5f);
+        const float s1 = tex2D<float>(src.t, u.y + 0.5f, v.y + 0.5f);
+        return f2(ok0 ? s0 : nan_f(), ok1 ? s1 : nan_f());
+    } else if constexpr (SAMP == kQuad || SAMP == kQuadH) {
         // 0 <= u, v < 2^22: u + 1.5*2^23 rounded down is 1.5*2^23 + floor(u), exactly, and the
         // integer part sits in the low mantissa bits
         const float2 M = f2(12582912.0f, 12582912.0f);
@@ -114,12 +137,23 @@ __device__ __forceinline__ float2 sample2(const Src<QUAD>& src, const WarpConst&
         // below W * H); a rejected element reads quad 0 and is replaced by NaN below
         const unsigned i0 = __float_as_uint(tv.x) * (unsigned)src.W + __float_as_uint(tu.x) - src.off;
         const unsigned i1 = __float_as_uint(tv.y) * (unsigned)src.W + __float_as_uint(tu.y) - src.off;
-        const float4 t0 = __ldg(src.q + (ok0 ? i0 : 0u));
-        const float4 t1 = __ldg(src.q + (ok1 ? i1 : 0u));
+        float2 lo0, hi0, lo1, hi1;
+        if constexpr (SAMP == kQuad) {
+            const float4 t0 = __ldg(src.q + (ok0 ? i0 : 0u));
+            const float4 t1 = __ldg(src.q + (ok1 ? i1 : 0u));
+            lo0 = f2(t0.x, t0.y); hi0 = f2(t0.z, t0.w);
+            lo1 = f2(t1.x, t1.y); hi1 = f2(t1.z, t1.w);
+        } else {
+            const uint2 t0 = __ldg(src.q + (ok0 ? i0 : 0u));
+            const uint2 t1 = __ldg(src.q + (ok1 ? i1 : 0u));
+            lo0 = __half22float2(*reinterpret_cast<const __half2*>(&t0.x));
+            hi0 = __half22float2(*reinterpret_cast<const __half2*>(&t0.y));
+            lo1 = __half22float2(*reinterpret_cast<const __half2*>(&t1.x));
+            hi1 = __half22float2(*reinterpret_cast<const __half2*>(&t1.y));
+        }
         // (top, bot) = fma(a, (I(x+1,y), I(x+1,y+1)) - (I(x,y), I(x,y+1)), (I(x,y), I(x,y+1)))
-        const float2 lo0 = f2(t0.x, t0.y), lo1 = f2(t1.x, t1.y);
-        const float2 p0 = __ffma2_rn(f2(a.x, a.x), sub2(f2(t0.z, t0.w), lo0), lo0);
-        const float2 p1 = __ffma2_rn(f2(a.y, a.y), sub2(f2(t1.z, t1.w), lo1), lo1);
+        const float2 p0 = __ffma2_rn(f2(a.x, a.x), sub2(hi0, lo0), lo0);
+        const float2 p1 = __ffma2_rn(f2(a.y, a.y), sub2(hi1, lo1), lo1);
         const float s0 = __fmaf_rn(b.x, __fsub_rn(p0.y, p0.x), p0.x);
         const float s1 = __fmaf_rn(b.y, __fsub_rn(p1.y, p1.x), p1.x);
         return f2(ok0 ? s0 : nan_f(), ok1 ? s1 : nan_f());
@@ -158,7 +192,7 @@ __device__ __forceinline__ void fold(float& acc, float& cn, float tmp, float r9,
 }
 
 // MODE 0: reference sample set (calc_cost.cu:83-199); MODE 1: corrected 3x3 patch.
-template <int MODE, bool HALF, bool QUAD>
+template <int MODE, bool HALF, int SAMP>
 __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* const refp = reinterpret_cast<float2*>(smem_raw + Smem::REF);
@@ -208,9 +242,14 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
     float* const cntp = cnts + (out_col ? lane - 1 : 0) * SP + 2 * warp;
 
     for (int s = 0; s < a.nsrc; ++s) {
-        Src<QUAD> src;
-        if constexpr (QUAD) {
+        Src<SAMP> src;
+        if constexpr (SAMP == kQuad) {
             src.q = a.srcq + (size_t)s * W * H;
+            src.off = 0x4B400000u * (unsigned)(W + 1);
+        } else if constexpr (SAMP == kTex) {
+            src.t = a.tex[s];
+        } else if constexpr (SAMP == kQuadH) {
+            src.q = reinterpret_cast<const uint2*>(a.srcq16) + (size_t)s * W * H;
             src.off = 0x4B400000u * (unsigned)(W + 1);
         } else {
             src.p = a.srcs + (size_t)s * W * H;
@@ -233,7 +272,7 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
         for (int r = 0; r < TY + 2; ++r) {
             float hx, hy, hz;
             homog(h, x, y0 - 1 + r, hx, hy, hz);
-            const float2 Sd = sample2<QUAD>(src, c, hx, hy, hz, rho);
+            const float2 Sd = sample2<SAMP>(src, c, hx, hy, hz, rho);
             const float2 Ld = shfl_up2(Sd), Rd_ = shfl_down2(Sd);
             const int o = r - 2;   // output row y0 + o
             if (o >= 0 && out_col && y0 + o < H) {
@@ -246,8 +285,8 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
                     // the corrupted neighbours (calc_cost.cu:49-51, 69-71) from the centre's x
                     const float xr = __fadd_rn(hxc, h.r11), yr = __fadd_rn(hxc, h.r21), zr = __fadd_rn(hxc, h.r31);
                     const float xru = __fsub_rn(xr, h.r12), yru = __fsub_rn(xr, h.r22), zru = __fsub_rn(xr, h.r32);
-                    const float2 B4 = sample2<QUAD>(src, c, xr, yr, zr, rho);
-                    const float2 B8 = sample2<QUAD>(src, c, xru, yru, zru, rho);
+                    const float2 B4 = sample2<SAMP>(src, c, xr, yr, zr, rho);
+                    const float2 B8 = sample2<SAMP>(src, c, xru, yru, zru, rho);
                     d[0] = sub2(Rc_, Sc);    // 0  (:93)
                     d[1] = sub2(Rd, Su);     // 1  warps (u, v-1), reads ref (u, v+1) (:106)
                     d[2] = sub2(Ru_, Sd);    // 2  warps (u, v+1), reads ref (u, v-1) (:119)
@@ -318,9 +357,9 @@ __global__ void __launch_bounds__(256) invalid_kernel(const void* cost, long npi
     if (lane == 0) invalid[pix] = any ? 1 : 0;
 }
 
-template <int MODE, bool HALF, bool QUAD>
+template <int MODE, bool HALF, int SAMP>
 cudaError_t launch_t(const CostLaunch& a, dim3 grid, cudaStream_t s) {
-    auto kern = cost_kernel<MODE, HALF, QUAD>;
+    auto kern = cost_kernel<MODE, HALF, SAMP>;
     if (Smem::BYTES > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Smem::BYTES);
         if (e != cudaSuccess) return e;
@@ -331,7 +370,9 @@ cudaError_t launch_t(const CostLaunch& a, dim3 grid, cudaStream_t s) {
 
 template <int MODE, bool HALF>
 cudaError_t launch_q(const CostLaunch& a, dim3 grid, cudaStream_t s) {
-    return a.srcq ? launch_t<MODE, HALF, true>(a, grid, s) : launch_t<MODE, HALF, false>(a, grid, s);
+    if (a.use_tex) return launch_t<MODE, HALF, kTex>(a, grid, s);
+    if (a.srcq16) return launch_t<MODE, HALF, kQuadH>(a, grid, s);
+    return a.srcq ? launch_t<MODE, HALF, kQuad>(a, grid, s) : launch_t<MODE, HALF, kPlain>(a, grid, s);
 }
 
 }  // namespace

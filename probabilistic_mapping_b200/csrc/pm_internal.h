@@ -17,6 +17,11 @@ struct CostLaunch {
     const float* ref;      // W*H scaled reference image
     const float* srcs;     // nsrc consecutive W*H scaled source images (used when srcq is null)
     const float4* srcq;    // nsrc consecutive W*H quad images (2x2 bilinear footprints)
+    // FP16 form: sources as FP16 quads (srcq16, 8 bytes per pixel), or, when use_tex is set,
+    // through these texture objects (FP16 pitched images, linear filtering, zero border)
+    const void* srcq16;
+    unsigned long long tex[kMaxSources];
+    int use_tex;
     int W, H, D, nsrc;
     float rho0, drho;
     int mode;              // 0 reference quirks, 1 corrected 3x3 patch
@@ -74,6 +79,15 @@ cudaError_t launch_to_float(int W, int H, const uint8_t* src, size_t src_pitch, 
                             float scale, cudaStream_t s);
 // uint8 -> scaled quad image: dst[y*W + x] = (I(x,y), I(x,y+1), I(x+1,y), I(x+1,y+1)), zero
 // outside the image (the border addressing of the reference textures, calc_cost.cu:230-237).
+// uint8 -> scaled FP16 image with a byte pitch (the FP16 form's texture storage).
+cudaError_t launch_to_half(int W, int H, const uint8_t* src, size_t src_pitch, void* dst, size_t dst_pitch,
+                           float scale, cudaStream_t s);
+// uint8 -> FP16 quads (the quad layout in halves, 8 bytes per pixel): the FP16 form's exact sampler.
+cudaError_t launch_to_quad_half(int W, int H, const uint8_t* src, size_t src_pitch, void* dst, float scale,
+                                cudaStream_t s);
+// uint8 -> scaled float image whose values are rounded to FP16 (the FP16 form's reference image).
+cudaError_t launch_to_float_h(int W, int H, const uint8_t* src, size_t src_pitch, float* dst, float scale,
+                              cudaStream_t s);
 cudaError_t launch_to_quad(int W, int H, const uint8_t* src, size_t src_pitch, float4* dst,
                            float scale, cudaStream_t s);
 cudaError_t launch_convert(int W, int H, const float* in, float* out, int flag, size_t pitch_bytes,

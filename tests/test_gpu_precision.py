@@ -1,0 +1,94 @@
+"""The FP16 form against the FP64 oracle, next to the FP32 form on the same frames.
+
+Precision configuration: 752x480 frames (fx = fy = 460), 128 planes, 5 sources, 8-path SGM,
+uniqueness 0.95, scaled intensities.  FP16 form = FP16 source images and reference values, FP16
+cost volume, FP32 SGM accumulators; its sources are sampled either with exact bilinear weights
+in FP32 arithmetic (PM_SAMPLER_EXACT) or by the texture unit (PM_SAMPLER_TEXTURE: 8-bit weights,
+as the reference's own textures).  Reported per pixel where both maps hold a depth: median and
+p99 of |rho - rho64| / rho64 (inverse depth), plus the WTA plane-index match rate over all pixels.
+With PM_REPORT_DIR set the numbers are also written to $PM_REPORT_DIR/precision_752x480x128.json.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from probabilistic_mapping_b200 import _lib, scene
+from probabilistic_mapping_b200.mapper import StereoMapper
+
+pytestmark = pytest.mark.gpu
+
+W, H, D, S, F = 752, 480, 128, 5, 460.0
+PARAMS = dict(p1=0.003, p2=0.01, tau_so=3.5 / 255, uniqueness=0.95)
+
+
+@pytest.fixture(scope="module")
+def frames():
+    return scene.make_frameset(W, H, F, S, seed=77)
+
+
+def run_gpu(fs, precision, mode, sampler=0):
+    rho0, drho = scene.plane_range(D)
+    m = StereoMapper(W, H, D, rho0=rho0, intensity_scale=1 / 255, num_paths=8, p1=PARAMS["p1"], p2=PARAMS["p2"],
+                     tau_so=PARAMS["tau_so"], uniqueness_ratio=PARAMS["uniqueness"], cost_mode=mode,
+                     precision=precision, sampler=sampler)
+    m.initIntrinsic(fs.K, 0.0, drho)
+    m.initReference(fs.ref)
+    for s in range(S):
+        m.update(fs.srcs[s], fs.R_ref, fs.T_ref, fs.R_srcs[s], fs.T_srcs[s])
+    depth = m.output()
+    idx = m.wta_index()
+    m.close()
+    return depth, idx
+
+
+def run_fp64(fs, mode):
+    rho0, drho = scene.plane_range(D)
+    o = oracle.Mapper(oracle.Params(W=W, H=H, D=D, drho=drho, rho0=rho0, intensity_scale=1 / 255, cost_mode=mode,
+                                    num_paths=8, **PARAMS), fs.K)
+    o.init_reference(fs.ref)
+    for s in range(S):
+        o.update(fs.srcs[s], fs.R_ref, fs.T_ref, fs.R_srcs[s], fs.T_srcs[s])
+    st = o.stages()
+    return st["depth"], st["idx"]
+
+
+def has_depth(d):
+    return (d > 0) & (d < 1000)
+
+
+def stats(depth, idx, d64, i64):
+    both = has_depth(depth) & has_depth(d64)
+    rel = np.abs(1.0 / depth[both].astype(np.float64) - 1.0 / d64[both]) * d64[both]
+    return {"wta_index_match": float((idx == i64).mean()),
+            "validity_match": float((has_depth(depth) == has_depth(d64)).mean()),
+            "rel_inv_depth_median": float(np.median(rel)), "rel_inv_depth_p99": float(np.percentile(rel, 99)),
+            "pixels_compared": int(both.sum())}
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_fp16_form_against_fp64(frames, mode):
+    d64, i64 = run_fp64(frames, mode)
+    d32, x32 = run_gpu(frames, _lib.PM_PREC_FP32, mode)
+    d16, x16 = run_gpu(frames, _lib.PM_PREC_FP16, mode, _lib.PM_SAMPLER_EXACT)
+    dtx, xtx = run_gpu(frames, _lib.PM_PREC_FP16, mode, _lib.PM_SAMPLER_TEXTURE)
+    r32, r16, rtx = stats(d32, x32, d64, i64), stats(d16, x16, d64, i64), stats(dtx, xtx, d64, i64)
+    report = {"config": f"{W}x{H}, f={F}, {D} planes, {S} sources, 8 paths, "
+                        f"{'reference' if mode == 0 else 'corrected'} cost samples",
+              "fp32": r32, "fp16_exact_sampler": r16, "fp16_texture_sampler": rtx}
+    print(json.dumps(report))
+    out = os.environ.get("PM_REPORT_DIR")
+    if out:
+        os.makedirs(out, exist_ok=True)
+        with open(os.path.join(out, f"precision_{W}x{H}x{D}_mode{mode}.json"), "w") as f:
+            json.dump(report, f, indent=1)
+    assert r32["wta_index_match"] >= 0.995
+    assert r32["rel_inv_depth_median"] < 1e-4
+    # the FP16 form's accuracy bound: <= 1 % inverse-depth error, >= 99.5 % identical WTA indices
+    assert r16["rel_inv_depth_median"] <= 0.01
+    assert r16["wta_index_match"] >= 0.995
+    # texture sampling keeps the depth error far inside the bound but moves more WTA indices
+    assert rtx["rel_inv_depth_median"] <= 0.01
+    assert rtx["wta_index_match"] >= 0.985
