@@ -189,9 +189,10 @@ PM_API pm_status pm_stage_calc_cost(const pm_config* cfg, const float* ref, cons
                              const float* homs, float* cost, float* cnt, uint8_t* invalid,
                              void* stream);
 
-/* sgm2 (sgm.cu:115-135): out := sum over cfg->num_paths paths; out needs no clearing.  The
- * paths run as four groups {g, g+4} with their own partial sums, added as
- * (S0 + S1) + (S2 + S3); scratch holds the partials of groups 1..3 (3*W*H*D floats). */
+/* sgm2 (sgm.cu:115-135): out := sum over cfg->num_paths paths; out needs no clearing.  Each
+ * path is aggregated into its own volume (out holds path 0, scratch the other num_paths - 1:
+ * (num_paths - 1)*W*H*D floats), opposite paths pairwise in one kernel, and the volumes are
+ * added as (P0 + P1) + (P2 + P3) [+ ((P4 + P5) + (P6 + P7))], paths in the reference's order. */
 PM_API pm_status pm_stage_sgm(const pm_config* cfg, const float* cost, const float* ref, float* out,
                        float* scratch, void* stream);
 
@@ -199,8 +200,8 @@ PM_API pm_status pm_stage_sgm(const pm_config* cfg, const float* cost, const flo
 PM_API pm_status pm_stage_filter(const pm_config* cfg, const float* sgm, float* depth, size_t pitch_bytes,
                           int32_t* index, void* stream);
 
-/* sgm2 + filter_cost fused: the last path finishes the sum in registers and runs the
- * winner-take-all; `scratch` holds the four partial sums (4*W*H*D floats). */
+/* sgm2 + filter_cost fused: the combine kernel adds the path volumes in registers and runs the
+ * winner-take-all; `scratch` holds the num_paths path volumes (num_paths*W*H*D floats). */
 PM_API pm_status pm_stage_sgm_filter(const pm_config* cfg, const float* cost, const float* ref,
                               float* scratch, float* depth, size_t pitch_bytes, int32_t* index,
                               void* stream);

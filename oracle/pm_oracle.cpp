@@ -231,11 +231,12 @@ const Dir kDirs[8] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1}, {-1, 1
 
 // a4 -- sgm.cu:5-113 (one scanline), host order sgm.cu:115-135.
 // sum_order 0 accumulates the paths in the reference's order (L->R, R->L, T->B, B->T, then
-// the diagonals) into one buffer.  sum_order 1 is the order of the B200 kernels, which run the
-// paths as four concurrent groups {r, r+4}: group g accumulates its paths into part[g], and
-// the result is (part0 + part1) + (part2 + part3).  The two differ only in FP rounding.
+// the diagonals) into one buffer.  sum_order 1 is the order of the B200 kernels, which write
+// every path into its own volume P_r (paths in the order above) and add them pairwise:
+// (P0 + P1) + (P2 + P3) for 4 paths, ((P0 + P1) + (P2 + P3)) + ((P4 + P5) + (P6 + P7)) for 8.
+// The two differ only in FP rounding.
 template <typename S>
-void sgm_paths(const orc_params* p, const uint8_t* ref8, const S* C, S* out, const int* group_of,
+void sgm_paths(const orc_params* p, const uint8_t* ref8, const S* C, const int* group_of, bool assign,
                std::vector<S*>& parts);
 
 template <typename S>
@@ -247,28 +248,27 @@ void sgm(const orc_params* p, const uint8_t* ref8, const S* C, S* out) {
     if (p->sum_order == 0) {
         for (int r = 0; r < 8; ++r) group_of[r] = 0;
         parts.push_back(out);
-    } else {
-        for (int r = 0; r < 8; ++r) group_of[r] = r % 4;
-        parts.push_back(out);
-        for (int g = 1; g < 4; ++g) {
-            bufs.emplace_back(V);
-            parts.push_back(bufs.back().data());
-        }
+        sgm_paths<S>(p, ref8, C, group_of, false, parts);
+        return;
     }
-    sgm_paths<S>(p, ref8, C, out, group_of, parts);
-    if (p->sum_order != 0) {
-        const S* a = parts[1];
-        const S* b = parts[2];
-        const S* c = parts[3];
+    for (int r = 0; r < 8; ++r) group_of[r] = r;
+    for (int r = 0; r < p->num_paths; ++r) {
+        bufs.emplace_back(V);
+        parts.push_back(bufs.back().data());
+    }
+    sgm_paths<S>(p, ref8, C, group_of, true, parts);
+    const bool eight = p->num_paths == 8;
 #pragma omp parallel for schedule(static)
-        for (long i = 0; i < (long)V; ++i) out[i] = (out[i] + a[i]) + (b[i] + c[i]);
+    for (long i = 0; i < (long)V; ++i) {
+        const S s4 = (parts[0][i] + parts[1][i]) + (parts[2][i] + parts[3][i]);
+        out[i] = eight ? s4 + ((parts[4][i] + parts[5][i]) + (parts[6][i] + parts[7][i])) : s4;
     }
 }
 
+// assign: each path writes its own buffer (o = L at a valid pixel) instead of accumulating.
 template <typename S>
-void sgm_paths(const orc_params* p, const uint8_t* ref8, const S* C, S* out, const int* group_of,
+void sgm_paths(const orc_params* p, const uint8_t* ref8, const S* C, const int* group_of, bool assign,
                std::vector<S*>& parts) {
-    (void)out;
     const int W = p->W, H = p->H, D = p->D;
     const size_t N = (size_t)W * H;
     std::vector<S> refv = to_scalar<S>(ref8, (int)N, p->intensity_scale);
@@ -304,7 +304,7 @@ void sgm_paths(const orc_params* p, const uint8_t* ref8, const S* C, S* out, con
                 if (k == 0) {
                     for (int d = 0; d < D; ++d) {
                         L[d] = invalid ? (S)0 : c[d];
-                        o[d] = invalid ? (S)0 : o[d] + L[d];
+                        o[d] = invalid ? (S)0 : (assign ? L[d] : o[d] + L[d]);
                     }
                 } else {
                     // D1 = |I(x,y) - I(x-dx,y-dy)| (:75); both inside the image here
@@ -318,7 +318,7 @@ void sgm_paths(const orc_params* p, const uint8_t* ref8, const S* C, S* out, con
                         if (d + 1 < D) v = std::min(v, L[d + 1] + P1);
                         v = cd + v - mprev;     // (:98)
                         val[d] = v;
-                        o[d] = invalid ? (S)0 : o[d] + v;
+                        o[d] = invalid ? (S)0 : (assign ? v : o[d] + v);
                     }
                     L.swap(val);
                 }

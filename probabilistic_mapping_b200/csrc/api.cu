@@ -43,7 +43,7 @@ struct pm_mapper {
 
     void* d_cost = nullptr;     // W*H*D float or half
     float* d_cnt = nullptr;     // allocated on the first fold
-    float* d_part[4] = {};      // SGM partial sums of the four path groups
+    float* d_part[8] = {};      // SGM: one volume per path (num_paths of them)
     SgmStreams side{};          // concurrent path groups
     bool have_side = false;
     float* d_depth = nullptr;   // WTA depth, linear
@@ -275,7 +275,7 @@ pm_status run_sgm_filter(pm_mapper* h) {
     fill_sgm_launch(c, h->order, a);
     a.cost = h->d_cost;
     a.ref = h->d_ref;
-    for (int g = 0; g < 4; ++g) a.part[g] = h->d_part[g];
+    for (int r = 0; r < c.num_paths; ++r) a.part[r] = h->d_part[r];
     a.total = h->store_sgm ? h->d_part[0] : nullptr;   // combine reads part[0] of a pixel before writing it
     a.depth = h->d_depth;
     a.depth_pitch = sizeof(float) * (size_t)c.width;
@@ -418,7 +418,7 @@ pm_status pm_create(const pm_config* cfg, pm_mapper** out) {
         td.normalizedCoords = 0;
         ok = note(cudaCreateTextureObject(&h->tex[s], &rd, &td, nullptr));
     }
-    for (int g4 = 0; g4 < 4 && ok; ++g4) ok = alloc((void**)&h->d_part[g4], 4 * V);
+    for (int r = 0; r < cfg->num_paths && ok; ++r) ok = alloc((void**)&h->d_part[r], 4 * V);
     for (int s = 0; s < 2 && ok; ++s)
         for (int k = 0; k < 4 && ok; ++k) ok = alloc((void**)&h->d_state[s][k], 4 * N);
     if (ok) {
@@ -750,7 +750,7 @@ pm_status pm_stage_sgm(const pm_config* cfg, const float* cost, const float* ref
     a.ref = ref;
     const size_t V = (size_t)cfg->width * cfg->height * cfg->num_planes;
     a.part[0] = out;   // the combine kernel reads part[0] of a pixel before it writes the total there
-    for (int g = 1; g < 4; ++g) a.part[g] = scratch + (g - 1) * V;
+    for (int r = 1; r < cfg->num_paths; ++r) a.part[r] = scratch + (r - 1) * V;
     a.total = out;
     return launch_sgm(a, false, (cudaStream_t)stream, nullptr) == cudaSuccess ? PM_OK : PM_ERR_CUDA;
 }
@@ -782,7 +782,7 @@ pm_status pm_stage_sgm_filter(const pm_config* cfg, const float* cost, const flo
     a.cost = cost;
     a.ref = ref;
     const size_t V = (size_t)cfg->width * cfg->height * cfg->num_planes;
-    for (int g = 0; g < 4; ++g) a.part[g] = scratch + g * V;
+    for (int r = 0; r < cfg->num_paths; ++r) a.part[r] = scratch + r * V;
     a.total = nullptr;
     a.depth = depth;
     a.depth_pitch = pitch;

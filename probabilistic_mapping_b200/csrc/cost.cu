@@ -33,18 +33,14 @@ constexpr int TY = 8;                    // output rows per tile
 constexpr int WARPS = 8;                 // one plane pair per warp
 constexpr int PCB = 2 * WARPS;           // planes per CTA
 constexpr int NT = 32 * WARPS;
-constexpr int SP = PCB + 1;              // staging pitch (odd: conflict-free column writes)
+constexpr int SP = PCB + 2;              // state pitch: even (8-byte pairs), conflict-free pairs
 constexpr int NPIX = TXU * TY;
-constexpr int MAXCNT = kMaxSources + 2;  // reciprocal table covers counts 0..kMaxSources+1
-
-static_assert(MAXCNT <= NT, "the reciprocal table is filled by one thread per entry");
 
 struct Smem {
     static constexpr size_t REF = 0;                                        // float2 [TY+2][32]
     static constexpr size_t ACC = REF + sizeof(float2) * (TY + 2) * 32;     // float [NPIX][SP]
     static constexpr size_t CNT = ACC + sizeof(float) * NPIX * SP;          // float [NPIX][SP]
-    static constexpr size_t RTAB = CNT + sizeof(float) * NPIX * SP;         // float [MAXCNT]
-    static constexpr size_t BYTES = RTAB + sizeof(float) * MAXCNT;
+    static constexpr size_t BYTES = CNT + sizeof(float) * NPIX * SP;
 };
 
 __device__ __forceinline__ float ref_at(const float* __restrict__ ref, int W, int H, int x, int y) {
@@ -172,23 +168,34 @@ __device__ __forceinline__ Hom load_hom(const CostLaunch& a, int s) {
     return h;
 }
 
-// One source's 9-term sum folded into the running state of a voxel: a rejected sample skips
-// the voxel (calc_cost.cu:89-91), the first measurement replaces the initial -1 (:200-203),
-// later ones update the running mean (cnt*last + tmp/9)/(cnt+1) (:205-206).
-__device__ __forceinline__ void fold(float& acc, float& cn, float tmp, float r9, const float* rtab) {
-    if (tmp == tmp) {
-        const float m = div_small(tmp, 9.0f, r9);
-        if (acc < 0.0f) {
-            acc = m;
-            cn = 1.0f;
-        } else {
-            const float n1 = __fadd_rn(cn, 1.0f);
-            const float num = __fmaf_rn(cn, acc, m);
-            const int ni = (int)n1;   // counts beyond the table (long running states)
-            acc = ni < MAXCNT ? div_small(num, n1, rtab[ni]) : __fdiv_rn(num, n1);
-            cn = n1;
-        }
+// One source's 9-term sums folded into the running state of the two voxels of a plane pair,
+// (cnt*last + tmp/9)/(cnt+1) and cnt+1 (calc_cost.cu:205-206); a NaN sum (a rejected sample)
+// leaves its voxel unchanged (:89-91).  The first measurement of a voxel (last = -1, cnt = 0)
+// comes out as tmp/9 exactly, which is the reference's separate branch (:200-203): every state
+// this library writes has cnt = 0 exactly where last < 0.  Both divisions are a
+// reciprocal-multiply with one FMA correction (RN(1/9) and the exact Newton reciprocal of
+// cnt+1), equal to IEEE division for divisors up to 33 and dividends 0 or >= 1e-30 (the
+// exhaustive check of pm_debug_check_arith); outside that the pair takes IEEE division.
+__device__ __forceinline__ void fold2(float2& acc, float2& cn, float2 tmp, float r9) {
+    const float2 r9p = f2(r9, r9);
+    const float2 n1 = __fadd2_rn(cn, f2(1.0f, 1.0f));
+    const float2 nn1 = __ffma2_rn(cn, f2(-1.0f, -1.0f), f2(-1.0f, -1.0f));   // -(cnt + 1), exact
+    const float2 q0 = __fmul2_rn(tmp, r9p);
+    const float2 m = __ffma2_rn(__ffma2_rn(q0, f2(-9.0f, -9.0f), tmp), r9p, q0);
+    const float2 num = __ffma2_rn(cn, acc, m);
+    const float2 r = rcp_warp2(n1);
+    const float2 p0 = __fmul2_rn(num, r);
+    float2 q = __ffma2_rn(__ffma2_rn(p0, nn1, num), r, p0);
+    const bool fast = n1.x <= 33.0f && n1.y <= 33.0f && !(tmp.x != 0.0f && tmp.x < 1e-30f) &&
+                      !(tmp.y != 0.0f && tmp.y < 1e-30f) && !(num.x != 0.0f && num.x < 1e-30f) &&
+                      !(num.y != 0.0f && num.y < 1e-30f);
+    if (!fast) {
+        q.x = __fdiv_rn(__fmaf_rn(cn.x, acc.x, __fdiv_rn(tmp.x, 9.0f)), n1.x);
+        q.y = __fdiv_rn(__fmaf_rn(cn.y, acc.y, __fdiv_rn(tmp.y, 9.0f)), n1.y);
     }
+    const bool v0 = tmp.x == tmp.x, v1 = tmp.y == tmp.y;
+    acc = f2(v0 ? q.x : acc.x, v1 ? q.y : acc.y);
+    cn = f2(v0 ? n1.x : cn.x, v1 ? n1.y : cn.y);
 }
 
 // MODE 0: reference sample set (calc_cost.cu:83-199); MODE 1: corrected 3x3 patch.
@@ -198,7 +205,6 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
     float2* const refp = reinterpret_cast<float2*>(smem_raw + Smem::REF);
     float* const accs = reinterpret_cast<float*>(smem_raw + Smem::ACC);
     float* const cnts = reinterpret_cast<float*>(smem_raw + Smem::CNT);
-    float* const rtab = reinterpret_cast<float*>(smem_raw + Smem::RTAB);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int W = a.W, H = a.H, D = a.D;
@@ -213,7 +219,6 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
         const float R = ref_at(a.ref, W, H, x0 - 1 + l, y0 - 1 + r);
         refp[i] = f2(R, R);
     }
-    if (tid < MAXCNT) rtab[tid] = tid == 0 ? 0.0f : __frcp_rn((float)tid);
 
     // running state of the tile's voxels, [pixel][plane] with pitch SP: from memory (the
     // state of earlier calls), or the initReference state cost = -1, count = 0
@@ -237,9 +242,10 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
     const int da = d0 + 2 * warp;   // idep = i * DEP_SAMPLE (calc_cost.cu:81), plus rho0
     const float2 rho = f2(__fmaf_rn((float)da, a.drho, a.rho0), __fmaf_rn((float)(da + 1), a.drho, a.rho0));
     const float r9 = __frcp_rn(9.0f);
-    // this lane's state slots; lanes outside the output columns never touch them
-    float* const accp = accs + (out_col ? lane - 1 : 0) * SP + 2 * warp;
-    float* const cntp = cnts + (out_col ? lane - 1 : 0) * SP + 2 * warp;
+    // this lane's state slots (one 8-byte pair per row); lanes outside the output columns never
+    // touch them
+    float2* const accp = reinterpret_cast<float2*>(accs + (out_col ? lane - 1 : 0) * SP + 2 * warp);
+    float2* const cntp = reinterpret_cast<float2*>(cnts + (out_col ? lane - 1 : 0) * SP + 2 * warp);
 
     for (int s = 0; s < a.nsrc; ++s) {
         Src<SAMP> src;
@@ -313,15 +319,12 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
                     tx = __fadd_rn(tx, fabsf(d[k].x));
                     ty = __fadd_rn(ty, fabsf(d[k].y));
                 }
-                float* const ap = accp + o * TXU * SP;
-                float* const cp = cntp + o * TXU * SP;
-                float a0 = ap[0], a1 = ap[1], n0 = cp[0], n1 = cp[1];
-                fold(a0, n0, tx, r9, rtab);
-                fold(a1, n1, ty, r9, rtab);
-                ap[0] = a0;
-                ap[1] = a1;
-                cp[0] = n0;
-                cp[1] = n1;
+                float2* const ap = accp + o * (TXU * SP / 2);
+                float2* const cp = cntp + o * (TXU * SP / 2);
+                float2 av = *ap, nv = *cp;
+                fold2(av, nv, f2(tx, ty), r9);
+                *ap = av;
+                *cp = nv;
             }
             Su = Sc; Sc = Sd;
             Lu = Lc; Lc = Ld;

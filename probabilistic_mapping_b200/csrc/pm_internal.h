@@ -50,7 +50,7 @@ struct SgmLaunch {
     const void* cost;      // W*H*D float or __half
     int cost_half;
     const float* ref;      // W*H scaled reference image (path gradient D1, sgm.cu:75)
-    float* part[4];        // W*H*D partial sums of the four path groups
+    float* part[8];        // W*H*D volume of each path (num_paths of them), reference path order
     float* total;          // W*H*D complete sum (may alias part[0]); nullptr: not stored
     int W, H, D, num_paths;
     float p1, p2, tau, q1, q2;
@@ -60,15 +60,15 @@ struct SgmLaunch {
     int32_t* index;        // W*H (optional)
     PlaneOrder order;
 };
-// Side streams for the concurrent path groups: groups 0..2 fork from the caller's stream
-// and join back before the final pass.
+// Side streams for the concurrent path pairs: pairs 0..2 fork from the caller's stream and join
+// back before the combine kernel.
 struct SgmStreams {
     cudaStream_t stream[3];
     cudaEvent_t fork;
     cudaEvent_t join[3];
 };
-// Runs the path groups {g, g+4}; the final pass adds (S0 + S1) + (S2 + S3) in registers and,
-// with fuse_filter, writes depth/index.  side == nullptr runs every pass on s.
+// Runs the opposite-path pairs (each path into part[r]), then adds the path volumes pairwise in
+// registers and, with fuse_filter, writes depth/index.  side == nullptr runs everything on s.
 cudaError_t launch_sgm(const SgmLaunch& a, bool fuse_filter, cudaStream_t s, const SgmStreams* side);
 cudaError_t launch_filter(const float* sum, int W, int H, int D, const FilterParams& fp,
                           const PlaneOrder& order, float* depth, size_t pitch, int32_t* index,

@@ -9,13 +9,15 @@
 //     redux.sync.min.f32;
 //   * the per-pixel plane vector (contiguous in the plane-innermost layout) is streamed with
 //     cp.async into a per-lane shared-memory ring PF steps ahead of the recurrence;
-//   * the paths run as four concurrent groups {r, r+4} (an axis direction and a diagonal),
-//     each accumulating into its own partial-sum volume, so four times as many scanlines are
-//     in flight as in a one-direction-at-a-time schedule;
-//   * a pixel-parallel combine kernel (one warp per pixel, full occupancy) adds the partials
-//     as (S0 + S1) + (S2 + S3) in registers and runs the winner-take-all directly, so the
-//     complete sum is never written.  The FP32 result therefore differs from the reference's
-//     sequential path order only by rounding; the CPU oracle replays this exact order.
+//   * opposite paths run as pairs: one warp walks a scanline from both ends at once, so it keeps
+//     two independent recurrences in flight; the pairs (L/R, T/B and the two diagonals) run
+//     concurrently on separate streams, and every path writes its own volume (no
+//     read-modify-write between passes);
+//   * a pixel-parallel combine kernel (one warp per pixel, full occupancy) adds the path volumes
+//     pairwise, (P0 + P1) + (P2 + P3) [+ ((P4 + P5) + (P6 + P7))], in registers and runs the
+//     winner-take-all directly, so the complete sum need not be written.  The FP32 result
+//     therefore differs from the reference's sequential path order only by rounding; the CPU
+//     oracle replays this exact order.
 #include <climits>
 #include <vector>
 
@@ -166,23 +168,91 @@ template <bool HALF> struct CostElem;
 template <> struct CostElem<false> { using T = float; };
 template <> struct CostElem<true> { using T = __half; };
 
-enum { FIRST = 0, ACC = 1 };
-
-// Bytes one lane moves per pixel step: the cost slice, the group's partial sum (ACC), and the
-// reference pixel for the path gradient.
-template <int PPL, int MODE, bool HALF> struct Slots {
+// Per-lane cost slice of one chain step, and the ring stage of a warp: for each of its two
+// chains the 32 lanes' cost slices followed by 32 copies of the reference pixel.
+template <int PPL, bool HALF> struct Ring {
     static constexpr int CB = PPL * (int)sizeof(typename CostElem<HALF>::T);
-    static constexpr int SB = MODE == ACC ? PPL * 4 : 0;
-    static constexpr int LANE_B = CB + SB + 4;
-    static constexpr int STAGE_B = 32 * LANE_B;
+    static constexpr int CHAIN_B = 32 * CB + 32 * 4;
+    static constexpr int STAGE_B = 2 * CHAIN_B;
 };
 
-// One direction pass accumulating into the partial-sum volume of its group.
-template <int PPL, int MODE, bool HALF>
-__global__ void __launch_bounds__(WARPS * 32) sgm_dir_kernel(const SgmLaunch a, int dx, int dy, int group) {
+template <int PPL, bool HALF>
+__device__ __forceinline__ void load_slice(float (&cv)[PPL], const unsigned char* p) {
+    if constexpr (HALF) {
+        const __half2* hp = reinterpret_cast<const __half2*>(p);
+#pragma unroll
+        for (int j = 0; j < PPL / 2; ++j) {
+            const float2 v = __half22float2(hp[j]);
+            cv[2 * j] = v.x;
+            cv[2 * j + 1] = v.y;
+        }
+    } else {
+        load_planes<PPL>(cv, reinterpret_cast<const float*>(p));
+    }
+}
+
+// Recurrence state of one path along one scanline.
+template <int PPL> struct PathState {
+    float L[PPL];
+    float mprev, Iprev;
+};
+
+// One pixel step of a path (sgm.cu:57-108): L(p, d) = C(p, d) + min(L(p-r, d), L(p-r, d+-1) + P1,
+// min_k L(p-r, k) + P2) - min_k L(p-r, k), P1/P2 scaled by q1/q2 where the reference image's
+// path gradient is below tau; a plane never measured (cost -1) makes the pixel invalid: its
+// cost counts as 0 and the path's output there is COST_INF = 0.  o receives the output.
+template <int PPL>
+__device__ __forceinline__ void path_step(const SgmLaunch& a, PathState<PPL>& s, const float (&cv)[PPL], float I,
+                                          bool first, uint32_t incl, int lane, float (&o)[PPL]) {
+    bool neg = false;
+#pragma unroll
+    for (int j = 0; j < PPL; ++j) neg |= (((incl >> j) & 1u) && cv[j] < 0.0f);
+    const bool inv = __any_sync(kFull, neg);
+    float Ln[PPL];
+    if (first) {
+#pragma unroll
+        for (int j = 0; j < PPL; ++j) Ln[j] = inv ? 0.0f : cv[j];
+    } else {
+        // adaptive penalties from the path gradient of the reference image (sgm.cu:75-82)
+        const float D1 = fabsf(__fsub_rn(I, s.Iprev));
+        float P1 = a.p1, P2 = a.p2;
+        if (D1 < a.tau) { P1 = __fmul_rn(P1, a.q1); P2 = __fmul_rn(P2, a.q2); }
+        const float mP2 = __fadd_rn(s.mprev, P2);
+        float lm = __shfl_up_sync(kFull, s.L[PPL - 1], 1);
+        float lp = __shfl_down_sync(kFull, s.L[0], 1);
+        if (lane == 0) lm = inf_f();
+        if (lane == 31) lp = inf_f();
+        // min(L[d], minL + P2, L[d-1] + P1, L[d+1] + P1) (sgm.cu:85-92); min(a+P1, b+P1) is
+        // min(a, b) + P1 exactly because rounding is monotonic
+#pragma unroll
+        for (int j = 0; j < PPL; ++j) {
+            const float left = (j == 0) ? lm : s.L[j - 1];
+            const float right = (j == PPL - 1) ? lp : s.L[j + 1];
+            const float vv = min3f(s.L[j], mP2, __fadd_rn(fminf(left, right), P1));
+            Ln[j] = __fsub_rn(__fadd_rn(inv ? 0.0f : cv[j], vv), s.mprev);   // (:98)
+        }
+    }
+    s.Iprev = I;
+    float lmin = inf_f();
+#pragma unroll
+    for (int j = 0; j < PPL; ++j) {
+        s.L[j] = Ln[j];
+        if ((incl >> j) & 1u) lmin = fminf(lmin, Ln[j]);
+        o[j] = inv ? 0.0f : Ln[j];
+    }
+    s.mprev = warp_min_f32(lmin);
+}
+
+// A pair of opposite paths along the same scanlines: warp c takes scanline c of direction
+// (dx, dy) and walks it from both ends at once, the forward path into part[slot] and the
+// backward one into part[slot + 1].  The two recurrences are independent, so each warp keeps two
+// dependency chains in flight.  The cost slices and reference pixels of both ends are streamed
+// PF steps ahead with cp.async into a per-warp shared ring.
+template <int PPL, bool HALF>
+__global__ void __launch_bounds__(WARPS * 32) sgm_pair_kernel(const SgmLaunch a, int dx, int dy, int slot) {
     using CT = typename CostElem<HALF>::T;
-    using SL = Slots<PPL, MODE, HALF>;
-    constexpr int CB = SL::CB, SB = SL::SB, STAGE_B = SL::STAGE_B;
+    using RG = Ring<PPL, HALF>;
+    constexpr int CB = RG::CB, CHAIN_B = RG::CHAIN_B, STAGE_B = RG::STAGE_B;
     extern __shared__ __align__(16) unsigned char ring[];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -190,115 +260,61 @@ __global__ void __launch_bounds__(WARPS * 32) sgm_dir_kernel(const SgmLaunch a, 
     const int c = blockIdx.x * WARPS + warp;
     if (c >= num_chains(dx, dy, W, H)) return;        // warp-uniform; no block barriers below
     const Chain ch = chain_start(c, dx, dy, W, H);
+    const long step = (long)dy * W + dx;
+    const long pf0 = (long)ch.y * W + ch.x;             // forward start
+    const long pb0 = pf0 + (long)(ch.n - 1) * step;     // backward start (the forward end)
 
-    // stage layout: [cost slices of 32 lanes][partial slices of 32 lanes][32 ref values]
-    unsigned char* wbase = ring + (size_t)warp * PF * STAGE_B;
-    const int off_c = lane * CB;
-    const int off_s = 32 * CB + lane * SB;
-    const int off_i = 32 * (CB + SB) + lane * 4;
-
-    float* const part = a.part[group];
+    unsigned char* const wbase = ring + (size_t)warp * PF * STAGE_B;
     const CT* __restrict__ cost = reinterpret_cast<const CT*>(a.cost);
-    const long pstep = (long)dy * W + dx;
-    long pix = (long)ch.y * W + ch.x;
+    float* const outf = a.part[slot];
+    float* const outb = a.part[slot + 1];
 
-    auto issue = [&](unsigned char* sb, long q) {
-        const size_t e = (size_t)q * D + lane * PPL;
-        cp_async_bytes<CB>(sb + off_c, cost + e);
-        if constexpr (MODE == ACC) cp_async_bytes<SB>(sb + off_s, part + e);
-        cp_async_4(sb + off_i, a.ref + q);
+    auto issue = [&](unsigned char* sb, int k) {
+        const long qf = pf0 + k * step, qb = pb0 - k * step;
+        cp_async_bytes<CB>(sb + lane * CB, cost + (size_t)qf * D + lane * PPL);
+        cp_async_4(sb + 32 * CB + lane * 4, a.ref + qf);
+        cp_async_bytes<CB>(sb + CHAIN_B + lane * CB, cost + (size_t)qb * D + lane * PPL);
+        cp_async_4(sb + CHAIN_B + 32 * CB + lane * 4, a.ref + qb);
     };
 #pragma unroll 1
     for (int k = 0; k < PF; ++k) {
-        if (k < ch.n) issue(wbase + k * STAGE_B, pix + k * pstep);
+        if (k < ch.n) issue(wbase + k * STAGE_B, k);
         cp_async_commit();
     }
 
     const uint32_t incl = a.order.incl[lane];
-    float L[PPL];
+    PathState<PPL> fs, bs;
 #pragma unroll
-    for (int j = 0; j < PPL; ++j) L[j] = 0.0f;
-    float mprev = 0.0f, Iprev = 0.0f;
+    for (int j = 0; j < PPL; ++j) fs.L[j] = bs.L[j] = 0.0f;
+    fs.mprev = bs.mprev = fs.Iprev = bs.Iprev = 0.0f;
     int st = 0;
 
 #pragma unroll 1
     for (int k = 0; k < ch.n; ++k) {
         cp_async_wait<PF - 1>();
         unsigned char* sb = wbase + st * STAGE_B;
-        float cv[PPL];
-        if constexpr (HALF) {
-            const __half* hp = reinterpret_cast<const __half*>(sb + off_c);
-#pragma unroll
-            for (int j = 0; j < PPL; ++j) cv[j] = __half2float(hp[j]);
-        } else {
-            load_planes<PPL>(cv, reinterpret_cast<const float*>(sb + off_c));
-        }
-        float sv[PPL];
-        if constexpr (MODE == ACC) load_planes<PPL>(sv, reinterpret_cast<const float*>(sb + off_s));
-        const float I = *reinterpret_cast<const float*>(sb + off_i);
-
-        // a plane never measured (cost -1) marks the pixel invalid (sgm.cu:33,67)
-        bool neg = false;
-#pragma unroll
-        for (int j = 0; j < PPL; ++j) neg |= (((incl >> j) & 1u) && cv[j] < 0.0f);
-        const bool inv = __any_sync(kFull, neg);
-
-        float Ln[PPL];
-        if (k == 0) {
-#pragma unroll
-            for (int j = 0; j < PPL; ++j) Ln[j] = inv ? 0.0f : cv[j];
-        } else {
-            // adaptive penalties from the path gradient of the reference image (sgm.cu:75-82)
-            const float D1 = fabsf(__fsub_rn(I, Iprev));
-            float P1 = a.p1, P2 = a.p2;
-            if (D1 < a.tau) { P1 = __fmul_rn(P1, a.q1); P2 = __fmul_rn(P2, a.q2); }
-            const float mP2 = __fadd_rn(mprev, P2);
-            float lm = __shfl_up_sync(kFull, L[PPL - 1], 1);
-            float lp = __shfl_down_sync(kFull, L[0], 1);
-            if (lane == 0) lm = inf_f();
-            if (lane == 31) lp = inf_f();
-            // min(L[d], minL + P2, L[d-1] + P1, L[d+1] + P1) (sgm.cu:85-92); min(a+P1, b+P1) is
-            // min(a, b) + P1 exactly because rounding is monotonic
-#pragma unroll
-            for (int j = 0; j < PPL; ++j) {
-                const float left = (j == 0) ? lm : L[j - 1];
-                const float right = (j == PPL - 1) ? lp : L[j + 1];
-                const float vv = min3f(L[j], mP2, __fadd_rn(fminf(left, right), P1));
-                Ln[j] = __fsub_rn(__fadd_rn(inv ? 0.0f : cv[j], vv), mprev);   // (:98)
-            }
-        }
-        Iprev = I;
-        float lmin = inf_f();
-#pragma unroll
-        for (int j = 0; j < PPL; ++j) {
-            L[j] = Ln[j];
-            if ((incl >> j) & 1u) lmin = fminf(lmin, Ln[j]);
-        }
-        mprev = warp_min_f32(lmin);
-
-        // the output is set to COST_INF = 0 at an invalid pixel, else accumulated (:101-108)
-        float o[PPL];
-        if constexpr (MODE == FIRST) {
-#pragma unroll
-            for (int j = 0; j < PPL; ++j) o[j] = inv ? 0.0f : Ln[j];
-        } else {
-#pragma unroll
-            for (int j = 0; j < PPL; ++j) o[j] = inv ? 0.0f : __fadd_rn(sv[j], Ln[j]);
-        }
-        store_planes<PPL>(part + (size_t)pix * D + lane * PPL, o);
+        float cf[PPL], cb[PPL];
+        load_slice<PPL, HALF>(cf, sb + lane * CB);
+        load_slice<PPL, HALF>(cb, sb + CHAIN_B + lane * CB);
+        const float If = *reinterpret_cast<const float*>(sb + 32 * CB + lane * 4);
+        const float Ib = *reinterpret_cast<const float*>(sb + CHAIN_B + 32 * CB + lane * 4);
+        float of[PPL], ob[PPL];
+        path_step<PPL>(a, fs, cf, If, k == 0, incl, lane, of);
+        path_step<PPL>(a, bs, cb, Ib, k == 0, incl, lane, ob);
+        store_planes<PPL>(outf + (size_t)(pf0 + k * step) * D + lane * PPL, of);
+        store_planes<PPL>(outb + (size_t)(pb0 - k * step) * D + lane * PPL, ob);
         // refill this stage (consumed above) with step k + PF
-        if (k + PF < ch.n) issue(sb, pix + PF * pstep);
+        if (k + PF < ch.n) issue(sb, k + PF);
         cp_async_commit();
-        pix += pstep;
         st = (st + 1 == PF) ? 0 : st + 1;
     }
     cp_async_wait<0>();
 }
 
-// Sum of the four group partials, (S0 + S1) + (S2 + S3), then (FILTER) the winner-take-all or
-// (!FILTER) a store of the sum.  One warp per pixel, grid-stride; the next pixel's partials are
-// loaded before the current one is reduced.
-template <int PPL, bool FILTER>
+// Sum of the path volumes in the pairwise order (P0 + P1) + (P2 + P3) [+ ((P4 + P5) + (P6 + P7))],
+// then (FILTER) the winner-take-all or (!FILTER) a store of the sum.  One warp per pixel,
+// grid-stride; the next pixel's path slices are loaded before the current one is reduced.
+template <int PPL, bool FILTER, int NP>
 __global__ void __launch_bounds__(256) combine_kernel(const SgmLaunch a) {
     const int lane = threadIdx.x & 31;
     const long nw = (long)gridDim.x * (blockDim.x >> 5);
@@ -307,19 +323,25 @@ __global__ void __launch_bounds__(256) combine_kernel(const SgmLaunch a) {
     uint32_t incl;
     uint16_t rk[PPL];
     lane_order<PPL>(a.order, lane, incl, rk);
-    auto load4 = [&](long pix, float (&s)[4][PPL]) {
+    auto loadp = [&](long pix, float (&s)[NP][PPL]) {
         const size_t e = (size_t)pix * D + lane * PPL;
 #pragma unroll
-        for (int g = 0; g < 4; ++g) load_planes<PPL>(s[g], a.part[g] + e);
+        for (int g = 0; g < NP; ++g) load_planes<PPL>(s[g], a.part[g] + e);
     };
     long pix = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    float cur[4][PPL], nxt[4][PPL];
-    if (pix < npix) load4(pix, cur);
+    float cur[NP][PPL], nxt[NP][PPL];
+    if (pix < npix) loadp(pix, cur);
     for (; pix < npix; pix += nw) {
-        if (pix + nw < npix) load4(pix + nw, nxt);
+        if (pix + nw < npix) loadp(pix + nw, nxt);
         float o[PPL];
 #pragma unroll
-        for (int j = 0; j < PPL; ++j) o[j] = __fadd_rn(__fadd_rn(cur[0][j], cur[1][j]), __fadd_rn(cur[2][j], cur[3][j]));
+        for (int j = 0; j < PPL; ++j) {
+            const float s4 = __fadd_rn(__fadd_rn(cur[0][j], cur[1][j]), __fadd_rn(cur[2][j], cur[3][j]));
+            if constexpr (NP == 8)
+                o[j] = __fadd_rn(s4, __fadd_rn(__fadd_rn(cur[4][j], cur[5][j]), __fadd_rn(cur[6][j], cur[7][j])));
+            else
+                o[j] = s4;
+        }
         if (a.total) store_planes<PPL>(a.total + (size_t)pix * D + lane * PPL, o);
         if constexpr (FILTER) {
             float depth;
@@ -333,7 +355,7 @@ __global__ void __launch_bounds__(256) combine_kernel(const SgmLaunch a) {
             }
         }
 #pragma unroll
-        for (int g = 0; g < 4; ++g)
+        for (int g = 0; g < NP; ++g)
 #pragma unroll
             for (int j = 0; j < PPL; ++j) cur[g][j] = nxt[g][j];
     }
@@ -361,19 +383,21 @@ __global__ void __launch_bounds__(128) filter_kernel(const float* __restrict__ s
     }
 }
 
+// Path r of the reference order (L->R, R->L, T->B, B->T, then TL->BR, BR->TL, TR->BL, BL->TR);
+// pair p = paths (2p, 2p+1) runs as one sgm_pair_kernel along direction kDirs[2p].
 const int kDirs[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1}, {-1, 1}, {1, -1}};
 
-template <int PPL, int MODE, bool HALF>
-cudaError_t launch_dir(const SgmLaunch& a, int dir, int group, cudaStream_t s) {
-    const size_t smem = (size_t)WARPS * PF * Slots<PPL, MODE, HALF>::STAGE_B;
-    auto kern = sgm_dir_kernel<PPL, MODE, HALF>;
+template <int PPL, bool HALF>
+cudaError_t launch_pair(const SgmLaunch& a, int pair, cudaStream_t s) {
+    const size_t smem = (size_t)WARPS * PF * Ring<PPL, HALF>::STAGE_B;
+    auto kern = sgm_pair_kernel<PPL, HALF>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    const int dx = kDirs[dir][0], dy = kDirs[dir][1];
+    const int dx = kDirs[2 * pair][0], dy = kDirs[2 * pair][1];
     const int nch = num_chains(dx, dy, a.W, a.H);
-    kern<<<(nch + WARPS - 1) / WARPS, WARPS * 32, smem, s>>>(a, dx, dy, group);
+    kern<<<(nch + WARPS - 1) / WARPS, WARPS * 32, smem, s>>>(a, dx, dy, 2 * pair);
     return cudaGetLastError();
 }
 
@@ -385,38 +409,35 @@ cudaError_t launch_combine(const SgmLaunch& a, bool fuse_filter, cudaStream_t s)
     const long npix = (long)a.W * a.H;
     const long blocks_needed = (npix + 7) / 8;   // 8 warps per block
     const int blocks = (int)(blocks_needed < (long)sms * 8 ? blocks_needed : (long)sms * 8);
-    if (fuse_filter) combine_kernel<PPL, true><<<blocks, 256, 0, s>>>(a);
-    else combine_kernel<PPL, false><<<blocks, 256, 0, s>>>(a);
+    const bool eight = a.num_paths == 8;
+    if (fuse_filter && eight) combine_kernel<PPL, true, 8><<<blocks, 256, 0, s>>>(a);
+    else if (fuse_filter) combine_kernel<PPL, true, 4><<<blocks, 256, 0, s>>>(a);
+    else if (eight) combine_kernel<PPL, false, 8><<<blocks, 256, 0, s>>>(a);
+    else combine_kernel<PPL, false, 4><<<blocks, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 
-// Groups g = 0..3 hold paths {g} (4-path mode) or {g, g+4} (8-path mode).  Groups 0..2 run on
-// their own streams when `side` is given; group 3 runs on `s`, which then joins the others and
-// runs the combine / winner-take-all kernel.
+// Path pairs p = 0 .. num_paths/2 - 1: pairs 0..np-2 run on their own side streams when `side`
+// is given, the last on `s`, which then joins the others and runs the combine kernel.
 template <int PPL, bool HALF>
 cudaError_t launch_sgm_t(const SgmLaunch& a, bool fuse_filter, cudaStream_t s, const SgmStreams* side) {
-    const bool eight = a.num_paths == 8;
+    const int np = a.num_paths / 2;
     cudaError_t e = cudaSuccess;
-    auto group_passes = [&](int g, cudaStream_t gs) -> cudaError_t {
-        cudaError_t r = launch_dir<PPL, FIRST, HALF>(a, g, g, gs);
-        if (r == cudaSuccess && eight) r = launch_dir<PPL, ACC, HALF>(a, g + 4, g, gs);
-        return r;
-    };
     if (side) {
         if ((e = cudaEventRecord(side->fork, s)) != cudaSuccess) return e;
-        for (int g = 0; g < 3; ++g) {
-            if ((e = cudaStreamWaitEvent(side->stream[g], side->fork, 0)) != cudaSuccess) return e;
-            if ((e = group_passes(g, side->stream[g])) != cudaSuccess) return e;
-            if ((e = cudaEventRecord(side->join[g], side->stream[g])) != cudaSuccess) return e;
+        for (int p = 0; p < np - 1; ++p) {
+            if ((e = cudaStreamWaitEvent(side->stream[p], side->fork, 0)) != cudaSuccess) return e;
+            if ((e = launch_pair<PPL, HALF>(a, p, side->stream[p])) != cudaSuccess) return e;
+            if ((e = cudaEventRecord(side->join[p], side->stream[p])) != cudaSuccess) return e;
         }
     } else {
-        for (int g = 0; g < 3 && e == cudaSuccess; ++g) e = group_passes(g, s);
+        for (int p = 0; p < np - 1 && e == cudaSuccess; ++p) e = launch_pair<PPL, HALF>(a, p, s);
         if (e != cudaSuccess) return e;
     }
-    if ((e = group_passes(3, s)) != cudaSuccess) return e;
+    if ((e = launch_pair<PPL, HALF>(a, np - 1, s)) != cudaSuccess) return e;
     if (side)
-        for (int g = 0; g < 3; ++g)
-            if ((e = cudaStreamWaitEvent(s, side->join[g], 0)) != cudaSuccess) return e;
+        for (int p = 0; p < np - 1; ++p)
+            if ((e = cudaStreamWaitEvent(s, side->join[p], 0)) != cudaSuccess) return e;
     return launch_combine<PPL>(a, fuse_filter, s);
 }
 

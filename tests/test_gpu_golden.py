@@ -53,7 +53,7 @@ def test_sgm_on_reference_cost(pm_lib, g, case):
     cost = torch.from_numpy(g[f"{case}_cost"]).cuda()
     ref = scaled(g, "ref_u8", scale)
     out = torch.empty_like(cost)
-    part = torch.empty((3,) + tuple(cost.shape), dtype=torch.float32, device="cuda")
+    part = torch.empty((p.num_paths - 1,) + tuple(cost.shape), dtype=torch.float32, device="cuda")
     cfg = config(p)
     assert pm_lib.pm_stage_sgm(ctypes.byref(cfg), vp(cost), vp(ref), vp(out), vp(part), None) == 0
     torch.cuda.synchronize()

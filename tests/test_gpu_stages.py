@@ -107,7 +107,7 @@ def test_sgm_and_filter_bit_exact(pm_lib, D, paths, compat, uniq):
     rf, _ = upload_images(pm_lib, fs, p.intensity_scale)
     dcost = torch.from_numpy(cost).cuda()
     out = torch.empty_like(dcost)
-    part = torch.empty((3,) + tuple(dcost.shape), dtype=torch.float32, device="cuda")
+    part = torch.empty((p.num_paths - 1,) + tuple(dcost.shape), dtype=torch.float32, device="cuda")
     cfg = config(p)
     assert pm_lib.pm_stage_sgm(ctypes.byref(cfg), vp(dcost), vp(rf), vp(out), vp(part), None) == 0
     depth = torch.empty((p.H, p.W), dtype=torch.float32, device="cuda")
@@ -124,7 +124,7 @@ def test_sgm_and_filter_bit_exact(pm_lib, D, paths, compat, uniq):
     p.sum_order = 1
     np.testing.assert_allclose(seq_sum, want_sum, rtol=2e-6, atol=1e-6)
     # fused last path + filter gives the same depth and index
-    scratch = torch.empty((4,) + tuple(dcost.shape), dtype=torch.float32, device="cuda")
+    scratch = torch.empty((p.num_paths,) + tuple(dcost.shape), dtype=torch.float32, device="cuda")
     depth2 = torch.zeros((p.H, p.W + 3), dtype=torch.float32, device="cuda")   # pitched output
     idx2 = torch.empty((p.H, p.W), dtype=torch.int32, device="cuda")
     assert pm_lib.pm_stage_sgm_filter(ctypes.byref(cfg), vp(dcost), vp(rf), vp(scratch), vp(depth2),
