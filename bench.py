@@ -1,17 +1,20 @@
 #!/usr/bin/env python
 """Benchmark of the motion-stereo depth-map pipeline on B200.
 
-One step = one depth map: a reference frame plus S source frames (cost volume), 8-path SGM,
-winner-take-all / flatness / uniqueness / subpixel, and one Bayesian fusion step against the
-previous keyframe's state.  Workload: 640x480, 128 inverse-depth planes uniform in
+One step = one depth map per sequence: a reference frame plus S source frames (cost volume),
+8-path SGM, winner-take-all / flatness / uniqueness / subpixel, and one Bayesian fusion step
+against the previous keyframe's state.  Workload: 640x480, 128 inverse-depth planes uniform in
 [0.1, 2.0] 1/m, 5 sources, f = 520, seeded synthetic scenes (six textured planes).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision fp32|fp16]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--form batched|plain] [--precision fp16|fp32] [--batch B]
 
-`value` is depth maps/s with inputs resident in HBM; `e2e` is the same through the public
-C ABI from pinned host buffers (uploads of the six uint8 frames and downloads of the fused
-depth and variance inside the timed region).  Under torchrun every rank maps its own
-sequence (no collective on the data path) and the slowest rank's time is used.
+Default (the headline): the FP16 form, B sequences batched (one CUDA-graph launch per step for
+all B), against the plain FP32 form (one StereoMapper, one map after the other) measured in the
+same run.  `value` is depth maps/s with inputs resident in HBM; `e2e` is the same through the
+public C ABI with pinned host frames and outputs copied inside the timed region.  Under
+torchrun every rank maps its own sequences (no collective on the data path) and the slowest
+rank's time is used.
 """
 from __future__ import annotations
 
@@ -137,12 +140,13 @@ def make_mapper(precision: int, device: int, cost_mode: int = 0):
 
 def algorithmic_bytes(e: int):
     """Per depth map: B_alg = (S+1) N + 3 e V + 8 V + 60 N (path-grouped lower bound), and the
-    bytes the SGM direction passes of this implementation must move (C read per pass, partial
-    sum written by the first pass, read+written by the middle ones, read by the last)."""
+    bytes the SGM stage of this implementation must move."""
     N = W * H
     V = N * D
     b_alg = (S + 1) * N + 3 * e * V + 8 * V + 60 * N
-    sgm_pass = PATHS * e * V + (1 + 2 * (PATHS - 2) + 1) * 4 * V + PATHS * 4 * N + 4 * N
+    # every path reads C and the reference image and writes its FP32 path volume; the combine
+    # reads the path volumes and writes depth and index
+    sgm_pass = PATHS * (e * V + 4 * V + 4 * N) + PATHS * 4 * V + 8 * N
     return b_alg, sgm_pass
 
 
@@ -159,7 +163,9 @@ def cost_kernel_work(e: int):
     return FLOP_PER_VOXEL_SOURCE * V * S, e * V + 4 * N + 16 * N * S
 
 
-def run_ours(args, rank, world):
+def run_ours(args, rank, world, precision: str = "fp32", passes=("dev", "e2e", "stage")):
+    """The plain form: one StereoMapper, one depth map after the other (device-resident frames for
+    `dev` and the stage times, pinned host frames for `e2e`)."""
     import torch
     from probabilistic_mapping_b200 import scene
     dev = int(os.environ.get("LOCAL_RANK", "0"))
@@ -167,7 +173,7 @@ def run_ours(args, rank, world):
     seq = scene.make_sequence(W, H, F_PX, S, N_KEYFRAMES, seed=1000 + rank)
     K = seq[0].K
     fx, fy, cx, cy = K[0, 0], K[1, 1], K[0, 2], K[1, 2]
-    prec = 1 if args.precision == "fp16" else 0
+    prec = 1 if precision == "fp16" else 0
     m, drho = make_mapper(prec, dev, 1 if args.cost_mode == "corrected" else 0)
     m.initIntrinsic(K, 0.0, drho)
     stream = torch.cuda.Stream(device=dev)
@@ -217,18 +223,84 @@ def run_ours(args, rank, world):
         m.enable_stage_timing(False)
         return e0.elapsed_time(e1), stage / args.steps
 
-    with ClockSampler(dev) as clk:
-        t_dev, _ = timed(d_ref, d_src, d_depth, d_var)
-    t_e2e, _ = timed(h_ref, h_src, h_depth, h_var)
-    # per-stage CUDA-event times (separate pass; the stage events synchronise every step)
-    _, stage_ms = timed(d_ref, d_src, d_depth, d_var, stage_timing=True)
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_dev, t_e2e = t.tolist()
+    t_dev = t_e2e = 0.0
+    stage_ms = np.zeros(4)
+    clk = ClockSampler(dev)
+    if "dev" in passes:
+        with clk:
+            t_dev, _ = timed(d_ref, d_src, d_depth, d_var)
+    if "e2e" in passes:
+        t_e2e, _ = timed(h_ref, h_src, h_depth, h_var)
+    if "stage" in passes:
+        # per-stage CUDA-event times (separate pass; the stage events synchronise every step)
+        _, stage_ms = timed(d_ref, d_src, d_depth, d_var, stage_timing=True)
+    t_dev, t_e2e = max_over_ranks([t_dev, t_e2e], world)
     m.close()
-    return t_dev, t_e2e, stage_ms, clk.summary()
+    return t_dev, t_e2e, stage_ms, clk.summary() if "dev" in passes else None
+
+
+def max_over_ranks(vals, world):
+    if world <= 1:
+        return vals
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def run_batched(args, rank, world, precision: str, B: int, host_io: bool, clocks: bool):
+    """B sequences of the bench workload in one pm_batch: each step is one CUDA-graph launch that
+    maps every sequence.  The two frame sets of the batch hold keyframes 0 and 1 of each
+    sequence (device memory, or pinned host memory copied inside the graph with host_io); the
+    steps alternate between them with the matching poses."""
+    import torch
+    from probabilistic_mapping_b200 import _lib, scene
+    from probabilistic_mapping_b200.batch import StereoBatch
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    rho0, drho = scene.plane_range(D)
+    prec = _lib.PM_PREC_FP16 if precision == "fp16" else _lib.PM_PREC_FP32
+    cfg = dict(width=W, height=H, num_planes=D, rho0=rho0, intensity_scale=1 / 255, num_paths=PATHS, p1=P1, p2=P2,
+               tau_so=TAU, uniqueness_ratio=UNIQ, cost_mode=1 if args.cost_mode == "corrected" else 0,
+               precision=prec, device=dev)
+    seqs = [scene.make_sequence(W, H, F_PX, S, 2, seed=2000 + 97 * rank + i) for i in range(B)]
+    b = StereoBatch([cfg] * B, S, lanes=0, host_io=host_io, autotune=True)
+    for i in range(B):
+        b.init_intrinsic(i, seqs[i][0].K, drho)
+
+    def feed(step):
+        k = step % 2
+        for i in range(B):
+            fs = seqs[i][k]
+            if step < 2:   # frames stay in the batch's buffer set k after the first two steps
+                b.set_frame(i, 0, fs.ref)
+                for s in range(S):
+                    b.set_frame(i, 1 + s, fs.srcs[s])
+            b.set_poses(i, fs.R_ref, fs.T_ref, list(fs.R_srcs), list(fs.T_srcs))
+
+    for i in range(args.warmup):
+        feed(i)
+        b.run()
+    b.synchronize()
+    stream = torch.cuda.ExternalStream(b.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(dev) if clocks else None
+    if sampler:
+        sampler.__enter__()
+    e0.record(stream)
+    for i in range(args.steps):
+        feed(args.warmup + i)
+        b.run()
+    e1.record(stream)
+    b.synchronize()
+    if sampler:
+        sampler.__exit__(None, None, None)
+    t = e0.elapsed_time(e1)
+    tuning = b.tuning(0)
+    b.close()
+    t = max_over_ranks([t], world)[0]
+    return t, (sampler.summary() if sampler else None), tuning
 
 
 def cpu_baseline_sample(threads: int | None = None, maps: int = 1):
@@ -266,7 +338,10 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp32", "fp16"], default="fp32")
+    ap.add_argument("--form", choices=["batched", "plain"], default="batched")
+    ap.add_argument("--precision", choices=["fp32", "fp16"], default=None,
+                    help="precision of the measured form (default: fp16 batched, fp32 plain)")
+    ap.add_argument("--batch", type=int, default=16, help="sequences per batch (batched form)")
     ap.add_argument("--cost-mode", choices=["reference", "corrected"], default="reference")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -275,8 +350,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
 
     if args.impl == "reference":
-        # The reference's CUDA does not build on CUDA 12 (texture references) and its CPU
-        # fusion variant needs OpenCV/ROS; its path is timed through the FP64 CPU port.
+        # The reference implements this path only in CUDA (its host code adds the CPU fusion
+        # variant alone), so its CPU arm is the FP64 port of that CUDA, on all host cores.
         if rank != 0:
             return
         warm = max(0, min(args.warmup, 1))
@@ -302,9 +377,32 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
-    t_dev, t_e2e, stage_ms, clocks = run_ours(args, rank, world)
-    value = world * args.steps / (t_dev / 1000.0)
-    e2e = world * args.steps / (t_e2e / 1000.0)
+    if args.precision is None:
+        args.precision = "fp16" if args.form == "batched" else "fp32"
+    # the plain FP32 form, always measured: the baseline of the batched form's speed-up and the
+    # source of the per-kernel stage times
+    t_plain, t_plain_e2e, stage_ms, clocks_plain = run_ours(args, rank, world, "fp32")
+    plain_value = world * args.steps / (t_plain / 1000.0)
+    plain_e2e = world * args.steps / (t_plain_e2e / 1000.0)
+    if args.form == "batched":
+        B = args.batch
+        t_b, clocks, tuning = run_batched(args, rank, world, args.precision, B, host_io=False, clocks=True)
+        t_be, _, _ = run_batched(args, rank, world, args.precision, B, host_io=True, clocks=False)
+        value = world * B * args.steps / (t_b / 1000.0)
+        e2e = world * B * args.steps / (t_be / 1000.0)
+        ms_per_step = t_b / args.steps
+        if args.precision == "fp16":   # stage times of the FP16 form's kernels (plain mapper)
+            _, _, stage_ms, _ = run_ours(args, rank, world, "fp16", passes=("stage",))
+    else:
+        B = 1
+        tuning = None
+        if args.precision == "fp32":
+            t_dev, t_e2e, clocks = t_plain, t_plain_e2e, clocks_plain
+        else:
+            t_dev, t_e2e, stage_ms, clocks = run_ours(args, rank, world, args.precision)
+        value = world * args.steps / (t_dev / 1000.0)
+        e2e = world * args.steps / (t_e2e / 1000.0)
+        ms_per_step = t_dev / args.steps
     e = 2 if args.precision == "fp16" else 4
     b_alg, sgm_bytes = algorithmic_bytes(e)
     peak_hbm, sm_mhz, peak_kind = peaks()
@@ -314,40 +412,48 @@ def main():
     cost_tflops = cost_flop / (cost_ms / 1000.0) / 1e12 if cost_ms > 0 else None
     cost_gbs = cost_bytes / (cost_ms / 1000.0) / 1e9 if cost_ms > 0 else None
     sgm_gbs = sgm_bytes / (sgm_ms / 1000.0) / 1e9 if sgm_ms > 0 else None
-    map_s = t_dev / args.steps / 1000.0
-    # to_float (reference) + to_quad (S sources), cost, 2 passes x 4 path groups (8 paths) or
-    # 1 x 4, combine + winner-take-all, fusion transform + update
-    launches_per_step = 1 + S + 1 + PATHS + 1 + 2
+    map_s = 1.0 / (value / world)   # seconds per map per GPU
+    # to_float (reference) + to_quad (S sources), cost, one kernel per opposite-path pair,
+    # combine + winner-take-all, fusion transform + update
+    launches_per_map = 1 + S + 1 + PATHS // 2 + 1 + 2
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "depth maps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_dev / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if e == 4 else "f16", "data": "synthetic",
             "config": {"workload": f"{W}x{H}, {D} planes, {S} sources, {PATHS}-path SGM, uniqueness {UNIQ}, "
-                                   f"fusion step; {args.precision} form, {args.cost_mode} cost samples",
-                       "global_batch": world, "seq_len": 0, "parallelism": f"replicas x{world}",
-                       "l2": "per-map working set (cost + partial-sum volumes, 315 MB FP32) exceeds the 126 MB L2"},
-            # the dominant kernel (cost_kernel, ~2/3 of the map) is FP32-ALU-bound, not HBM-bound
+                                   f"fusion step; {args.precision} {args.form} form"
+                                   + (f", {B} sequences per CUDA-graph launch" if args.form == "batched" else "")
+                                   + f", {args.cost_mode} cost samples",
+                       "global_batch": world * B, "seq_len": 0, "parallelism": f"replicas x{world}",
+                       "l2": "per-map working set (cost + path volumes, >1 GB) exceeds the 126 MB L2"},
+            "plain_fp32": {"value": plain_value, "e2e": plain_e2e, "ms_per_map": t_plain / args.steps,
+                           "unit": "depth maps/s"},
+            "speedup_vs_plain_fp32": value / plain_value,
+            # the dominant kernel (cost_kernel, ~2/3 of a map) is FP32-ALU-bound, not HBM-bound
             "roofline": {"bound": "fp32", "kernel": "cost_kernel", "achieved": cost_tflops, "peak": peak_fp32,
                          "unit": "TFLOP/s", "frac": (cost_tflops / peak_fp32) if cost_tflops else None,
-                         "traffic": ncu_traffic("cost_kernel"), "ms_per_launch": cost_ms,
+                         "traffic": ncu_traffic("cost_kernel") if e == 4 else None, "ms_per_launch": cost_ms,
                          "algorithmic_flop_per_launch": cost_flop, "algorithmic_bytes_per_launch": cost_bytes,
                          "hbm_achieved_gbs": cost_gbs, "hbm_frac": (cost_gbs / peak_hbm) if cost_gbs else None,
+                         "precision": args.precision,
                          "peak_kind": f"derived: 148 SM x 128 lanes x 2 flop x {sm_mhz:.0f} MHz ({peak_kind} clock)"},
-            "roofline_sgm": {"bound": "hbm", "kernel": "sgm direction passes + combine/winner-take-all",
+            "roofline_sgm": {"bound": "hbm", "kernel": "sgm_pair_kernel x 4 + combine_kernel (winner-take-all)",
                              "achieved": sgm_gbs, "peak": peak_hbm, "unit": "GB/s",
                              "frac": (sgm_gbs / peak_hbm) if sgm_gbs else None,
                              "algorithmic_bytes_per_map": sgm_bytes, "ms": sgm_ms, "peak_kind": peak_kind},
-            "map_roofline": {"b_alg_bytes": b_alg, "f_alg_flop": cost_flop, "ms": t_dev / args.steps,
+            "map_roofline": {"b_alg_bytes": b_alg, "f_alg_flop": cost_flop, "ms_per_map_per_gpu": map_s * 1000,
                              "frac_of_hbm": b_alg / map_s / 1e9 / peak_hbm,
                              "frac_of_fp32": cost_flop / map_s / 1e12 / peak_fp32},
             "stage_ms": {"cost": cost_ms, "sgm_wta": sgm_ms, "fusion": float(stage_ms[2]),
-                         "copy_out": float(stage_ms[3])},
-            "e2e": {"value": e2e, "unit": "depth maps/s", "h2d_bytes_per_step": (S + 1) * W * H,
-                    "d2h_bytes_per_step": 2 * 4 * W * H},
-            "gpu_launches": launches_per_step * args.steps,
+                         "copy_out": float(stage_ms[3]), "source": f"plain {args.precision} mapper, CUDA events"},
+            "e2e": {"value": e2e, "unit": "depth maps/s", "h2d_bytes_per_step": B * (S + 1) * W * H,
+                    "d2h_bytes_per_step": B * 2 * 4 * W * H},
+            "gpu_launches": launches_per_map * B * args.steps,
             "clocks": clocks,
         }
+        if tuning:
+            line["sgm_schedule"] = {"pair_warps": tuning[0], "serial_pairs": tuning[1], "tuned_ms": tuning[2]}
         if not args.no_cpu_baseline:
             rate, cores = cpu_baseline_sample(maps=3)
             line["cpu_baseline"] = {"value": rate, "unit": "depth maps/s", "cores": cores, "kind": "port",

@@ -172,6 +172,50 @@ PM_API const char* pm_last_error(const pm_mapper* h);
 PM_API const char* pm_status_string(pm_status s);
 
 /* ---------------------------------------------------------------------------------------
+ * Batched form (no counterpart in the reference): many independent sequences, each with its
+ * own pm_config (resolution, planes, precision, parameters), stepped together.  One
+ * pm_batch_run is one keyframe of every sequence -- initReference(frame 0), pm_update of frames
+ * 1..num_sources with their poses, then outputFusion(R_ref, T_ref) -- exactly the StereoMapper
+ * calls, issued as ONE CUDA-graph launch in which the sequences are independent branches.
+ * Sequences of the same shape share `lanes` sets of cost and path volumes (0: one set each).
+ * Two buffer sets alternate by step, so frames for step t+1 can be written while step t runs.
+ * The texture sampler and the CPU fusion variant are not available in a batch.
+ * --------------------------------------------------------------------------------------- */
+typedef struct pm_batch pm_batch;
+#define PM_BATCH_HOST_IO 1  /* frames in and fused depth/variance out through batch-owned pinned
+                               host buffers, copied inside the graph; else device buffers */
+#define PM_BATCH_AUTOTUNE 2 /* time the SGM schedules for each distinct shape at creation */
+PM_API pm_status pm_batch_create(const pm_config* cfgs, int num_sequences, int num_sources, int lanes, int flags,
+                                 pm_batch** out);
+PM_API void pm_batch_destroy(pm_batch* b);
+PM_API pm_status pm_batch_init_intrinsic(pm_batch* b, int seq, const double K[9], float dep_sample);
+/* Buffer of frame f (0 = reference, 1..num_sources = sources) of sequence seq for the next
+ * pm_batch_run: W*H uint8, row pitch W, host memory with PM_BATCH_HOST_IO, else device. */
+PM_API pm_status pm_batch_frame(pm_batch* b, int seq, int frame, uint8_t** ptr);
+/* Copies a W*H uint8 frame (host or device memory, row pitch in bytes, 0 = W) into that buffer. */
+PM_API pm_status pm_batch_put_frame(pm_batch* b, int seq, int frame, const uint8_t* img, size_t pitch);
+/* Poses of the next step: reference frame and the num_sources source frames (R_src 9 doubles
+ * and T_src 3 doubles per source, row-major, as pm_update). */
+PM_API pm_status pm_batch_set_poses(pm_batch* b, int seq, const double R_ref[9], const double T_ref[3],
+                                    const double* R_src, const double* T_src);
+PM_API pm_status pm_batch_run(pm_batch* b);
+PM_API pm_status pm_batch_synchronize(pm_batch* b);
+/* Fused depth and variance (W*H float) of the last step of sequence seq, after
+ * pm_batch_synchronize: pinned host buffers with PM_BATCH_HOST_IO, device buffers otherwise. */
+PM_API pm_status pm_batch_output(pm_batch* b, int seq, const float** depth, const float** variance);
+/* Copies them into caller buffers (host or device, byte pitches, 0 = packed) after waiting for
+ * the batch's stream. */
+PM_API pm_status pm_batch_copy_output(pm_batch* b, int seq, float* depth, size_t pitch, float* variance,
+                                      size_t var_pitch);
+/* Winner-take-all depth (device, W*H float) of the last step of sequence seq. */
+PM_API pm_status pm_batch_wta_depth(pm_batch* b, int seq, const float** depth);
+/* SGM schedule of sequence seq: scanlines per block of the path-pair kernel, serial (1) or
+ * concurrent (0) path pairs, and the stage time the autotuner measured (ms; 0 if untuned). */
+PM_API pm_status pm_batch_tuning(pm_batch* b, int seq, int* pair_warps, int* serial_pairs, float* ms);
+PM_API void* pm_batch_stream(pm_batch* b);
+PM_API const char* pm_batch_last_error(const pm_batch* b);
+
+/* ---------------------------------------------------------------------------------------
  * Stage-level calls: one call per reference launch wrapper.  Device pointers, caller-owned
  * buffers, asynchronous on `stream`.  Status codes report argument errors and launch errors.
  * --------------------------------------------------------------------------------------- */

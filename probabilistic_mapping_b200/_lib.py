@@ -24,6 +24,8 @@ PM_PREC_FP32 = 0
 PM_PREC_FP16 = 1
 PM_SAMPLER_EXACT = 0
 PM_SAMPLER_TEXTURE = 1
+PM_BATCH_HOST_IO = 1
+PM_BATCH_AUTOTUNE = 2
 PM_FUSION_GPU = 0
 PM_FUSION_CPU_PATH = 1
 
@@ -83,6 +85,20 @@ SIGNATURES = {
     "pm_stage_convert": (_I, [_I, _I, _VP, _VP, _I, _SZ, _VP]),
     "pm_stage_depth_fuse_noalloc": (_I, [_I, _I, _P(ctypes.c_float), _P(ctypes.c_float), _VP, _P(_VP),
                                          _P(_VP), _VP, _VP]),
+    "pm_batch_create": (_I, [_P(PmConfig), _I, _I, _I, _I, _P(_VP)]),
+    "pm_batch_destroy": (None, [_VP]),
+    "pm_batch_init_intrinsic": (_I, [_VP, _I, _D, _F]),
+    "pm_batch_frame": (_I, [_VP, _I, _I, _P(_VP)]),
+    "pm_batch_put_frame": (_I, [_VP, _I, _I, _VP, _SZ]),
+    "pm_batch_set_poses": (_I, [_VP, _I, _D, _D, _D, _D]),
+    "pm_batch_run": (_I, [_VP]),
+    "pm_batch_synchronize": (_I, [_VP]),
+    "pm_batch_output": (_I, [_VP, _I, _P(_VP), _P(_VP)]),
+    "pm_batch_copy_output": (_I, [_VP, _I, _VP, _SZ, _VP, _SZ]),
+    "pm_batch_wta_depth": (_I, [_VP, _I, _P(_VP)]),
+    "pm_batch_tuning": (_I, [_VP, _I, _P(_I), _P(_I), _P(_F)]),
+    "pm_batch_stream": (_VP, [_VP]),
+    "pm_batch_last_error": (ctypes.c_char_p, [_VP]),
 }
 
 _lib = None

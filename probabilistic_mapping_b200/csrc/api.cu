@@ -67,6 +67,65 @@ struct pm_mapper {
     bool ev_valid[PM_NUM_STAGES] = {};
 };
 
+namespace pm {
+
+void matmul3(const double* A, const double* B, double* C) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double s = 0;
+            for (int k = 0; k < 3; ++k) s += A[3 * i + k] * B[3 * k + j];
+            C[3 * i + j] = s;
+        }
+}
+void matvec3(const double* A, const double* x, double* y) {
+    for (int i = 0; i < 3; ++i) {
+        double s = 0;
+        for (int k = 0; k < 3; ++k) s += A[3 * i + k] * x[k];
+        y[i] = s;
+    }
+}
+void transpose3(const double* A, double* T) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) T[3 * j + i] = A[3 * i + j];
+}
+bool finite_n(const double* v, int n) {
+    for (int i = 0; i < n; ++i)
+        if (!std::isfinite(v[i])) return false;
+    return true;
+}
+
+// H1 = K R_r^T R_l K^-1, H2 = K R_r^T (T_l - T_r) in FP64 (stereo_mapper.cpp:79-80), with the
+// closed-form inverse of the upper-triangular K.
+void compose_homography(const double* K, const double* Rl, const double* Tl, const double* Rr,
+                        const double* Tr, float out[12]) {
+    const double fx = K[0], s = K[1], cx = K[2], fy = K[4], cy = K[5];
+    const double Ki[9] = {1.0 / fx, -s / (fx * fy), (s * cy - cx * fy) / (fx * fy), 0.0, 1.0 / fy, -cy / fy,
+                          0.0, 0.0, 1.0};
+    double RrT[9], A[9], B[9], H1[9];
+    transpose3(Rr, RrT);
+    matmul3(K, RrT, A);
+    matmul3(A, Rl, B);
+    matmul3(B, Ki, H1);
+    const double dT[3] = {Tl[0] - Tr[0], Tl[1] - Tr[1], Tl[2] - Tr[2]};
+    double H2[3];
+    matvec3(A, dT, H2);
+    for (int i = 0; i < 9; ++i) out[i] = (float)H1[i];
+    for (int i = 0; i < 3; ++i) out[9 + i] = (float)H2[i];
+}
+
+// R_p2c = R^T R_prev, t_p2c = R^T (t_prev - t) (stereo_mapper.cpp:155-156), as floats.
+void fusion_pose(const double* R, const double* t, const double* R_prev, const double* t_prev, float out[12]) {
+    double RT[9], Rpc[9], tpc[3];
+    transpose3(R, RT);
+    matmul3(RT, R_prev, Rpc);
+    const double dt[3] = {t_prev[0] - t[0], t_prev[1] - t[1], t_prev[2] - t[2]};
+    matvec3(RT, dt, tpc);
+    for (int i = 0; i < 9; ++i) out[i] = (float)Rpc[i];
+    for (int i = 0; i < 3; ++i) out[9 + i] = (float)tpc[i];
+}
+
+}  // namespace pm
+
 namespace {
 
 pm_status fail(pm_mapper* h, pm_status s, const char* fmt, ...) {
@@ -133,50 +192,6 @@ pm_status check_config(const pm_config* c, pm_mapper* h) {
     if (!(c->rho_step > 0.0f) || !std::isfinite(c->rho0))
         return fail(h, PM_ERR_INVALID_ARGUMENT, "rho_step must be positive and rho0 finite");
     return PM_OK;
-}
-
-void matmul3(const double* A, const double* B, double* C) {
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) {
-            double s = 0;
-            for (int k = 0; k < 3; ++k) s += A[3 * i + k] * B[3 * k + j];
-            C[3 * i + j] = s;
-        }
-}
-void matvec3(const double* A, const double* x, double* y) {
-    for (int i = 0; i < 3; ++i) {
-        double s = 0;
-        for (int k = 0; k < 3; ++k) s += A[3 * i + k] * x[k];
-        y[i] = s;
-    }
-}
-void transpose3(const double* A, double* T) {
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) T[3 * j + i] = A[3 * i + j];
-}
-bool finite_n(const double* v, int n) {
-    for (int i = 0; i < n; ++i)
-        if (!std::isfinite(v[i])) return false;
-    return true;
-}
-
-// H1 = K R_r^T R_l K^-1, H2 = K R_r^T (T_l - T_r) in FP64 (stereo_mapper.cpp:79-80), with the
-// closed-form inverse of the upper-triangular K.
-void compose_homography(const double* K, const double* Rl, const double* Tl, const double* Rr,
-                        const double* Tr, float out[12]) {
-    const double fx = K[0], s = K[1], cx = K[2], fy = K[4], cy = K[5];
-    const double Ki[9] = {1.0 / fx, -s / (fx * fy), (s * cy - cx * fy) / (fx * fy), 0.0, 1.0 / fy, -cy / fy,
-                          0.0, 0.0, 1.0};
-    double RrT[9], A[9], B[9], H1[9];
-    transpose3(Rr, RrT);
-    matmul3(K, RrT, A);
-    matmul3(A, Rl, B);
-    matmul3(B, Ki, H1);
-    const double dT[3] = {Tl[0] - Tr[0], Tl[1] - Tr[1], Tl[2] - Tr[2]};
-    double H2[3];
-    matvec3(A, dT, H2);
-    for (int i = 0; i < 9; ++i) out[i] = (float)H1[i];
-    for (int i = 0; i < 3; ++i) out[9 + i] = (float)H2[i];
 }
 
 void fill_cost_launch(const pm_config& c, CostLaunch& a) {
@@ -341,6 +356,10 @@ void release(pm_mapper* h) {
 }
 
 }  // namespace
+
+namespace pm {
+pm_status validate_config(const pm_config* c) { return check_config(c, nullptr); }
+}  // namespace pm
 
 extern "C" {
 
@@ -557,18 +576,11 @@ pm_status pm_output_fusion(pm_mapper* h, float* depth, size_t depth_pitch, float
         PM_CK(h, cudaMemsetAsync(h->d_fused, 0, 4 * N, h->stream));
         PM_CK(h, cudaMemsetAsync(h->d_var, 0, 4 * N, h->stream));
     } else {
-        // R_p2c = R^T R_prev, t_p2c = R^T (t_prev - t) (stereo_mapper.cpp:155-156)
-        double RT[9], Rpc[9], tpc[3];
-        transpose3(R, RT);
-        matmul3(RT, h->R_prev, Rpc);
-        const double dt[3] = {h->t_prev[0] - t[0], h->t_prev[1] - t[1], h->t_prev[2] - t[2]};
-        matvec3(RT, dt, tpc);
         FuseLaunch f;
         std::memset(&f, 0, sizeof f);
         f.W = W;
         f.H = H;
-        for (int i = 0; i < 9; ++i) f.pose[i] = (float)Rpc[i];
-        for (int i = 0; i < 3; ++i) f.pose[9 + i] = (float)tpc[i];
+        fusion_pose(R, t, h->R_prev, h->t_prev, f.pose);
         f.cam[0] = fx; f.cam[1] = fy; f.cam[2] = cx; f.cam[3] = cy;
         PM_CK(h, cudaMemcpyAsync(h->d_fused, h->d_depth, 4 * N, cudaMemcpyDeviceToDevice, h->stream));
         f.depth = h->d_fused;

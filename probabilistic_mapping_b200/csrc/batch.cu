@@ -1,0 +1,651 @@
+// batch.cu -- the batched form: many independent sequences (each its own pm_config: resolution,
+// plane count, precision, parameters) stepped together.
+//
+// One pm_batch_run is one keyframe of every sequence -- initReference, num_sources updates and
+// outputFusion, exactly as the StereoMapper calls (stereo_mapper.cpp:63-244) -- issued as ONE
+// CUDA-graph launch.  The graph is captured once: every value that changes from step to step
+// (homographies, the relative pose of the fusion step, the first-keyframe flag and the state
+// ping-pong index) lives in a small parameter block that the graph copies from pinned host
+// memory into device memory at its start, and the kernels read it from there.  The sequences are
+// independent branches of the graph, so the ALU-bound cost volume of one sequence runs beside the
+// latency-bound SGM passes of others.  Sequences of the same shape share a pool of `lanes` sets
+// of cost and path volumes (the large buffers), chained by graph dependencies, which bounds the
+// memory of a large batch.  Two graph instances alternate by step parity over double-buffered
+// parameter blocks and frame buffers, so the host prepares step t+1 while step t runs.
+// An optional autotuner times the SGM schedules (scanlines per block of the path-pair kernel,
+// concurrent or serial path pairs) for each distinct shape and keeps the fastest.
+#include <cuda_fp16.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "pm_internal.h"
+#include "pm_stereo.h"
+
+namespace pm {
+pm_status validate_config(const pm_config* c);
+}
+
+using namespace pm;
+
+namespace {
+
+// Large buffers one sequence needs only while its cost volume and SGM are in flight.
+struct LaneBufs {
+    void* cost = nullptr;
+    float* part[8] = {};
+    int last_user = -1;   // sequence index that used this set last in the capture order
+};
+
+struct Seq {
+    pm_config cfg{};
+    int S = 0;
+    size_t N = 0, V = 0;
+    double K[9]{};
+    bool have_K = false;
+    float cam[4]{};
+    // frames (1 + S uint8 images of W*H) and the step parameter block, per buffer set
+    uint8_t* h_frames[2] = {};   // pinned host (host I/O)
+    uint8_t* d_frames[2] = {};
+    float* h_par[2] = {};        // pinned host
+    float* d_par[2] = {};
+    size_t par_floats = 0;       // 12*S homographies, 12 pose + 4 cam, 2 ints
+    float* h_out[2] = {};        // pinned host: fused depth then variance (host I/O)
+    // persistent device state
+    float* d_ref = nullptr;
+    float4* d_srcq = nullptr;
+    void* d_srcq16 = nullptr;
+    float* d_depth = nullptr;
+    int32_t* d_idx = nullptr;
+    float* d_state[2][4] = {};
+    unsigned long long* d_ztable = nullptr;
+    int32_t* d_table = nullptr;
+    float* d_fused = nullptr;
+    float* d_var = nullptr;
+    PlaneOrder order{};
+    int lane = -1;               // index into the batch's lane sets
+    // host step state (stereo_mapper.cpp:128-156)
+    bool first = true;
+    int pre_index = 0;
+    double R_prev[9]{}, t_prev[3]{};
+    double R_ref[9]{}, T_ref[3]{};
+    std::vector<double> R_src, T_src;
+    bool have_pose = false;
+    // SGM schedule
+    int pair_warps = 4, serial_pairs = 0;
+    float tuned_ms = 0.0f;
+    // capture streams and events
+    cudaStream_t st[4] = {};
+    SgmStreams side{};
+    cudaEvent_t done = nullptr, lane_free = nullptr;
+};
+
+}  // namespace
+
+struct pm_batch {
+    std::vector<Seq> seqs;
+    std::vector<LaneBufs> lanes;
+    int S = 0;
+    int flags = 0;
+    int device = 0;
+    cudaStream_t run = nullptr;
+    cudaEvent_t root = nullptr;
+    cudaEvent_t launched[2] = {};
+    cudaGraph_t graph[2] = {};
+    cudaGraphExec_t exec[2] = {};
+    bool built = false;
+    long step = 0;
+    std::string err;
+};
+
+namespace {
+
+pm_status bfail(pm_batch* b, pm_status s, const char* fmt, ...) {
+    if (b) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        b->err = buf;
+    }
+    return s;
+}
+
+#define PB_CK(b, call)                                                                          \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return bfail((b), e_ == cudaErrorMemoryAllocation ? PM_ERR_OUT_OF_MEMORY : PM_ERR_CUDA, \
+                         "%s: %s", #call, cudaGetErrorString(e_));                              \
+    } while (0)
+
+struct DevGuard {
+    int prev = -1;
+    explicit DevGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DevGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+using ShapeKey = std::tuple<int, int, int, int, int>;   // W, H, D, precision, num_paths
+ShapeKey key_of(const pm_config& c) { return {c.width, c.height, c.num_planes, c.precision, c.num_paths}; }
+
+void free_batch(pm_batch* b) {
+    for (int k = 0; k < 2; ++k) {
+        if (b->exec[k]) cudaGraphExecDestroy(b->exec[k]);
+        if (b->graph[k]) cudaGraphDestroy(b->graph[k]);
+        if (b->launched[k]) cudaEventDestroy(b->launched[k]);
+    }
+    for (auto& l : b->lanes) {
+        cudaFree(l.cost);
+        for (auto* p : l.part) cudaFree(p);
+    }
+    for (auto& q : b->seqs) {
+        for (int k = 0; k < 2; ++k) {
+            cudaFreeHost(q.h_frames[k]);
+            cudaFree(q.d_frames[k]);
+            cudaFreeHost(q.h_par[k]);
+            cudaFree(q.d_par[k]);
+            cudaFreeHost(q.h_out[k]);
+        }
+        cudaFree(q.d_ref);
+        cudaFree(q.d_srcq);
+        cudaFree(q.d_srcq16);
+        cudaFree(q.d_depth);
+        cudaFree(q.d_idx);
+        for (auto& s : q.d_state)
+            for (auto* p : s) cudaFree(p);
+        cudaFree(q.d_ztable);
+        cudaFree(q.d_table);
+        cudaFree(q.d_fused);
+        cudaFree(q.d_var);
+        for (auto& s : q.st)
+            if (s) cudaStreamDestroy(s);
+        if (q.side.fork) cudaEventDestroy(q.side.fork);
+        for (auto& e : q.side.join)
+            if (e) cudaEventDestroy(e);
+        if (q.done) cudaEventDestroy(q.done);
+        if (q.lane_free) cudaEventDestroy(q.lane_free);
+    }
+    if (b->root) cudaEventDestroy(b->root);
+    if (b->run) cudaStreamDestroy(b->run);
+}
+
+SgmLaunch sgm_launch(const Seq& q, const LaneBufs& l) {
+    SgmLaunch a;
+    std::memset(&a, 0, sizeof a);
+    const pm_config& c = q.cfg;
+    a.cost = l.cost;
+    a.cost_half = c.precision == PM_PREC_FP16;
+    a.ref = q.d_ref;
+    for (int r = 0; r < c.num_paths; ++r) a.part[r] = l.part[r];
+    a.W = c.width;
+    a.H = c.height;
+    a.D = c.num_planes;
+    a.num_paths = c.num_paths;
+    a.p1 = c.p1; a.p2 = c.p2; a.tau = c.tau_so; a.q1 = c.q1; a.q2 = c.q2;
+    a.fp.var_scale = c.var_scale;
+    a.fp.uniq = c.uniqueness_ratio;
+    a.fp.rho0 = c.rho0;
+    a.fp.drho = c.rho_step;
+    a.depth = q.d_depth;
+    a.depth_pitch = sizeof(float) * (size_t)c.width;
+    a.index = q.d_idx;
+    a.order = q.order;
+    a.pair_warps = q.pair_warps;
+    a.serial_pairs = q.serial_pairs;
+    return a;
+}
+
+// The work of one sequence for buffer set k, on its own streams (captured into the graph).
+cudaError_t enqueue_seq(pm_batch* b, int i, int k) {
+    Seq& q = b->seqs[i];
+    LaneBufs& l = b->lanes[q.lane];
+    const pm_config& c = q.cfg;
+    const int W = c.width, H = c.height, S = q.S;
+    const size_t N = q.N;
+    const bool host = b->flags & PM_BATCH_HOST_IO;
+    const bool half = c.precision == PM_PREC_FP16;
+    cudaStream_t m = q.st[0];
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(q.d_par[k], q.h_par[k], sizeof(float) * q.par_floats, cudaMemcpyHostToDevice, m)))
+        return e;
+    if (host && (e = cudaMemcpyAsync(q.d_frames[k], q.h_frames[k], (1 + S) * N, cudaMemcpyHostToDevice, m)))
+        return e;
+    const float sc = c.intensity_scale;
+    e = half ? launch_to_float_h(W, H, q.d_frames[k], W, q.d_ref, sc, m)
+             : launch_to_float(W, H, q.d_frames[k], W, q.d_ref, sc, m);
+    if (e) return e;
+    for (int s = 0; s < S; ++s) {
+        const uint8_t* f = q.d_frames[k] + (1 + s) * N;
+        e = half ? launch_to_quad_half(W, H, f, W, (char*)q.d_srcq16 + (size_t)s * 8 * N, sc, m)
+                 : launch_to_quad(W, H, f, W, q.d_srcq + (size_t)s * N, sc, m);
+        if (e) return e;
+    }
+    // the lane's volumes are free once the previous sequence in this lane has finished its SGM
+    if (l.last_user >= 0 && (e = cudaStreamWaitEvent(m, b->seqs[l.last_user].lane_free, 0))) return e;
+    l.last_user = i;
+    CostLaunch a;
+    std::memset(&a, 0, sizeof a);
+    a.ref = q.d_ref;
+    a.srcq = half ? nullptr : q.d_srcq;
+    a.srcq16 = half ? q.d_srcq16 : nullptr;
+    a.W = W;
+    a.H = H;
+    a.D = c.num_planes;
+    a.nsrc = S;
+    a.rho0 = c.rho0;
+    a.drho = c.rho_step;
+    a.mode = c.cost_mode;
+    a.hom_dev = q.d_par[k];
+    a.cost = l.cost;
+    a.cost_half = half;
+    if ((e = launch_cost(a, m))) return e;
+    const SgmLaunch g = sgm_launch(q, l);
+    if ((e = launch_sgm(g, true, m, &q.side))) return e;
+    if ((e = cudaEventRecord(q.lane_free, m))) return e;
+    // fusion (stereo_mapper.cpp:111-244) with the step's pose, flags and state index from d_par
+    if ((e = cudaMemcpyAsync(q.d_fused, q.d_depth, 4 * N, cudaMemcpyDeviceToDevice, m))) return e;
+    FuseLaunch f;
+    std::memset(&f, 0, sizeof f);
+    f.W = W;
+    f.H = H;
+    f.depth = q.d_fused;
+    f.ztable = q.d_ztable;
+    f.table = q.d_table;
+    f.variance = q.d_var;
+    f.params_dev = q.d_par[k] + 12 * S;
+    f.flags_dev = reinterpret_cast<const int*>(q.d_par[k] + 12 * S + 16);
+    for (int s = 0; s < 2; ++s)
+        for (int j = 0; j < 4; ++j) f.state[s][j] = q.d_state[s][j];
+    if ((e = launch_fuse_gpu(f, m))) return e;
+    if (host) {
+        if ((e = cudaMemcpyAsync(q.h_out[k], q.d_fused, 4 * N, cudaMemcpyDeviceToHost, m))) return e;
+        if ((e = cudaMemcpyAsync(q.h_out[k] + N, q.d_var, 4 * N, cudaMemcpyDeviceToHost, m))) return e;
+    }
+    return cudaSuccess;
+}
+
+pm_status build_graphs(pm_batch* b) {
+    for (int k = 0; k < 2; ++k) {
+        for (auto& l : b->lanes) l.last_user = -1;
+        PB_CK(b, cudaStreamBeginCapture(b->run, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaEventRecord(b->root, b->run);
+        for (int i = 0; i < (int)b->seqs.size() && e == cudaSuccess; ++i) {
+            Seq& q = b->seqs[i];
+            e = cudaStreamWaitEvent(q.st[0], b->root, 0);
+            if (e == cudaSuccess) e = enqueue_seq(b, i, k);
+            if (e == cudaSuccess) e = cudaEventRecord(q.done, q.st[0]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(b->run, q.done, 0);
+        }
+        cudaGraph_t g = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(b->run, &g);
+        if (e != cudaSuccess || ee != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return bfail(b, PM_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : ee));
+        }
+        b->graph[k] = g;
+        PB_CK(b, cudaGraphInstantiate(&b->exec[k], g, 0));
+    }
+    b->built = true;
+    return PM_OK;
+}
+
+// Times the SGM stage of one sequence per distinct shape for every schedule candidate and keeps
+// the fastest for all sequences of that shape.
+pm_status autotune(pm_batch* b) {
+    std::map<ShapeKey, int> done;
+    cudaEvent_t t0, t1;
+    PB_CK(b, cudaEventCreate(&t0));
+    PB_CK(b, cudaEventCreate(&t1));
+    pm_status st = PM_OK;
+    for (int i = 0; i < (int)b->seqs.size() && st == PM_OK; ++i) {
+        Seq& q = b->seqs[i];
+        auto it = done.find(key_of(q.cfg));
+        if (it != done.end()) {
+            const Seq& t = b->seqs[it->second];
+            q.pair_warps = t.pair_warps;
+            q.serial_pairs = t.serial_pairs;
+            q.tuned_ms = t.tuned_ms;
+            continue;
+        }
+        LaneBufs& l = b->lanes[q.lane];
+        const size_t esz = q.cfg.precision == PM_PREC_FP16 ? 2 : 4;
+        float best = 1e30f;
+        int bw = 4, bs = 0;
+        const int warps[3] = {2, 4, 8};
+        cudaError_t e = cudaMemsetAsync(l.cost, 0, esz * q.V, b->run);
+        if (e == cudaSuccess) e = cudaMemsetAsync(q.d_ref, 0, 4 * q.N, b->run);
+        for (int w : warps)
+            for (int serial = 0; serial < 2 && e == cudaSuccess; ++serial) {
+                q.pair_warps = w;
+                q.serial_pairs = serial;
+                const SgmLaunch g = sgm_launch(q, l);
+                e = launch_sgm(g, true, b->run, &q.side);   // warm-up
+                if (e == cudaSuccess) e = cudaEventRecord(t0, b->run);
+                for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = launch_sgm(g, true, b->run, &q.side);
+                if (e == cudaSuccess) e = cudaEventRecord(t1, b->run);
+                if (e == cudaSuccess) e = cudaEventSynchronize(t1);
+                float ms = 0.0f;
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, t0, t1);
+                ms /= 3.0f;
+                if (e == cudaSuccess && ms < best) {
+                    best = ms;
+                    bw = w;
+                    bs = serial;
+                }
+            }
+        if (e != cudaSuccess) st = bfail(b, PM_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+        q.pair_warps = bw;
+        q.serial_pairs = bs;
+        q.tuned_ms = best;
+        done[key_of(q.cfg)] = i;
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+pm_status pm_batch_create(const pm_config* cfgs, int n, int num_sources, int lanes, int flags, pm_batch** out) {
+    if (!out) return PM_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (!cfgs || n < 1 || num_sources < 1 || num_sources > kMaxSources || lanes < 0)
+        return PM_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < n; ++i) {
+        if (validate_config(&cfgs[i]) != PM_OK) return PM_ERR_INVALID_ARGUMENT;
+        if (cfgs[i].sampler != PM_SAMPLER_EXACT || cfgs[i].fusion_variant != PM_FUSION_GPU ||
+            cfgs[i].device != cfgs[0].device)
+            return PM_ERR_UNSUPPORTED;
+    }
+    pm_batch* b = new pm_batch();
+    b->S = num_sources;
+    b->flags = flags;
+    b->device = cfgs[0].device;
+    DevGuard dg(b->device);
+    cudaError_t first_err = cudaSuccess;
+    auto note = [&](cudaError_t e) {
+        if (e != cudaSuccess && first_err == cudaSuccess) first_err = e;
+        return e == cudaSuccess;
+    };
+    auto alloc = [&](void** p, size_t bytes) { return note(cudaMalloc(p, bytes)); };
+    bool ok = note(cudaStreamCreateWithFlags(&b->run, cudaStreamNonBlocking)) &&
+              note(cudaEventCreateWithFlags(&b->root, cudaEventDisableTiming)) &&
+              note(cudaEventCreateWithFlags(&b->launched[0], cudaEventDisableTiming)) &&
+              note(cudaEventCreateWithFlags(&b->launched[1], cudaEventDisableTiming));
+    b->seqs.resize(n);
+    // lanes: per distinct shape, `lanes` sets of cost + path volumes (0: one per sequence)
+    std::map<ShapeKey, std::vector<int>> lane_of_shape;
+    std::map<ShapeKey, int> count_of_shape;
+    for (int i = 0; i < n && ok; ++i) {
+        Seq& q = b->seqs[i];
+        q.cfg = cfgs[i];
+        q.S = num_sources;
+        q.N = (size_t)q.cfg.width * q.cfg.height;
+        q.V = q.N * q.cfg.num_planes;
+        q.par_floats = 12 * (size_t)q.S + 16 + 2;
+        q.R_src.assign(9 * (size_t)q.S, 0.0);
+        q.T_src.assign(3 * (size_t)q.S, 0.0);
+        plane_order(q.cfg.num_planes, q.cfg.tree_compat, q.order);
+        const ShapeKey key = key_of(q.cfg);
+        const int j = count_of_shape[key]++;
+        std::vector<int>& pool = lane_of_shape[key];
+        if (lanes == 0 || (int)pool.size() < lanes) {
+            pool.push_back((int)b->lanes.size());
+            LaneBufs l;
+            const size_t esz = q.cfg.precision == PM_PREC_FP16 ? 2 : 4;
+            ok = alloc(&l.cost, esz * q.V);
+            for (int r = 0; r < q.cfg.num_paths && ok; ++r) ok = alloc((void**)&l.part[r], 4 * q.V);
+            b->lanes.push_back(l);
+            if (!ok) break;
+        }
+        q.lane = pool[lanes == 0 ? j : j % lanes];
+        const bool half = q.cfg.precision == PM_PREC_FP16;
+        const size_t N = q.N;
+        for (int k = 0; k < 2 && ok; ++k) {
+            ok = note(cudaMallocHost((void**)&q.h_par[k], sizeof(float) * q.par_floats)) &&
+                 alloc((void**)&q.d_par[k], sizeof(float) * q.par_floats) &&
+                 alloc((void**)&q.d_frames[k], (1 + q.S) * N);
+            if (ok && (flags & PM_BATCH_HOST_IO))
+                ok = note(cudaMallocHost((void**)&q.h_frames[k], (1 + q.S) * N)) &&
+                     note(cudaMallocHost((void**)&q.h_out[k], 2 * 4 * N));
+            if (ok) std::memset(q.h_par[k], 0, sizeof(float) * q.par_floats);
+        }
+        ok = ok && alloc((void**)&q.d_ref, 4 * N) &&
+             (half ? alloc(&q.d_srcq16, 8 * N * q.S) : alloc((void**)&q.d_srcq, 16 * N * q.S)) &&
+             alloc((void**)&q.d_depth, 4 * N) && alloc((void**)&q.d_idx, 4 * N) &&
+             alloc((void**)&q.d_ztable, 8 * N) && alloc((void**)&q.d_table, 4 * N) &&
+             alloc((void**)&q.d_fused, 4 * N) && alloc((void**)&q.d_var, 4 * N);
+        for (int s = 0; s < 2 && ok; ++s)
+            for (int k = 0; k < 4 && ok; ++k) ok = alloc((void**)&q.d_state[s][k], 4 * N);
+        for (int s = 0; s < 4 && ok; ++s) ok = note(cudaStreamCreateWithFlags(&q.st[s], cudaStreamNonBlocking));
+        if (ok) {
+            for (int s = 0; s < 3; ++s) q.side.stream[s] = q.st[1 + s];
+            ok = note(cudaEventCreateWithFlags(&q.side.fork, cudaEventDisableTiming)) &&
+                 note(cudaEventCreateWithFlags(&q.done, cudaEventDisableTiming)) &&
+                 note(cudaEventCreateWithFlags(&q.lane_free, cudaEventDisableTiming));
+            for (int s = 0; s < 3 && ok; ++s)
+                ok = note(cudaEventCreateWithFlags(&q.side.join[s], cudaEventDisableTiming));
+        }
+    }
+    pm_status tune = PM_OK;
+    if (ok && (flags & PM_BATCH_AUTOTUNE)) {
+        tune = autotune(b);
+        ok = tune == PM_OK;
+    }
+    if (ok) ok = note(cudaStreamSynchronize(b->run));
+    if (!ok) {
+        cudaGetLastError();
+        free_batch(b);
+        delete b;
+        if (tune != PM_OK) return tune;
+        return first_err == cudaErrorMemoryAllocation ? PM_ERR_OUT_OF_MEMORY : PM_ERR_CUDA;
+    }
+    *out = b;
+    return PM_OK;
+}
+
+void pm_batch_destroy(pm_batch* b) {
+    if (!b) return;
+    DevGuard dg(b->device);
+    if (b->run) cudaStreamSynchronize(b->run);
+    free_batch(b);
+    delete b;
+}
+
+pm_status pm_batch_init_intrinsic(pm_batch* b, int seq, const double K[9], float dep_sample) {
+    if (!b) return PM_ERR_INVALID_ARGUMENT;
+    if (seq < 0 || seq >= (int)b->seqs.size()) return bfail(b, PM_ERR_INVALID_ARGUMENT, "no sequence %d", seq);
+    if (!K || !finite_n(K, 9) || K[0] == 0.0 || K[4] == 0.0 || K[3] != 0.0 || K[6] != 0.0 || K[7] != 0.0 ||
+        K[8] != 1.0)
+        return bfail(b, PM_ERR_INVALID_ARGUMENT, "K must be upper triangular with K[2][2] = 1 and nonzero fx, fy");
+    if (!(dep_sample > 0.0f)) return bfail(b, PM_ERR_INVALID_ARGUMENT, "dep_sample must be positive");
+    if (b->built && dep_sample != b->seqs[seq].cfg.rho_step)
+        return bfail(b, PM_ERR_BAD_STATE, "the plane spacing is fixed once the batch has run");
+    Seq& q = b->seqs[seq];
+    std::memcpy(q.K, K, sizeof q.K);
+    q.have_K = true;
+    q.cfg.rho_step = dep_sample;
+    q.cam[0] = (float)K[0];
+    q.cam[1] = (float)K[4];
+    q.cam[2] = (float)K[2];
+    q.cam[3] = (float)K[5];
+    return PM_OK;
+}
+
+pm_status pm_batch_frame(pm_batch* b, int seq, int frame, uint8_t** ptr) {
+    if (!b || !ptr) return PM_ERR_INVALID_ARGUMENT;
+    if (seq < 0 || seq >= (int)b->seqs.size() || frame < 0 || frame > b->S)
+        return bfail(b, PM_ERR_INVALID_ARGUMENT, "no frame %d of sequence %d", frame, seq);
+    DevGuard dg(b->device);
+    const int k = (int)(b->step & 1);
+    // the set is free once the launch two steps back (which read it) has completed
+    if (b->step >= 2) PB_CK(b, cudaEventSynchronize(b->launched[k]));
+    Seq& q = b->seqs[seq];
+    uint8_t* base = (b->flags & PM_BATCH_HOST_IO) ? q.h_frames[k] : q.d_frames[k];
+    *ptr = base + (size_t)frame * q.N;
+    return PM_OK;
+}
+
+pm_status pm_batch_put_frame(pm_batch* b, int seq, int frame, const uint8_t* img, size_t pitch) {
+    if (!b || !img) return PM_ERR_INVALID_ARGUMENT;
+    uint8_t* dst = nullptr;
+    pm_status st = pm_batch_frame(b, seq, frame, &dst);
+    if (st != PM_OK) return st;
+    const Seq& q = b->seqs[seq];
+    const int W = q.cfg.width, H = q.cfg.height;
+    if (pitch == 0) pitch = (size_t)W;
+    if (pitch < (size_t)W) return bfail(b, PM_ERR_INVALID_ARGUMENT, "image pitch %zu < width %d", pitch, W);
+    cudaPointerAttributes at;
+    const bool dev_src = cudaPointerGetAttributes(&at, img) == cudaSuccess &&
+                         (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged);
+    cudaGetLastError();
+    DevGuard dg(b->device);
+    if (b->flags & PM_BATCH_HOST_IO) {
+        if (dev_src) {
+            PB_CK(b, cudaMemcpy2D(dst, (size_t)W, img, pitch, (size_t)W, (size_t)H, cudaMemcpyDeviceToHost));
+        } else {
+            for (int y = 0; y < H; ++y) std::memcpy(dst + (size_t)y * W, img + (size_t)y * pitch, (size_t)W);
+        }
+    } else {
+        PB_CK(b, cudaMemcpy2DAsync(dst, (size_t)W, img, pitch, (size_t)W, (size_t)H,
+                                   dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->run));
+    }
+    return PM_OK;
+}
+
+pm_status pm_batch_set_poses(pm_batch* b, int seq, const double R_ref[9], const double T_ref[3], const double* R_src,
+                             const double* T_src) {
+    if (!b) return PM_ERR_INVALID_ARGUMENT;
+    if (seq < 0 || seq >= (int)b->seqs.size()) return bfail(b, PM_ERR_INVALID_ARGUMENT, "no sequence %d", seq);
+    Seq& q = b->seqs[seq];
+    if (!R_ref || !T_ref || !R_src || !T_src || !finite_n(R_ref, 9) || !finite_n(T_ref, 3) ||
+        !finite_n(R_src, 9 * q.S) || !finite_n(T_src, 3 * q.S))
+        return bfail(b, PM_ERR_INVALID_ARGUMENT, "poses must be finite");
+    std::memcpy(q.R_ref, R_ref, sizeof q.R_ref);
+    std::memcpy(q.T_ref, T_ref, sizeof q.T_ref);
+    std::memcpy(q.R_src.data(), R_src, sizeof(double) * 9 * q.S);
+    std::memcpy(q.T_src.data(), T_src, sizeof(double) * 3 * q.S);
+    q.have_pose = true;
+    return PM_OK;
+}
+
+pm_status pm_batch_run(pm_batch* b) {
+    if (!b) return PM_ERR_INVALID_ARGUMENT;
+    DevGuard dg(b->device);
+    for (int i = 0; i < (int)b->seqs.size(); ++i) {
+        const Seq& q = b->seqs[i];
+        if (!q.have_K) return bfail(b, PM_ERR_BAD_STATE, "sequence %d: run before init_intrinsic", i);
+        if (!q.have_pose) return bfail(b, PM_ERR_BAD_STATE, "sequence %d: run before set_poses", i);
+    }
+    if (!b->built) {
+        pm_status st = build_graphs(b);
+        if (st != PM_OK) return st;
+    }
+    const int k = (int)(b->step & 1);
+    if (b->step >= 2) PB_CK(b, cudaEventSynchronize(b->launched[k]));
+    for (auto& q : b->seqs) {
+        float* par = q.h_par[k];
+        for (int s = 0; s < q.S; ++s)   // initReference + update of every source (stereo_mapper.cpp:79-80)
+            compose_homography(q.K, q.R_ref, q.T_ref, &q.R_src[9 * s], &q.T_src[3 * s], par + 12 * s);
+        float* pose = par + 12 * q.S;
+        int* flags = reinterpret_cast<int*>(pose + 16);
+        std::memcpy(pose + 12, q.cam, sizeof q.cam);
+        if (q.first) {   // stereo_mapper.cpp:128-146
+            q.first = false;
+            q.pre_index = 0;
+            std::memset(pose, 0, 12 * sizeof(float));
+            flags[0] = 1;
+            flags[1] = 0;
+        } else {
+            fusion_pose(q.R_ref, q.T_ref, q.R_prev, q.t_prev, pose);
+            flags[0] = 0;
+            flags[1] = q.pre_index;
+            q.pre_index ^= 1;   // stereo_mapper.cpp:237-241
+        }
+        std::memcpy(q.R_prev, q.R_ref, sizeof q.R_prev);
+        std::memcpy(q.t_prev, q.T_ref, sizeof q.t_prev);
+    }
+    PB_CK(b, cudaGraphLaunch(b->exec[k], b->run));
+    PB_CK(b, cudaEventRecord(b->launched[k], b->run));
+    ++b->step;
+    return PM_OK;
+}
+
+pm_status pm_batch_synchronize(pm_batch* b) {
+    if (!b) return PM_ERR_INVALID_ARGUMENT;
+    DevGuard dg(b->device);
+    PB_CK(b, cudaStreamSynchronize(b->run));
+    return PM_OK;
+}
+
+pm_status pm_batch_output(pm_batch* b, int seq, const float** depth, const float** variance) {
+    if (!b) return PM_ERR_INVALID_ARGUMENT;
+    if (seq < 0 || seq >= (int)b->seqs.size()) return bfail(b, PM_ERR_INVALID_ARGUMENT, "no sequence %d", seq);
+    if (b->step == 0) return bfail(b, PM_ERR_BAD_STATE, "no step has run");
+    const Seq& q = b->seqs[seq];
+    const int k = (int)((b->step - 1) & 1);
+    if (b->flags & PM_BATCH_HOST_IO) {
+        if (depth) *depth = q.h_out[k];
+        if (variance) *variance = q.h_out[k] + q.N;
+    } else {
+        if (depth) *depth = q.d_fused;
+        if (variance) *variance = q.d_var;
+    }
+    return PM_OK;
+}
+
+pm_status pm_batch_copy_output(pm_batch* b, int seq, float* depth, size_t pitch, float* variance, size_t var_pitch) {
+    if (!b) return PM_ERR_INVALID_ARGUMENT;
+    const float* d = nullptr;
+    const float* v = nullptr;
+    pm_status st = pm_batch_output(b, seq, &d, &v);
+    if (st != PM_OK) return st;
+    const Seq& q = b->seqs[seq];
+    const size_t row = sizeof(float) * (size_t)q.cfg.width;
+    if (pitch == 0) pitch = row;
+    if (var_pitch == 0) var_pitch = row;
+    if (pitch < row || var_pitch < row) return bfail(b, PM_ERR_INVALID_ARGUMENT, "output pitch too small");
+    DevGuard dg(b->device);
+    PB_CK(b, cudaStreamSynchronize(b->run));
+    if (depth) PB_CK(b, cudaMemcpy2D(depth, pitch, d, row, row, (size_t)q.cfg.height, cudaMemcpyDefault));
+    if (variance) PB_CK(b, cudaMemcpy2D(variance, var_pitch, v, row, row, (size_t)q.cfg.height, cudaMemcpyDefault));
+    return PM_OK;
+}
+
+pm_status pm_batch_wta_depth(pm_batch* b, int seq, const float** depth) {
+    if (!b || !depth) return PM_ERR_INVALID_ARGUMENT;
+    if (seq < 0 || seq >= (int)b->seqs.size()) return bfail(b, PM_ERR_INVALID_ARGUMENT, "no sequence %d", seq);
+    *depth = b->seqs[seq].d_depth;
+    return PM_OK;
+}
+
+pm_status pm_batch_tuning(pm_batch* b, int seq, int* pair_warps, int* serial_pairs, float* ms) {
+    if (!b) return PM_ERR_INVALID_ARGUMENT;
+    if (seq < 0 || seq >= (int)b->seqs.size()) return bfail(b, PM_ERR_INVALID_ARGUMENT, "no sequence %d", seq);
+    const Seq& q = b->seqs[seq];
+    if (pair_warps) *pair_warps = q.pair_warps;
+    if (serial_pairs) *serial_pairs = q.serial_pairs;
+    if (ms) *ms = q.tuned_ms;
+    return PM_OK;
+}
+
+void* pm_batch_stream(pm_batch* b) { return b ? (void*)b->run : nullptr; }
+
+const char* pm_batch_last_error(const pm_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+}  // extern "C"

@@ -161,6 +161,14 @@ __device__ __forceinline__ float2 sample2(const Src<SAMP>& src, const WarpConst&
 
 __device__ __forceinline__ Hom load_hom(const CostLaunch& a, int s) {
     Hom h;
+    if (a.hom_dev) {
+        const float* p = a.hom_dev + 12 * s;
+        h.r11 = __ldg(p + 0); h.r12 = __ldg(p + 1); h.r13 = __ldg(p + 2);
+        h.r21 = __ldg(p + 3); h.r22 = __ldg(p + 4); h.r23 = __ldg(p + 5);
+        h.r31 = __ldg(p + 6); h.r32 = __ldg(p + 7); h.r33 = __ldg(p + 8);
+        h.t1 = __ldg(p + 9); h.t2 = __ldg(p + 10); h.t3 = __ldg(p + 11);
+        return h;
+    }
     h.r11 = a.hom[s][0]; h.r12 = a.hom[s][1]; h.r13 = a.hom[s][2];
     h.r21 = a.hom[s][3]; h.r22 = a.hom[s][4]; h.r23 = a.hom[s][5];
     h.r31 = a.hom[s][6]; h.r32 = a.hom[s][7]; h.r33 = a.hom[s][8];

@@ -18,22 +18,59 @@ namespace {
 
 constexpr unsigned long long kEmpty = ~0ull;
 
+// The per-step view of a launch: by value (one mapper call) or from device memory (batched form).
+struct FuseView {
+    const float* pose;
+    const float* cam;
+    float* pre[4];
+    float* cur[4];
+    bool first;
+};
+
+__device__ __forceinline__ FuseView view(const FuseLaunch& a) {
+    FuseView v;
+    if (a.flags_dev) {
+        const int idx = a.flags_dev[1] & 1;
+        v.first = a.flags_dev[0] != 0;
+        v.pose = a.params_dev;
+        v.cam = a.params_dev + 12;
+        for (int k = 0; k < 4; ++k) {
+            v.pre[k] = a.state[idx][k];
+            v.cur[k] = a.state[idx ^ 1][k];
+        }
+    } else {
+        v.first = false;
+        v.pose = a.pose;
+        v.cam = a.cam;
+        for (int k = 0; k < 4; ++k) {
+            v.pre[k] = a.pre[k];
+            v.cur[k] = a.cur[k];
+        }
+    }
+    return v;
+}
+
 __global__ void __launch_bounds__(256) fuse_transform_kernel(const FuseLaunch a) {
     const int W = a.W, H = a.H;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= W || y >= H) return;
     const int index = y * W + x;
-    const float al = a.pre[0][index];
+    const FuseView v = view(a);
+    if (v.first) {   // first keyframe: both state sets start from zero (stereo_mapper.cpp:138-141)
+        for (int k = 0; k < 4; ++k) a.state[0][k][index] = a.state[1][k][index] = 0.0f;
+        return;
+    }
+    const float al = v.pre[0][index];
     if ((double)al < kFloatEps) return;                                    // (:26)
-    const float be = a.pre[1][index];
+    const float be = v.pre[1][index];
     if ((double)__fdiv_rn(al, __fadd_rn(al, be)) < 0.4) return;            // (:30)
-    const float dep = a.pre[2][index];
-    const float fx = a.cam[0], fy = a.cam[1], cx = a.cam[2], cy = a.cam[3];
+    const float dep = v.pre[2][index];
+    const float fx = v.cam[0], fy = v.cam[1], cx = v.cam[2], cy = v.cam[3];
     const float px = __fmul_rn(__fdiv_rn(__fsub_rn((float)x, cx), fx), dep);   // (:34)
     const float py = __fmul_rn(__fdiv_rn(__fsub_rn((float)y, cy), fy), dep);
     const float pz = dep;
-    const float* p = a.pose;
+    const float* p = v.pose;
     // r11*px+r12*py+r13*pz + t1 (:37-39) with the multiply-add contraction of the reference's
     // nvcc build, so the transformed depth and the target pixel agree with it bit for bit
     const float px2 = __fadd_rn(__fmaf_rn(p[2], pz, __fmaf_rn(p[1], py, __fmul_rn(p[0], px))), p[9]);
@@ -43,8 +80,8 @@ __global__ void __launch_bounds__(256) fuse_transform_kernel(const FuseLaunch a)
     const int x2 = __double2int_rz(__dadd_rn((double)__fmaf_rn(__fdiv_rn(px2, pz2), fx, cx), 0.5));   // (:43)
     const int y2 = __double2int_rz(__dadd_rn((double)__fmaf_rn(__fdiv_rn(py2, pz2), fy, cy), 0.5));
     if (x2 < 0 || x2 >= W || y2 < 0 || y2 >= H) return;
-    a.pre[2][index] = pz2;                                                 // (:48)
-    a.pre[3][index] = __double2float_rn(__dadd_rn((double)a.pre[3][index], __dmul_rn((double)pz2, 0.05)));
+    v.pre[2][index] = pz2;                                                 // (:48)
+    v.pre[3][index] = __double2float_rn(__dadd_rn((double)v.pre[3][index], __dmul_rn((double)pz2, 0.05)));
     if (index == 0) return;   // index 0 encodes "empty" in the reference's table
     const unsigned long long key = ((unsigned long long)__float_as_uint(pz2) << 32) | (unsigned)index;
     atomicMin(a.ztable + (size_t)y2 * W + x2, key);
@@ -62,6 +99,13 @@ __global__ void __launch_bounds__(256) fuse_update_kernel(const FuseLaunch a) {
     const int y = blockIdx.y;
     if (x >= W || y >= H) return;
     const int e = y * W + x;
+    const FuseView v = view(a);
+    if (v.first) {   // first keyframe: the fused map and its variance are zero
+        a.depth[e] = 0.0f;
+        if (a.variance) a.variance[e] = 0.0f;
+        if (a.table) a.table[e] = 0;
+        return;
+    }
 
     // hole filling (:80-105): an empty cell takes the last occupied interior neighbour in
     // raster order, the writer whose own 3x3 loop (:96-103) reaches it first
@@ -83,7 +127,7 @@ __global__ void __launch_bounds__(256) fuse_update_kernel(const FuseLaunch a) {
     if (t == 0) {
         ca = -1.0f;
     } else {
-        ca = a.pre[0][t]; cb = a.pre[1][t]; cm = a.pre[2][t]; cs = a.pre[3][t];
+        ca = v.pre[0][t]; cb = v.pre[1][t]; cm = v.pre[2][t]; cs = v.pre[3][t];
     }
 
     // depthUpdate (:139-225)
@@ -129,10 +173,10 @@ __global__ void __launch_bounds__(256) fuse_update_kernel(const FuseLaunch a) {
         write_all = true;
         out_d = ((double)__fdiv_rn(aa, ab) > 0.6) ? mu_p : 0.0f;             // (:219)
     }
-    a.cur[0][e] = ca;
-    if (write_all) { a.cur[1][e] = cb; a.cur[2][e] = cm; a.cur[3][e] = cs; }
+    v.cur[0][e] = ca;
+    if (write_all) { v.cur[1][e] = cb; v.cur[2][e] = cm; v.cur[3][e] = cs; }
     a.depth[e] = out_d;
-    if (a.variance) a.variance[e] = write_all ? cs : a.cur[3][e];
+    if (a.variance) a.variance[e] = write_all ? cs : v.cur[3][e];
 }
 
 }  // namespace

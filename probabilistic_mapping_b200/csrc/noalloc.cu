@@ -49,7 +49,7 @@ extern "C" pm_status pm_stage_depth_fuse_noalloc(int W, int H, const float pose[
                                                 int32_t* table, void* stream) {
     if (W <= 0 || H <= 0 || !pose || !cam || !depth || !pre || !cur) return PM_ERR_INVALID_ARGUMENT;
     if ((size_t)W * (size_t)H > kNoAllocMaxPixels) return PM_ERR_INVALID_ARGUMENT;   // beyond the array
-    pm::FuseLaunch f;
+    pm::FuseLaunch f{};   // value-initialised: no device-side step parameters
     f.W = W;
     f.H = H;
     for (int i = 0; i < 12; ++i) f.pose[i] = pose[i];

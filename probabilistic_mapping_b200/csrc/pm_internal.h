@@ -26,6 +26,7 @@ struct CostLaunch {
     float rho0, drho;
     int mode;              // 0 reference quirks, 1 corrected 3x3 patch
     float hom[kMaxSources][12];
+    const float* hom_dev;  // batched form: the homographies (nsrc x 12) in device memory, or nullptr
     void* cost;            // W*H*D float, or __half when cost_half
     int cost_half;
     float* cnt;            // running count (incremental mode) or nullptr
@@ -59,6 +60,8 @@ struct SgmLaunch {
     size_t depth_pitch;
     int32_t* index;        // W*H (optional)
     PlaneOrder order;
+    int pair_warps;        // scanlines per block of the path-pair kernel: 2, 4 or 8 (0: 4)
+    int serial_pairs;      // 1: run the path pairs one after another on the caller's stream
 };
 // Side streams for the concurrent path pairs: pairs 0..2 fork from the caller's stream and join
 // back before the combine kernel.
@@ -104,7 +107,25 @@ struct FuseLaunch {
     unsigned long long* ztable;  // W*H scratch z-buffer
     int32_t* table;        // W*H filled propagation table (optional)
     float* variance;       // W*H sigma^2 of the current state (optional)
+    // Batched form (values that change every step, read from device memory so that a captured
+    // graph stays valid): params_dev = pose[12], cam[4]; flags_dev = {first, pre_index}; the
+    // state sets are state[pre_index] (previous) and state[pre_index ^ 1] (current).  On the first
+    // frame both state sets, the fused depth and the variance are cleared (stereo_mapper.cpp:128-146).
+    const float* params_dev;
+    const int* flags_dev;
+    float* state[2][4];
 };
 cudaError_t launch_fuse_gpu(const FuseLaunch& a, cudaStream_t s);
+
+// ---- host-side geometry, FP64 (api.cu) -----------------------------------------------------
+void matmul3(const double* A, const double* B, double* C);
+void matvec3(const double* A, const double* x, double* y);
+void transpose3(const double* A, double* T);
+bool finite_n(const double* v, int n);
+// H1 = K R_r^T R_l K^-1 and H2 = K R_r^T (T_l - T_r) (stereo_mapper.cpp:79-80) as 12 floats
+void compose_homography(const double* K, const double* Rl, const double* Tl, const double* Rr,
+                        const double* Tr, float out[12]);
+// relative pose of the previous keyframe in the current one (stereo_mapper.cpp:155-156), 12 floats
+void fusion_pose(const double* R, const double* t, const double* R_prev, const double* t_prev, float out[12]);
 
 }  // namespace pm

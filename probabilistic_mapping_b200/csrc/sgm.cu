@@ -56,7 +56,6 @@ void plane_order(int D, int compat, PlaneOrder& out) {
 
 namespace {
 
-constexpr int WARPS = 4;   // scanlines per block
 constexpr int PF = 8;      // prefetch distance in pixel steps
 
 struct Chain {
@@ -248,8 +247,8 @@ __device__ __forceinline__ void path_step(const SgmLaunch& a, PathState<PPL>& s,
 // backward one into part[slot + 1].  The two recurrences are independent, so each warp keeps two
 // dependency chains in flight.  The cost slices and reference pixels of both ends are streamed
 // PF steps ahead with cp.async into a per-warp shared ring.
-template <int PPL, bool HALF>
-__global__ void __launch_bounds__(WARPS * 32) sgm_pair_kernel(const SgmLaunch a, int dx, int dy, int slot) {
+template <int PPL, bool HALF, int NW>
+__global__ void __launch_bounds__(NW * 32) sgm_pair_kernel(const SgmLaunch a, int dx, int dy, int slot) {
     using CT = typename CostElem<HALF>::T;
     using RG = Ring<PPL, HALF>;
     constexpr int CB = RG::CB, CHAIN_B = RG::CHAIN_B, STAGE_B = RG::STAGE_B;
@@ -257,7 +256,7 @@ __global__ void __launch_bounds__(WARPS * 32) sgm_pair_kernel(const SgmLaunch a,
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int W = a.W, H = a.H, D = a.D;
-    const int c = blockIdx.x * WARPS + warp;
+    const int c = blockIdx.x * NW + warp;
     if (c >= num_chains(dx, dy, W, H)) return;        // warp-uniform; no block barriers below
     const Chain ch = chain_start(c, dx, dy, W, H);
     const long step = (long)dy * W + dx;
@@ -387,18 +386,28 @@ __global__ void __launch_bounds__(128) filter_kernel(const float* __restrict__ s
 // pair p = paths (2p, 2p+1) runs as one sgm_pair_kernel along direction kDirs[2p].
 const int kDirs[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1}, {-1, 1}, {1, -1}};
 
-template <int PPL, bool HALF>
-cudaError_t launch_pair(const SgmLaunch& a, int pair, cudaStream_t s) {
-    const size_t smem = (size_t)WARPS * PF * Ring<PPL, HALF>::STAGE_B;
-    auto kern = sgm_pair_kernel<PPL, HALF>;
+template <int PPL, bool HALF, int NW>
+cudaError_t launch_pair_nw(const SgmLaunch& a, int pair, cudaStream_t s) {
+    const size_t smem = (size_t)NW * PF * Ring<PPL, HALF>::STAGE_B;
+    auto kern = sgm_pair_kernel<PPL, HALF, NW>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     const int dx = kDirs[2 * pair][0], dy = kDirs[2 * pair][1];
     const int nch = num_chains(dx, dy, a.W, a.H);
-    kern<<<(nch + WARPS - 1) / WARPS, WARPS * 32, smem, s>>>(a, dx, dy, 2 * pair);
+    kern<<<(nch + NW - 1) / NW, NW * 32, smem, s>>>(a, dx, dy, 2 * pair);
     return cudaGetLastError();
+}
+
+// scanlines (warps) per block: a.pair_warps in {2, 4, 8}, 4 when unset
+template <int PPL, bool HALF>
+cudaError_t launch_pair(const SgmLaunch& a, int pair, cudaStream_t s) {
+    switch (a.pair_warps) {
+        case 2: return launch_pair_nw<PPL, HALF, 2>(a, pair, s);
+        case 8: return launch_pair_nw<PPL, HALF, 8>(a, pair, s);
+        default: return launch_pair_nw<PPL, HALF, 4>(a, pair, s);
+    }
 }
 
 template <int PPL>
@@ -423,6 +432,7 @@ template <int PPL, bool HALF>
 cudaError_t launch_sgm_t(const SgmLaunch& a, bool fuse_filter, cudaStream_t s, const SgmStreams* side) {
     const int np = a.num_paths / 2;
     cudaError_t e = cudaSuccess;
+    if (a.serial_pairs) side = nullptr;
     if (side) {
         if ((e = cudaEventRecord(side->fork, s)) != cudaSuccess) return e;
         for (int p = 0; p < np - 1; ++p) {

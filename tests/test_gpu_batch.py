@@ -1,0 +1,85 @@
+"""The batched form against separate StereoMapper runs.
+
+A batch of sequences with different shapes, precisions, path counts and cost modes (two of them
+sharing one lane of cost/path volumes) is stepped over several keyframes; after every step each
+sequence's fused depth and variance must equal, bit for bit, what a StereoMapper fed the same
+frames and poses returns: the batch runs the same kernels, with the per-step values read from
+device memory instead of kernel parameters.
+"""
+import numpy as np
+import pytest
+
+from probabilistic_mapping_b200 import scene
+from probabilistic_mapping_b200.batch import StereoBatch
+from probabilistic_mapping_b200.mapper import StereoMapper
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+S = 3
+COMMON = dict(intensity_scale=1 / 255, p1=0.003, p2=0.01, tau_so=3.5 / 255, uniqueness_ratio=0.95)
+SEQS = [
+    dict(width=96, height=64, num_planes=64, precision=0, cost_mode=0, num_paths=8),
+    dict(width=128, height=96, num_planes=128, precision=1, cost_mode=1, num_paths=8),
+    dict(width=96, height=64, num_planes=64, precision=0, cost_mode=0, num_paths=4),
+    dict(width=96, height=64, num_planes=64, precision=0, cost_mode=0, num_paths=8),   # shares seq 0's lane
+]
+
+
+def make_configs():
+    out = []
+    for c in SEQS:
+        rho0, _ = scene.plane_range(c["num_planes"])
+        out.append(dict(c, rho0=rho0, **COMMON))
+    return out
+
+
+@pytest.mark.parametrize("host_io,autotune", [(True, False), (False, True)])
+def test_batch_matches_separate_mappers(host_io, autotune):
+    cfgs = make_configs()
+    seqs = [scene.make_sequence(c["width"], c["height"], 0.8 * c["width"], S, 3, seed=50 + i)
+            for i, c in enumerate(cfgs)]
+    b = StereoBatch(cfgs, S, lanes=1, host_io=host_io, autotune=autotune)
+    mappers = []
+    for i, c in enumerate(cfgs):
+        W, H, D = c["width"], c["height"], c["num_planes"]
+        params = {k: v for k, v in c.items() if k not in ("width", "height", "num_planes")}
+        m = StereoMapper(W, H, D, **params)
+        _, drho = scene.plane_range(D)
+        K = seqs[i][0].K
+        m.initIntrinsic(K, 0.0, drho)
+        b.init_intrinsic(i, K, drho)
+        mappers.append(m)
+    if autotune:
+        for i in range(len(cfgs)):
+            w, serial, ms = b.tuning(i)
+            assert w in (2, 4, 8) and serial in (0, 1) and ms > 0
+    for step in range(3):
+        for i, c in enumerate(cfgs):
+            fs = seqs[i][step]
+            frames = [fs.ref] + [fs.srcs[s] for s in range(S)]
+            if not host_io:
+                frames = [torch.from_numpy(np.ascontiguousarray(img)).cuda() for img in frames]
+                torch.cuda.synchronize()   # the batch copies on its own stream
+            for f, img in enumerate(frames):
+                b.set_frame(i, f, img)
+            b.set_poses(i, fs.R_ref, fs.T_ref, list(fs.R_srcs), list(fs.T_srcs))
+        b.run()
+        b.synchronize()
+        for i, c in enumerate(cfgs):
+            fs = seqs[i][step]
+            m = mappers[i]
+            m.initReference(fs.ref)
+            for s in range(S):
+                m.update(fs.srcs[s], fs.R_ref, fs.T_ref, fs.R_srcs[s], fs.T_srcs[s])
+            K = fs.K
+            want_d, want_v = m.outputFusion(fs.R_ref, fs.T_ref, K[0, 0], K[1, 1], K[0, 2], K[1, 2])
+            got_d, got_v = b.output(i) if host_io else b.copy_output(i)
+            assert (got_d.view(np.uint32) == want_d.view(np.uint32)).all(), (step, i)
+            assert (got_v.view(np.uint32) == want_v.view(np.uint32)).all(), (step, i)
+            if step > 0:   # the fusion step produces depths after the first keyframe
+                assert (got_d > 0).mean() > 0.3
+    for m in mappers:
+        m.close()
+    b.close()
