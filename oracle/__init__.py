@@ -70,8 +70,9 @@ class Params:
 
 def build(force: bool = False) -> str:
     """Compile oracle/pm_oracle.cpp (needs g++ with OpenMP)."""
+    srcs = ("pm_oracle.cpp", "pm_oracle_diff.cpp", "pm_oracle.h")
     if force or not os.path.exists(_LIB_PATH) or (
-            os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "pm_oracle.cpp"))):
+            os.path.getmtime(_LIB_PATH) < max(os.path.getmtime(os.path.join(_HERE, f)) for f in srcs)):
         subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
 
@@ -101,6 +102,11 @@ def lib():
                                    f, f, f, f, f, u32]
         L.orc_convert.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                   ctypes.c_int, ctypes.c_uint64]
+        dp = P(OrcDiffParams)
+        L.orc_diff_forward.argtypes = [dp, d, d, d, d, d, d, d, u8]
+        L.orc_diff_forward.restype = ctypes.c_double
+        L.orc_diff_backward.argtypes = [dp, d, d, d, d, d, d, d, d]
+        L.orc_diff_backward.restype = ctypes.c_double
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -312,3 +318,80 @@ class Mapper:
         self.R_prev, self.t_prev = np.array(R, np.float64), np.array(t, np.float64)
         self.pre_index ^= 1
         return st
+
+
+# ---- differentiable form (pm_oracle_diff.cpp) ---------------------------------------------
+class OrcDiffParams(ctypes.Structure):
+    _fields_ = [("W", ctypes.c_int), ("H", ctypes.c_int), ("D", ctypes.c_int), ("S", ctypes.c_int),
+                ("num_paths", ctypes.c_int), ("rho0", ctypes.c_double), ("drho", ctypes.c_double),
+                ("temperature", ctypes.c_double), ("p1", ctypes.c_double), ("p2", ctypes.c_double),
+                ("tau_so", ctypes.c_double), ("q1", ctypes.c_double), ("q2", ctypes.c_double)]
+
+
+@dataclass
+class DiffParams:
+    """The differentiable form: corrected 3x3 cost, 8 SGM paths, soft-argmin at temperature T,
+    L1 loss against the ground-truth inverse depth."""
+    W: int
+    H: int
+    D: int
+    S: int
+    rho0: float
+    drho: float
+    temperature: float = 0.05
+    p1: float = 0.003
+    p2: float = 0.01
+    tau_so: float = 3.5 / 255
+    q1: float = 2.0
+    q2: float = 3.0
+    num_paths: int = 8
+
+    def c(self):
+        return OrcDiffParams(self.W, self.H, self.D, self.S, self.num_paths, self.rho0, self.drho,
+                             self.temperature, self.p1, self.p2, self.tau_so, self.q1, self.q2)
+
+
+def _diff_args(p: DiffParams, ref, srcs, K, R, t, rho_gt):
+    arrs = [_f64(ref).reshape(-1), _f64(srcs).reshape(-1), _f64(K).reshape(-1), _f64(R).reshape(-1),
+            _f64(t).reshape(-1), _f64(rho_gt).reshape(-1)]
+    assert arrs[1].size == p.S * p.W * p.H and arrs[3].size == 9 * p.S and arrs[4].size == 3 * p.S
+    return arrs
+
+
+def diff_forward(p: DiffParams, ref, srcs, K, R, t, rho_gt):
+    """FP64 loss, rho_hat (H, W) and pixel validity of the differentiable form."""
+    a = _diff_args(p, ref, srcs, K, R, t, rho_gt)
+    rho_hat = np.zeros(p.W * p.H)
+    valid = np.zeros(p.W * p.H, np.uint8)
+    cp = p.c()
+    loss = lib().orc_diff_forward(ctypes.byref(cp), *[_ptr(x, ctypes.c_double) for x in a],
+                                  _ptr(rho_hat, ctypes.c_double), _ptr(valid, ctypes.c_uint8))
+    return loss, rho_hat.reshape(p.H, p.W), valid.reshape(p.H, p.W)
+
+
+def diff_backward(p: DiffParams, ref, srcs, K, R, t, rho_gt):
+    """FP64 loss and its gradients: w.r.t. the source images (S, H, W) and w.r.t. the left se(3)
+    perturbation (omega, upsilon) of each source pose (S, 6)."""
+    a = _diff_args(p, ref, srcs, K, R, t, rho_gt)
+    g_srcs = np.zeros(p.S * p.W * p.H)
+    g_pose = np.zeros(6 * p.S)
+    cp = p.c()
+    loss = lib().orc_diff_backward(ctypes.byref(cp), *[_ptr(x, ctypes.c_double) for x in a],
+                                   _ptr(g_srcs, ctypes.c_double), _ptr(g_pose, ctypes.c_double))
+    return loss, g_srcs.reshape(p.S, p.H, p.W), g_pose.reshape(p.S, 6)
+
+
+def so3_exp(w):
+    """Rodrigues' formula, FP64."""
+    w = np.asarray(w, np.float64)
+    th = np.linalg.norm(w)
+    Wx = np.array([[0, -w[2], w[1]], [w[2], 0, -w[0]], [-w[1], w[0], 0]])
+    if th < 1e-12:
+        return np.eye(3) + Wx
+    return np.eye(3) + np.sin(th) / th * Wx + (1 - np.cos(th)) / th ** 2 * (Wx @ Wx)
+
+
+def perturb_pose(R, t, xi):
+    """Left se(3) perturbation of a source-from-reference pose: P -> exp([omega]) P + upsilon."""
+    E = so3_exp(xi[:3])
+    return E @ R, E @ t + np.asarray(xi[3:], np.float64)

@@ -78,7 +78,7 @@ void orc_tree_order(int D, int tree_compat, int32_t* rank, int32_t* incl);
 
 /* a6-a10: GPU depth-fusion step (depth_fusion.cu:8-225) with the races replaced by a
  * deterministic rule: the z-buffer keeps the smallest transformed depth, ties to the smaller
- * pixel index; hole filling takes the first occupied interior 3x3 neighbour in raster order.
+ * pixel index; hole filling takes the last occupied interior 3x3 neighbour in raster order.
  * depth: in = WTA depth, out = fused depth.  pre_* are modified in place like transformMap.
  * pose: float R_p2c[9], t_p2c[3]; cam: fx, fy, cx, cy. */
 void orc_fuse_gpu_f64(int W, int H, const float pose[12], const float cam[4], double* depth,
@@ -101,6 +101,21 @@ void orc_convert(int W, int H, const void* in, void* out, int flag, uint64_t pit
 
 int orc_num_threads(void);
 void orc_set_num_threads(int n);
+
+/* Differentiable form (pm_oracle_diff.cpp): FP64 forward (cost over the corrected 3x3 patch, 8
+ * SGM paths, soft-argmin at temperature T, L1 loss against rho_gt over valid pixels with
+ * rho_gt > 0) and its adjoint.  ref: W*H, srcs: S*W*H scaled intensities; K: 3x3 without skew;
+ * R: S*9, t: S*3 source-from-reference poses.  g_pose: S*6, the left se(3) perturbation
+ * (omega, upsilon) of each source pose. */
+typedef struct orc_diff_params {
+    int W, H, D, S, num_paths;
+    double rho0, drho, temperature;
+    double p1, p2, tau_so, q1, q2;
+} orc_diff_params;
+double orc_diff_forward(const orc_diff_params* p, const double* ref, const double* srcs, const double* K,
+                        const double* R, const double* t, const double* rho_gt, double* rho_hat, uint8_t* valid);
+double orc_diff_backward(const orc_diff_params* p, const double* ref, const double* srcs, const double* K,
+                         const double* R, const double* t, const double* rho_gt, double* g_srcs, double* g_pose);
 
 #ifdef __cplusplus
 }
