@@ -216,6 +216,42 @@ PM_API void* pm_batch_stream(pm_batch* b);
 PM_API const char* pm_batch_last_error(const pm_batch* b);
 
 /* ---------------------------------------------------------------------------------------
+ * Differentiation form (no counterpart in the reference): a differentiable depth loss over the
+ * path and its hand-written adjoint.  Forward: corrected 3x3 cost averaged over the valid
+ * sources, 8 SGM paths (their states kept, or recomputed per path in the backward), soft-argmin
+ * rho_hat = sum_d softmax(-S/T)_d rho_d, loss = mean |rho_hat - rho_gt| over valid pixels with
+ * rho_gt > 0.  Backward: gradients with respect to the source intensities and to the left se(3)
+ * perturbation of every source pose (P_s -> exp([omega]) P_s + upsilon; omega first).
+ * --------------------------------------------------------------------------------------- */
+typedef struct pm_diff pm_diff;
+typedef struct pm_diff_config {
+    int width, height;
+    int num_planes;      /* 32, 64, 128 or 256 */
+    int num_sources;     /* 1 .. 4 */
+    float rho0, rho_step;
+    float temperature;   /* soft-argmin temperature in cost units */
+    float p1, p2, tau_so, q1, q2;
+    int store_paths;     /* 1: keep the 8 path-state volumes from the forward; 0: recompute */
+    int device;
+} pm_diff_config;
+PM_API void pm_diff_config_default(pm_diff_config* c, int width, int height, int num_planes, int num_sources);
+PM_API pm_status pm_diff_create(const pm_diff_config* c, pm_diff** out);
+PM_API void pm_diff_destroy(pm_diff* d);
+/* Device memory the handle holds (bytes). */
+PM_API pm_status pm_diff_memory(const pm_diff* d, size_t* bytes);
+/* ref (W*H), srcs (num_sources*W*H), rho_gt (W*H): device float images (scaled intensities,
+ * ground-truth inverse depth, <= 0 where unknown); K without skew; R (9 per source) and t (3
+ * per source): source-from-reference poses, row-major doubles; rho_hat: optional device W*H
+ * output (0 outside the loss mask); *loss on the host.  The inputs must stay valid for the
+ * backward. */
+PM_API pm_status pm_diff_forward(pm_diff* d, const float* ref, const float* srcs, const double K[9], const double* R,
+                                 const double* t, const float* rho_gt, float* rho_hat, double* loss, void* stream);
+/* Gradients of the last forward's loss: grad_srcs (device, num_sources*W*H, overwritten) and
+ * grad_pose (host, 6 per source: omega then upsilon). */
+PM_API pm_status pm_diff_backward(pm_diff* d, float* grad_srcs, double* grad_pose, void* stream);
+PM_API const char* pm_diff_last_error(const pm_diff* d);
+
+/* ---------------------------------------------------------------------------------------
  * Stage-level calls: one call per reference launch wrapper.  Device pointers, caller-owned
  * buffers, asynchronous on `stream`.  Status codes report argument errors and launch errors.
  * --------------------------------------------------------------------------------------- */

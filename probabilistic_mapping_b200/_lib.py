@@ -44,6 +44,16 @@ class PmConfig(ctypes.Structure):
     ]
 
 
+class PmDiffConfig(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_int), ("height", ctypes.c_int), ("num_planes", ctypes.c_int),
+        ("num_sources", ctypes.c_int), ("rho0", ctypes.c_float), ("rho_step", ctypes.c_float),
+        ("temperature", ctypes.c_float), ("p1", ctypes.c_float), ("p2", ctypes.c_float),
+        ("tau_so", ctypes.c_float), ("q1", ctypes.c_float), ("q2", ctypes.c_float),
+        ("store_paths", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
 class PmBuffers(ctypes.Structure):
     _fields_ = [("cost", ctypes.c_void_p), ("sgm", ctypes.c_void_p), ("wta_index", ctypes.c_void_p),
                 ("wta_depth", ctypes.c_void_p), ("table", ctypes.c_void_p)]
@@ -99,6 +109,13 @@ SIGNATURES = {
     "pm_batch_tuning": (_I, [_VP, _I, _P(_I), _P(_I), _P(_F)]),
     "pm_batch_stream": (_VP, [_VP]),
     "pm_batch_last_error": (ctypes.c_char_p, [_VP]),
+    "pm_diff_config_default": (None, [_P(PmDiffConfig), _I, _I, _I, _I]),
+    "pm_diff_create": (_I, [_P(PmDiffConfig), _P(_VP)]),
+    "pm_diff_destroy": (None, [_VP]),
+    "pm_diff_memory": (_I, [_VP, _P(_SZ)]),
+    "pm_diff_forward": (_I, [_VP, _VP, _VP, _D, _D, _D, _VP, _VP, _D, _VP]),
+    "pm_diff_backward": (_I, [_VP, _VP, _D, _VP]),
+    "pm_diff_last_error": (ctypes.c_char_p, [_VP]),
 }
 
 _lib = None
