@@ -55,6 +55,12 @@ struct pm_mapper {
     int32_t* d_table = nullptr;
     float* d_fused = nullptr;
     float* d_var = nullptr;
+    // CPU fusion variant scratch (allocated when the mapper is created with it)
+    uint8_t* d_cmask = nullptr;
+    float* d_corig = nullptr;
+    int* d_chead = nullptr;
+    int* d_cnext = nullptr;
+    uint32_t* d_ctab = nullptr;
     int pre_index = 0;
     bool first_fusion = true;
     double R_prev[9]{}, t_prev[3]{};
@@ -113,15 +119,19 @@ void compose_homography(const double* K, const double* Rl, const double* Tl, con
     for (int i = 0; i < 3; ++i) out[9 + i] = (float)H2[i];
 }
 
-// R_p2c = R^T R_prev, t_p2c = R^T (t_prev - t) (stereo_mapper.cpp:155-156), as floats.
-void fusion_pose(const double* R, const double* t, const double* R_prev, const double* t_prev, float out[12]) {
-    double RT[9], Rpc[9], tpc[3];
+// R_p2c = R^T R_prev, t_p2c = R^T (t_prev - t) (stereo_mapper.cpp:155-156, :766-767).
+void fusion_pose_d(const double* R, const double* t, const double* R_prev, const double* t_prev, double out[12]) {
+    double RT[9];
     transpose3(R, RT);
-    matmul3(RT, R_prev, Rpc);
+    matmul3(RT, R_prev, out);
     const double dt[3] = {t_prev[0] - t[0], t_prev[1] - t[1], t_prev[2] - t[2]};
-    matvec3(RT, dt, tpc);
-    for (int i = 0; i < 9; ++i) out[i] = (float)Rpc[i];
-    for (int i = 0; i < 3; ++i) out[9 + i] = (float)tpc[i];
+    matvec3(RT, dt, out + 9);
+}
+
+void fusion_pose(const double* R, const double* t, const double* R_prev, const double* t_prev, float out[12]) {
+    double d[12];
+    fusion_pose_d(R, t, R_prev, t_prev, d);
+    for (int i = 0; i < 12; ++i) out[i] = (float)d[i];
 }
 
 }  // namespace pm
@@ -345,6 +355,11 @@ void release(pm_mapper* h) {
     cudaFree(h->d_table);
     cudaFree(h->d_fused);
     cudaFree(h->d_var);
+    cudaFree(h->d_cmask);
+    cudaFree(h->d_corig);
+    cudaFree(h->d_chead);
+    cudaFree(h->d_cnext);
+    cudaFree(h->d_ctab);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
     for (int g = 0; g < 3; ++g) {
@@ -438,6 +453,11 @@ pm_status pm_create(const pm_config* cfg, pm_mapper** out) {
         ok = note(cudaCreateTextureObject(&h->tex[s], &rd, &td, nullptr));
     }
     for (int r = 0; r < cfg->num_paths && ok; ++r) ok = alloc((void**)&h->d_part[r], 4 * V);
+    if (ok && cfg->fusion_variant == PM_FUSION_CPU_PATH) {
+        if (cfg->width >= 65536 || cfg->height >= 65536) ok = note(cudaErrorInvalidValue);
+        ok = ok && alloc((void**)&h->d_cmask, N) && alloc((void**)&h->d_corig, 4 * N) &&
+             alloc((void**)&h->d_chead, 4 * N) && alloc((void**)&h->d_cnext, 4 * N) && alloc((void**)&h->d_ctab, 4 * N);
+    }
     for (int s = 0; s < 2 && ok; ++s)
         for (int k = 0; k < 4 && ok; ++k) ok = alloc((void**)&h->d_state[s][k], 4 * N);
     if (ok) {
@@ -554,8 +574,6 @@ pm_status pm_output_fusion(pm_mapper* h, float* depth, size_t depth_pitch, float
     if (!h->have_ref) return fail(h, PM_ERR_BAD_STATE, "outputFusion before initReference");
     if (!depth) return fail(h, PM_ERR_INVALID_ARGUMENT, "depth pointer is NULL");
     if (!R || !t || !finite_n(R, 9) || !finite_n(t, 3)) return fail(h, PM_ERR_INVALID_ARGUMENT, "pose must be finite");
-    if (h->cfg.fusion_variant != PM_FUSION_GPU)
-        return fail(h, PM_ERR_UNSUPPORTED, "fusion_variant %d is not available in this build", h->cfg.fusion_variant);
     DeviceGuard g(h->cfg.device);
     const int W = h->cfg.width, H = h->cfg.height;
     const size_t N = (size_t)W * H;
@@ -575,6 +593,30 @@ pm_status pm_output_fusion(pm_mapper* h, float* depth, size_t depth_pitch, float
         PM_CK(h, cudaMemsetAsync(h->d_state[1][0], 0, 4 * N, h->stream));
         PM_CK(h, cudaMemsetAsync(h->d_fused, 0, 4 * N, h->stream));
         PM_CK(h, cudaMemsetAsync(h->d_var, 0, 4 * N, h->stream));
+    } else if (h->cfg.fusion_variant == PM_FUSION_CPU_PATH) {   // outputFusionCPU (:741-804)
+        FuseCpuLaunch f;
+        std::memset(&f, 0, sizeof f);
+        f.W = W;
+        f.H = H;
+        fusion_pose_d(R, t, h->R_prev, h->t_prev, f.pose);
+        f.cam[0] = fx; f.cam[1] = fy; f.cam[2] = cx; f.cam[3] = cy;
+        PM_CK(h, cudaMemcpyAsync(h->d_fused, h->d_depth, 4 * N, cudaMemcpyDeviceToDevice, h->stream));
+        f.result = h->d_fused;
+        for (int k = 0; k < 4; ++k) {
+            f.pre[k] = h->d_state[h->pre_index][k];
+            f.cur[k] = h->d_state[h->pre_index ^ 1][k];
+        }
+        f.table = reinterpret_cast<uint32_t*>(h->d_table);
+        f.variance = h->d_var;
+        f.mask = h->d_cmask;
+        f.orig_mu = h->d_corig;
+        f.head = h->d_chead;
+        f.next = h->d_cnext;
+        f.tab0 = h->d_ctab;
+        PM_CK(h, launch_fuse_cpu_variant(f, h->stream));
+        std::memcpy(h->R_prev, R, sizeof h->R_prev);
+        std::memcpy(h->t_prev, t, sizeof h->t_prev);
+        h->pre_index ^= 1;
     } else {
         FuseLaunch f;
         std::memset(&f, 0, sizeof f);

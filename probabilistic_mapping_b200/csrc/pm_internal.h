@@ -117,6 +117,25 @@ struct FuseLaunch {
 };
 cudaError_t launch_fuse_gpu(const FuseLaunch& a, cudaStream_t s);
 
+// The CPU fusion variant (outputFusionCPU, stereo_mapper.cpp:625-820) run on the GPU.
+struct FuseCpuLaunch {
+    int W, H;              // both below 65536 (packed (y << 16) | x table)
+    double pose[12];       // R_p2c row-major, t_p2c (double, as the reference's Eigen code)
+    float cam[4];          // fx, fy, cx, cy
+    float* result;         // in: WTA depth, out: fused and masked depth (W*H)
+    float* pre[4];         // alpha, beta, mu, sigma of the previous keyframe (modified)
+    float* cur[4];         // state of the current keyframe
+    uint32_t* table;       // W*H filled propagation table, packed (y << 16) | x (optional)
+    float* variance;       // W*H sigma^2 of the current state (optional)
+    // scratch, W*H each
+    uint8_t* mask;
+    float* orig_mu;
+    int* head;
+    int* next;
+    uint32_t* tab0;
+};
+cudaError_t launch_fuse_cpu_variant(const FuseCpuLaunch& a, cudaStream_t s);
+
 // ---- host-side geometry, FP64 (api.cu) -----------------------------------------------------
 void matmul3(const double* A, const double* B, double* C);
 void matvec3(const double* A, const double* x, double* y);
@@ -127,5 +146,6 @@ void compose_homography(const double* K, const double* Rl, const double* Tl, con
                         const double* Tr, float out[12]);
 // relative pose of the previous keyframe in the current one (stereo_mapper.cpp:155-156), 12 floats
 void fusion_pose(const double* R, const double* t, const double* R_prev, const double* t_prev, float out[12]);
+void fusion_pose_d(const double* R, const double* t, const double* R_prev, const double* t_prev, double out[12]);
 
 }  // namespace pm
