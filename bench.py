@@ -240,11 +240,13 @@ def run_ours(args, rank, world, precision: str = "fp32", passes=("dev", "e2e", "
 
 
 def max_over_ranks(vals, world):
+    """Element-wise maximum of the ranks' values (device tensors over nccl, host over gloo)."""
     if world <= 1:
         return vals
     import torch
     import torch.distributed as dist
-    t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(vals, dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return t.tolist()
 
