@@ -124,6 +124,20 @@ PM_API pm_status pm_output_fusion(pm_mapper* h, float* depth, size_t depth_pitch
                            size_t variance_pitch, const double R[9], const double t[3],
                            float fx, float fy, float cx, float cy);
 
+/* The debug outputs of outputFusionCPU, selected there by the global CASE (stereo_mapper.cpp:
+ * 628-719; evaluate.cc:314-319 reads it from argv[1], default 0):
+ *   PM_CASE_RAW_ARGMIN  argmin of the plane-sweep cost itself (:628-662);
+ *   PM_CASE_SGM_ARGMIN  argmin of the SGM sum (:668-706);
+ *   PM_CASE_FILTERED    the winner-take-all filter's depth, as pm_output (:712-719).
+ * The argmin outputs scan the planes in order (first strict minimum below 100000 wins) and write
+ * 10000 where |min| < 1e-5, 0 at the first and last plane, else 1 / (rho0 + d * rho_step) with no
+ * subpixel refinement.  CASE >= 3 is pm_output_fusion with PM_FUSION_CPU_PATH.  pm_get_wta_index
+ * afterwards gives the argmin's plane.  The fusion state is not touched. */
+#define PM_CASE_RAW_ARGMIN 0
+#define PM_CASE_SGM_ARGMIN 1
+#define PM_CASE_FILTERED 2
+PM_API pm_status pm_output_case(pm_mapper* h, int output_case, float* result, size_t pitch_bytes);
+
 /* The winner-take-all depth of the last output call (the reference's `dep`). */
 PM_API pm_status pm_get_wta_depth(pm_mapper* h, float* depth, size_t pitch_bytes);
 
@@ -309,6 +323,54 @@ PM_API pm_status pm_stage_depth_fuse_noalloc(int W, int H, const float pose[12],
  * pitch is in BYTES (the reference passed a byte step but indexed with it in floats). */
 PM_API pm_status pm_stage_convert(int W, int H, const float* in, float* out, int flag,
                            size_t pitch_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Sequence tools: the image work and the output formats of the reference's driver
+ * (evaluate.cc).  Kernels take device pointers and byte pitches (0 = packed) and run on
+ * `stream`; the file functions take host memory.
+ * --------------------------------------------------------------------------------------- */
+
+/* cv::pyrDown(img, img, Size(W/2, H/2)) (evaluate.cc:176-178, 221-225): 5x5 binomial filter
+ * [1 4 6 4 1]^T [1 4 6 4 1] / 256 at even pixels, mirrored borders (BORDER_REFLECT_101), rounded
+ * half up.  dst is (W/2) x (H/2).  W, H >= 2. */
+PM_API pm_status pm_pyr_down_u8(int W, int H, const uint8_t* src, size_t src_pitch, uint8_t* dst,
+                                size_t dst_pitch, void* stream);
+
+/* depthUp (evaluate.cc:121-135): each pixel of the W x H float map repeated in a 2x2 block of
+ * the 2W x 2H dst. */
+PM_API pm_status pm_depth_up2(int W, int H, const float* src, size_t src_pitch, float* dst, size_t dst_pitch,
+                              void* stream);
+
+/* The depth range mask of evaluate.cc:278-289, in place: depth < min_depth -> 0, then
+ * depth > max_depth -> 0 (the driver uses 0.2 and 20). */
+PM_API pm_status pm_depth_range_mask(int W, int H, float* depth, size_t pitch, float min_depth, float max_depth,
+                                     void* stream);
+
+/* The debug view of evaluate.cc:291-307.  level (optional, W x H bytes) receives
+ * cv::normalize(depth, 0, 255, NORM_MINMAX, CV_8U); bgr (optional, 3 bytes per pixel, B G R)
+ * receives a colour map of that level with pixels of depth < 0.001 black.  The colour map is
+ * this library's own hue ramp (red, yellow, green, cyan, blue, magenta), not OpenCV's
+ * COLORMAP_RAINBOW table.  scratch: 2 unsigned ints of device memory. */
+PM_API pm_status pm_colorize_depth(int W, int H, const float* depth, size_t pitch, uint8_t* level,
+                                   size_t level_pitch, uint8_t* bgr, size_t bgr_pitch, unsigned* scratch,
+                                   void* stream);
+
+/* The depth output message of evaluate.cc:271-276 (sensor_msgs/Image "32FC1", filled by
+ * toImageMsg, src/tools/transport_util.h:103-132) becomes a file: PFM ("Pf", little-endian,
+ * rows stored bottom-up as the format requires) or NPY (version 1.0, '<f4', shape (H, W)).
+ * Host memory; pitch in bytes (0 = packed).  PM_ERR_INVALID_ARGUMENT when the file cannot be
+ * written. */
+PM_API pm_status pm_write_pfm(const char* path, int W, int H, const float* data, size_t pitch);
+PM_API pm_status pm_write_npy(const char* path, int W, int H, const float* data, size_t pitch);
+/* A B G R 8-bit image (pm_colorize_depth's bgr) as binary PPM (P6). */
+PM_API pm_status pm_write_ppm(const char* path, int W, int H, const uint8_t* bgr, size_t pitch);
+
+/* Reads an 8-bit frame for the driver: binary PGM/PPM (P5/P6), PNG (8-bit grey, grey+alpha,
+ * palette, RGB, RGBA; 16-bit grey and RGB keep the high byte; not interlaced) or a 2-D uint8 NPY.
+ * Colour becomes grey as cv::cvtColor(RGB2GRAY) does: (9798 R + 19235 G + 3735 B + 16384) >> 15.
+ * Writes the size to *W, *H; with dst == NULL (or capacity too small, then
+ * PM_ERR_INVALID_ARGUMENT) only the size.  dst rows are packed (pitch W). */
+PM_API pm_status pm_read_image_u8(const char* path, int* W, int* H, uint8_t* dst, size_t capacity);
 
 #ifdef __cplusplus
 }

@@ -28,6 +28,9 @@ PM_BATCH_HOST_IO = 1
 PM_BATCH_AUTOTUNE = 2
 PM_FUSION_GPU = 0
 PM_FUSION_CPU_PATH = 1
+PM_CASE_RAW_ARGMIN = 0
+PM_CASE_SGM_ARGMIN = 1
+PM_CASE_FILTERED = 2
 
 
 class PmConfig(ctypes.Structure):
@@ -72,6 +75,7 @@ SIGNATURES = {
     "pm_update": (_I, [_VP, _VP, _SZ, _D, _D, _D, _D]),
     "pm_output": (_I, [_VP, _VP, _SZ]),
     "pm_output_fusion": (_I, [_VP, _VP, _SZ, _VP, _SZ, _D, _D, _F, _F, _F, _F]),
+    "pm_output_case": (_I, [_VP, _I, _VP, _SZ]),
     "pm_get_wta_depth": (_I, [_VP, _VP, _SZ]),
     "pm_get_wta_index": (_I, [_VP, _VP]),
     "pm_get_state": (_I, [_VP, _VP, _VP, _VP, _VP]),
@@ -116,6 +120,14 @@ SIGNATURES = {
     "pm_diff_forward": (_I, [_VP, _VP, _VP, _D, _D, _D, _VP, _VP, _D, _VP]),
     "pm_diff_backward": (_I, [_VP, _VP, _D, _VP]),
     "pm_diff_last_error": (ctypes.c_char_p, [_VP]),
+    "pm_pyr_down_u8": (_I, [_I, _I, _VP, _SZ, _VP, _SZ, _VP]),
+    "pm_depth_up2": (_I, [_I, _I, _VP, _SZ, _VP, _SZ, _VP]),
+    "pm_depth_range_mask": (_I, [_I, _I, _VP, _SZ, _F, _F, _VP]),
+    "pm_colorize_depth": (_I, [_I, _I, _VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, _VP]),
+    "pm_write_pfm": (_I, [ctypes.c_char_p, _I, _I, _VP, _SZ]),
+    "pm_write_npy": (_I, [ctypes.c_char_p, _I, _I, _VP, _SZ]),
+    "pm_write_ppm": (_I, [ctypes.c_char_p, _I, _I, _VP, _SZ]),
+    "pm_read_image_u8": (_I, [ctypes.c_char_p, _P(_I), _P(_I), _VP, _SZ]),
 }
 
 _lib = None

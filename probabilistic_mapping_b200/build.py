@@ -1,7 +1,7 @@
 """Build recipe for libpm_stereo.so (sm_100a).
 
-Compiles every .cu under csrc/ with nvcc for sm_100a and links one shared library next to
-this file.  -fmad=false: FP32 expressions are written with explicit fused/unfused
+Compiles every .cu under csrc/ with nvcc for sm_100a (and the host-only .cpp files there with
+g++) and links one shared library next to this file.  -fmad=false: FP32 expressions are written with explicit fused/unfused
 intrinsics, so the compiler must not contract multiply-adds on its own (the CPU oracle replays
 the same operation order).
 """
@@ -19,6 +19,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libpm_stereo.so")
+CLI_SRC = os.path.join(HERE, "cli", "pm_sequence.cpp")
+CLI = os.path.join(HERE, "pm_sequence")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
@@ -33,14 +35,45 @@ def nvcc() -> str:
     return path
 
 
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+
+
 def _sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
 
+def _host_sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cpp")))
+
+
 def _deps_mtime() -> float:
-    files = _sources() + glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
+    files = _sources() + _host_sources() + glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
         glob.glob(os.path.join(ROOT, "include", "*.h")) + [os.path.abspath(__file__)]
     return max(os.path.getmtime(f) for f in files)
+
+
+def cuda_home() -> str:
+    return os.path.dirname(os.path.dirname(os.path.realpath(nvcc())))
+
+
+def build_cli(force: bool = False) -> str:
+    """The headless sequence driver: cli/pm_sequence.cpp linked against libpm_stereo.so (found
+    next to the binary through its rpath) and the static CUDA runtime."""
+    newest = max(os.path.getmtime(CLI_SRC), os.path.getmtime(LIB),
+                 max(os.path.getmtime(f) for f in glob.glob(os.path.join(ROOT, "include", "*.h"))))
+    if not force and os.path.exists(CLI) and os.path.getmtime(CLI) >= newest:
+        return CLI
+    cuda = cuda_home()
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(cuda, "include"),
+           CLI_SRC, "-o", CLI + ".tmp", "-L", HERE, "-lpm_stereo", "-Wl,-rpath,$ORIGIN",
+           "-L", os.path.join(cuda, "lib64"), "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"building pm_sequence failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(CLI + ".tmp", CLI)
+    return CLI
 
 
 def _compile(src: str, extra: list[str]) -> str:
@@ -54,20 +87,32 @@ def _compile(src: str, extra: list[str]) -> str:
     return obj
 
 
+def _compile_host(src: str) -> str:
+    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+    cxx = shutil.which("g++") or "g++"
+    r = subprocess.run([cxx] + CXX_FLAGS + ["-c", src, "-o", obj], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"g++ failed on {src}:\n{r.stdout}\n{r.stderr}")
+    return obj
+
+
 def build(force: bool = False, verbose_ptxas: bool = False) -> str:
     """Compile csrc/*.cu for sm_100a into libpm_stereo.so (skipped when up to date)."""
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _deps_mtime():
+        build_cli()
         return LIB
     os.makedirs(BUILD, exist_ok=True)
     extra = ["-Xptxas", "-v"] if verbose_ptxas else []
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, extra), _sources()))
+        objs += list(ex.map(_compile_host, _host_sources()))
     tmp = LIB + ".tmp"
-    cmd = [nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcuda"]
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcuda", "-lz"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, LIB)
+    build_cli(force=True)
     return LIB
 
 

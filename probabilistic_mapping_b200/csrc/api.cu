@@ -305,7 +305,7 @@ pm_status run_sgm_filter(pm_mapper* h) {
     a.depth = h->d_depth;
     a.depth_pitch = sizeof(float) * (size_t)c.width;
     a.index = h->d_idx;
-    PM_CK(h, launch_sgm(a, true, h->stream, h->have_side ? &h->side : nullptr));
+    PM_CK(h, launch_sgm(a, kCombineFilter, h->stream, h->have_side ? &h->side : nullptr));
     return PM_OK;
 }
 
@@ -568,6 +568,41 @@ pm_status pm_output(pm_mapper* h, float* depth, size_t pitch) {
     return st;
 }
 
+pm_status pm_output_case(pm_mapper* h, int output_case, float* result, size_t pitch) {
+    if (!h) return PM_ERR_INVALID_ARGUMENT;
+    if (output_case == PM_CASE_FILTERED) return pm_output(h, result, pitch);
+    if (output_case != PM_CASE_RAW_ARGMIN && output_case != PM_CASE_SGM_ARGMIN)
+        return fail(h, PM_ERR_INVALID_ARGUMENT, "output_case %d is not 0, 1 or 2", output_case);
+    if (!h->have_ref) return fail(h, PM_ERR_BAD_STATE, "output before initReference");
+    if (!result) return fail(h, PM_ERR_INVALID_ARGUMENT, "result pointer is NULL");
+    DeviceGuard g(h->cfg.device);
+    const pm_config& c = h->cfg;
+    for (bool& v : h->ev_valid) v = false;
+    mark(h, 0);
+    pm_status st = evaluate_cost(h, false);
+    mark_done(h, 0);
+    if (st != PM_OK) return st;
+    SgmLaunch a;
+    fill_sgm_launch(c, h->order, a);
+    if (output_case == PM_CASE_RAW_ARGMIN) {   // stereo_mapper.cpp:628-662
+        PM_CK(h, launch_case_argmin(h->d_cost, a.cost_half, c.width, c.height, c.num_planes, a.fp, h->d_fused,
+                                    sizeof(float) * (size_t)c.width, h->d_idx, h->stream));
+    } else {                                   // stereo_mapper.cpp:668-706
+        a.cost = h->d_cost;
+        a.ref = h->d_ref;
+        for (int r = 0; r < c.num_paths; ++r) a.part[r] = h->d_part[r];
+        a.depth = h->d_fused;
+        a.depth_pitch = sizeof(float) * (size_t)c.width;
+        a.index = h->d_idx;
+        PM_CK(h, launch_sgm(a, kCombineArgmin, h->stream, h->have_side ? &h->side : nullptr));
+    }
+    mark_done(h, 1);
+    mark(h, 3);
+    st = copy_out(h, result, pitch, h->d_fused);
+    mark_done(h, 3);
+    return st;
+}
+
 pm_status pm_output_fusion(pm_mapper* h, float* depth, size_t depth_pitch, float* variance, size_t var_pitch,
                            const double R[9], const double t[3], float fx, float fy, float cx, float cy) {
     if (!h) return PM_ERR_INVALID_ARGUMENT;
@@ -806,7 +841,7 @@ pm_status pm_stage_sgm(const pm_config* cfg, const float* cost, const float* ref
     a.part[0] = out;   // the combine kernel reads part[0] of a pixel before it writes the total there
     for (int r = 1; r < cfg->num_paths; ++r) a.part[r] = scratch + (r - 1) * V;
     a.total = out;
-    return launch_sgm(a, false, (cudaStream_t)stream, nullptr) == cudaSuccess ? PM_OK : PM_ERR_CUDA;
+    return launch_sgm(a, kCombineStore, (cudaStream_t)stream, nullptr) == cudaSuccess ? PM_OK : PM_ERR_CUDA;
 }
 
 pm_status pm_stage_filter(const pm_config* cfg, const float* sgm, float* depth, size_t pitch, int32_t* index,
@@ -841,7 +876,7 @@ pm_status pm_stage_sgm_filter(const pm_config* cfg, const float* cost, const flo
     a.depth = depth;
     a.depth_pitch = pitch;
     a.index = index;
-    return launch_sgm(a, true, (cudaStream_t)stream, nullptr) == cudaSuccess ? PM_OK : PM_ERR_CUDA;
+    return launch_sgm(a, kCombineFilter, (cudaStream_t)stream, nullptr) == cudaSuccess ? PM_OK : PM_ERR_CUDA;
 }
 
 pm_status pm_stage_depth_fuse(int W, int H, const float pose[12], const float cam[4], float* depth,

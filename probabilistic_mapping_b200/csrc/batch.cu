@@ -252,7 +252,7 @@ cudaError_t enqueue_seq(pm_batch* b, int i, int k) {
     a.cost_half = half;
     if ((e = launch_cost(a, m))) return e;
     const SgmLaunch g = sgm_launch(q, l);
-    if ((e = launch_sgm(g, true, m, &q.side))) return e;
+    if ((e = launch_sgm(g, kCombineFilter, m, &q.side))) return e;
     if ((e = cudaEventRecord(q.lane_free, m))) return e;
     // fusion (stereo_mapper.cpp:111-244) with the step's pose, flags and state index from d_par
     if ((e = cudaMemcpyAsync(q.d_fused, q.d_depth, 4 * N, cudaMemcpyDeviceToDevice, m))) return e;
@@ -332,9 +332,9 @@ pm_status autotune(pm_batch* b) {
                 q.pair_warps = w;
                 q.serial_pairs = serial;
                 const SgmLaunch g = sgm_launch(q, l);
-                e = launch_sgm(g, true, b->run, &q.side);   // warm-up
+                e = launch_sgm(g, kCombineFilter, b->run, &q.side);   // warm-up
                 if (e == cudaSuccess) e = cudaEventRecord(t0, b->run);
-                for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = launch_sgm(g, true, b->run, &q.side);
+                for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = launch_sgm(g, kCombineFilter, b->run, &q.side);
                 if (e == cudaSuccess) e = cudaEventRecord(t1, b->run);
                 if (e == cudaSuccess) e = cudaEventSynchronize(t1);
                 float ms = 0.0f;

@@ -11,6 +11,7 @@ constexpr int kMaxSources = 32;   // source frames evaluated in one cost pass
 constexpr int kMaxPlanes = 256;   // 32 lanes x up to 8 planes per lane
 constexpr float kDepInf = 1000.0f;   // DEP_INF (parameters.h:29)
 constexpr double kFloatEps = 1e-5;   // FLOAT_EPS (parameters.h:6)
+constexpr float kCaseInf = 10000.0f; // no-overlap value of the CASE 0/1 debug outputs (stereo_mapper.cpp:651)
 
 // ---- plane-sweep cost volume (calc_cost.cu) ----------------------------------------------
 struct CostLaunch {
@@ -70,9 +71,15 @@ struct SgmStreams {
     cudaEvent_t fork;
     cudaEvent_t join[3];
 };
+// What the combine kernel does with the summed path volumes.
+enum CombineMode { kCombineStore = 0, kCombineFilter = 1, kCombineArgmin = 2 };
 // Runs the opposite-path pairs (each path into part[r]), then adds the path volumes pairwise in
-// registers and, with fuse_filter, writes depth/index.  side == nullptr runs everything on s.
-cudaError_t launch_sgm(const SgmLaunch& a, bool fuse_filter, cudaStream_t s, const SgmStreams* side);
+// registers and writes depth/index with the winner-take-all filter (kCombineFilter) or the debug
+// argmin (kCombineArgmin); kCombineStore only writes `total`.  side == nullptr runs everything on s.
+cudaError_t launch_sgm(const SgmLaunch& a, int mode, cudaStream_t s, const SgmStreams* side);
+// The debug argmin over a float (half = 0) or __half (half = 1) W*H*D volume.
+cudaError_t launch_case_argmin(const void* vol, int half, int W, int H, int D, const FilterParams& fp, float* depth,
+                               size_t pitch, int32_t* index, cudaStream_t s);
 cudaError_t launch_filter(const float* sum, int W, int H, int D, const FilterParams& fp,
                           const PlaneOrder& order, float* depth, size_t pitch, int32_t* index,
                           cudaStream_t s);

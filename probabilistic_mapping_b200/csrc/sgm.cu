@@ -163,6 +163,31 @@ __device__ __forceinline__ void wta_filter(const float (&s)[PPL], uint32_t incl,
     idx_out = idx;
 }
 
+// The debug winner-take-all of outputFusionCPU's CASE 0 and CASE 1 (stereo_mapper.cpp:636-660,
+// 680-704): planes scanned in order from a minimum of 100000, the first strictly smaller value
+// wins (so ties go to the lower plane); |min| < FLOAT_EPS gives 10000, the first and last plane
+// give 0, otherwise the depth of the plane itself, 1 / (rho0 + d * drho), without subpixel
+// refinement.  When no plane is below 100000 the reference leaves its index unset; plane 0 (and
+// so 0) is reported here.
+template <int PPL>
+__device__ __forceinline__ void case_argmin(const float (&s)[PPL], int lane, int D, const FilterParams& fp,
+                                            float& out, int& idx_out) {
+    float m = 100000.0f;
+    unsigned mi = 0xffffffffu;
+#pragma unroll
+    for (int j = 0; j < PPL; ++j)
+        if (s[j] < m) { m = s[j]; mi = (unsigned)(lane * PPL + j); }
+    const float mn = warp_min_f32(m);
+    const unsigned r = __reduce_min_sync(kFull, m == mn ? mi : 0xffffffffu);
+    const int idx = r < (unsigned)D ? (int)r : 0;
+    float v;
+    if ((double)mn < kFloatEps) v = kCaseInf;
+    else if (idx == 0 || idx == D - 1) v = 0.0f;
+    else v = __frcp_rn(__fmaf_rn((float)idx, fp.drho, fp.rho0));
+    out = v;
+    idx_out = idx;
+}
+
 template <bool HALF> struct CostElem;
 template <> struct CostElem<false> { using T = float; };
 template <> struct CostElem<true> { using T = __half; };
@@ -311,9 +336,10 @@ __global__ void __launch_bounds__(NW * 32) sgm_pair_kernel(const SgmLaunch a, in
 }
 
 // Sum of the path volumes in the pairwise order (P0 + P1) + (P2 + P3) [+ ((P4 + P5) + (P6 + P7))],
-// then (FILTER) the winner-take-all or (!FILTER) a store of the sum.  One warp per pixel,
-// grid-stride; the next pixel's path slices are loaded before the current one is reduced.
-template <int PPL, bool FILTER, int NP>
+// then the winner-take-all filter (MODE kCombineFilter), the debug argmin (kCombineArgmin) or
+// only a store of the sum (kCombineStore).  One warp per pixel, grid-stride; the next pixel's
+// path slices are loaded before the current one is reduced.
+template <int PPL, int MODE, int NP>
 __global__ void __launch_bounds__(256) combine_kernel(const SgmLaunch a) {
     const int lane = threadIdx.x & 31;
     const long nw = (long)gridDim.x * (blockDim.x >> 5);
@@ -342,10 +368,11 @@ __global__ void __launch_bounds__(256) combine_kernel(const SgmLaunch a) {
                 o[j] = s4;
         }
         if (a.total) store_planes<PPL>(a.total + (size_t)pix * D + lane * PPL, o);
-        if constexpr (FILTER) {
+        if constexpr (MODE != kCombineStore) {
             float depth;
             int idx;
-            wta_filter<PPL>(o, incl, rk, lane, D, a.fp, depth, idx);
+            if constexpr (MODE == kCombineFilter) wta_filter<PPL>(o, incl, rk, lane, D, a.fp, depth, idx);
+            else case_argmin<PPL>(o, lane, D, a.fp, depth, idx);
             if (lane == 0) {
                 const int y = (int)(pix / a.W), x = (int)(pix - (long)y * a.W);
                 *reinterpret_cast<float*>(reinterpret_cast<char*>(a.depth) + (size_t)y * a.depth_pitch +
@@ -382,6 +409,32 @@ __global__ void __launch_bounds__(128) filter_kernel(const float* __restrict__ s
     }
 }
 
+// CASE 0 of outputFusionCPU: the debug argmin straight on the plane-sweep cost volume.
+template <int PPL, bool HALF>
+__global__ void __launch_bounds__(128) case_kernel(const void* __restrict__ vol, int W, int H, int D,
+                                                   const FilterParams fp, float* depth, size_t pitch,
+                                                   int32_t* index) {
+    const int lane = threadIdx.x & 31;
+    const long pix = (long)blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (pix >= (long)W * H) return;
+    float s[PPL];
+    if constexpr (HALF) {
+        const __half* p = static_cast<const __half*>(vol) + (size_t)pix * D + lane * PPL;
+#pragma unroll
+        for (int j = 0; j < PPL; ++j) s[j] = __half2float(p[j]);
+    } else {
+        load_planes<PPL>(s, static_cast<const float*>(vol) + (size_t)pix * D + lane * PPL);
+    }
+    float dep;
+    int idx;
+    case_argmin<PPL>(s, lane, D, fp, dep, idx);
+    if (lane == 0) {
+        const int y = (int)(pix / W), x = (int)(pix - (long)y * W);
+        *reinterpret_cast<float*>(reinterpret_cast<char*>(depth) + (size_t)y * pitch + (size_t)x * 4) = dep;
+        if (index) index[pix] = idx;
+    }
+}
+
 // Path r of the reference order (L->R, R->L, T->B, B->T, then TL->BR, BR->TL, TR->BL, BL->TR);
 // pair p = paths (2p, 2p+1) runs as one sgm_pair_kernel along direction kDirs[2p].
 const int kDirs[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1}, {-1, 1}, {1, -1}};
@@ -411,7 +464,7 @@ cudaError_t launch_pair(const SgmLaunch& a, int pair, cudaStream_t s) {
 }
 
 template <int PPL>
-cudaError_t launch_combine(const SgmLaunch& a, bool fuse_filter, cudaStream_t s) {
+cudaError_t launch_combine(const SgmLaunch& a, int mode, cudaStream_t s) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -419,17 +472,19 @@ cudaError_t launch_combine(const SgmLaunch& a, bool fuse_filter, cudaStream_t s)
     const long blocks_needed = (npix + 7) / 8;   // 8 warps per block
     const int blocks = (int)(blocks_needed < (long)sms * 8 ? blocks_needed : (long)sms * 8);
     const bool eight = a.num_paths == 8;
-    if (fuse_filter && eight) combine_kernel<PPL, true, 8><<<blocks, 256, 0, s>>>(a);
-    else if (fuse_filter) combine_kernel<PPL, true, 4><<<blocks, 256, 0, s>>>(a);
-    else if (eight) combine_kernel<PPL, false, 8><<<blocks, 256, 0, s>>>(a);
-    else combine_kernel<PPL, false, 4><<<blocks, 256, 0, s>>>(a);
+    if (mode == kCombineFilter && eight) combine_kernel<PPL, kCombineFilter, 8><<<blocks, 256, 0, s>>>(a);
+    else if (mode == kCombineFilter) combine_kernel<PPL, kCombineFilter, 4><<<blocks, 256, 0, s>>>(a);
+    else if (mode == kCombineArgmin && eight) combine_kernel<PPL, kCombineArgmin, 8><<<blocks, 256, 0, s>>>(a);
+    else if (mode == kCombineArgmin) combine_kernel<PPL, kCombineArgmin, 4><<<blocks, 256, 0, s>>>(a);
+    else if (eight) combine_kernel<PPL, kCombineStore, 8><<<blocks, 256, 0, s>>>(a);
+    else combine_kernel<PPL, kCombineStore, 4><<<blocks, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 
 // Path pairs p = 0 .. num_paths/2 - 1: pairs 0..np-2 run on their own side streams when `side`
 // is given, the last on `s`, which then joins the others and runs the combine kernel.
 template <int PPL, bool HALF>
-cudaError_t launch_sgm_t(const SgmLaunch& a, bool fuse_filter, cudaStream_t s, const SgmStreams* side) {
+cudaError_t launch_sgm_t(const SgmLaunch& a, int mode, cudaStream_t s, const SgmStreams* side) {
     const int np = a.num_paths / 2;
     cudaError_t e = cudaSuccess;
     if (a.serial_pairs) side = nullptr;
@@ -448,7 +503,7 @@ cudaError_t launch_sgm_t(const SgmLaunch& a, bool fuse_filter, cudaStream_t s, c
     if (side)
         for (int p = 0; p < np - 1; ++p)
             if ((e = cudaStreamWaitEvent(s, side->join[p], 0)) != cudaSuccess) return e;
-    return launch_combine<PPL>(a, fuse_filter, s);
+    return launch_combine<PPL>(a, mode, s);
 }
 
 template <int PPL>
@@ -462,23 +517,23 @@ cudaError_t launch_filter_t(const float* sum, int W, int H, int D, const FilterP
 
 }  // namespace
 
-cudaError_t launch_sgm(const SgmLaunch& a, bool fuse_filter, cudaStream_t s, const SgmStreams* side) {
+cudaError_t launch_sgm(const SgmLaunch& a, int mode, cudaStream_t s, const SgmStreams* side) {
     const int ppl = a.D / 32;
     // FP16 volumes need an even number of planes per lane (4-byte cp.async pieces)
     if (a.cost_half && (ppl % 2)) return cudaErrorInvalidValue;
     switch (ppl) {
-        case 1: return launch_sgm_t<1, false>(a, fuse_filter, s, side);
-        case 2: return a.cost_half ? launch_sgm_t<2, true>(a, fuse_filter, s, side)
-                                   : launch_sgm_t<2, false>(a, fuse_filter, s, side);
-        case 3: return launch_sgm_t<3, false>(a, fuse_filter, s, side);
-        case 4: return a.cost_half ? launch_sgm_t<4, true>(a, fuse_filter, s, side)
-                                   : launch_sgm_t<4, false>(a, fuse_filter, s, side);
-        case 5: return launch_sgm_t<5, false>(a, fuse_filter, s, side);
-        case 6: return a.cost_half ? launch_sgm_t<6, true>(a, fuse_filter, s, side)
-                                   : launch_sgm_t<6, false>(a, fuse_filter, s, side);
-        case 7: return launch_sgm_t<7, false>(a, fuse_filter, s, side);
-        case 8: return a.cost_half ? launch_sgm_t<8, true>(a, fuse_filter, s, side)
-                                   : launch_sgm_t<8, false>(a, fuse_filter, s, side);
+        case 1: return launch_sgm_t<1, false>(a, mode, s, side);
+        case 2: return a.cost_half ? launch_sgm_t<2, true>(a, mode, s, side)
+                                   : launch_sgm_t<2, false>(a, mode, s, side);
+        case 3: return launch_sgm_t<3, false>(a, mode, s, side);
+        case 4: return a.cost_half ? launch_sgm_t<4, true>(a, mode, s, side)
+                                   : launch_sgm_t<4, false>(a, mode, s, side);
+        case 5: return launch_sgm_t<5, false>(a, mode, s, side);
+        case 6: return a.cost_half ? launch_sgm_t<6, true>(a, mode, s, side)
+                                   : launch_sgm_t<6, false>(a, mode, s, side);
+        case 7: return launch_sgm_t<7, false>(a, mode, s, side);
+        case 8: return a.cost_half ? launch_sgm_t<8, true>(a, mode, s, side)
+                                   : launch_sgm_t<8, false>(a, mode, s, side);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -495,6 +550,27 @@ cudaError_t launch_filter(const float* sum, int W, int H, int D, const FilterPar
         case 6: return launch_filter_t<6>(sum, W, H, D, fp, order, depth, pitch, index, s);
         case 7: return launch_filter_t<7>(sum, W, H, D, fp, order, depth, pitch, index, s);
         case 8: return launch_filter_t<8>(sum, W, H, D, fp, order, depth, pitch, index, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int PPL, bool HALF>
+cudaError_t launch_case_t(const void* vol, int W, int H, int D, const FilterParams& fp, float* depth, size_t pitch,
+                          int32_t* index, cudaStream_t s) {
+    const long n = (long)W * H;
+    case_kernel<PPL, HALF><<<(unsigned)((n + 3) / 4), 128, 0, s>>>(vol, W, H, D, fp, depth, pitch, index);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_case_argmin(const void* vol, int half, int W, int H, int D, const FilterParams& fp, float* depth,
+                               size_t pitch, int32_t* index, cudaStream_t s) {
+    switch (D / 32) {
+#define PM_CASE_PPL(P) \
+        case P: return half ? launch_case_t<P, true>(vol, W, H, D, fp, depth, pitch, index, s) \
+                            : launch_case_t<P, false>(vol, W, H, D, fp, depth, pitch, index, s);
+        PM_CASE_PPL(1) PM_CASE_PPL(2) PM_CASE_PPL(3) PM_CASE_PPL(4)
+        PM_CASE_PPL(5) PM_CASE_PPL(6) PM_CASE_PPL(7) PM_CASE_PPL(8)
+#undef PM_CASE_PPL
         default: return cudaErrorInvalidValue;
     }
 }

@@ -102,6 +102,13 @@ class StereoMapper:
                                               float(cx), float(cy)), "outputFusion")
         return out, variance
 
+    # -- outputFusionCPU's CASE 0 / 1 / 2 debug outputs (stereo_mapper.cpp:628-719)
+    def outputCase(self, case: int, out=None):
+        if out is None:
+            out = np.empty((self.H, self.W), np.float32)
+        self._check(self.lib.pm_output_case(self.h, int(case), _ptr(out), 0), "pm_output_case")
+        return out
+
     def wta_depth(self, out=None):
         if out is None:
             out = np.empty((self.H, self.W), np.float32)

@@ -178,6 +178,28 @@ def make_sequence(W: int, H: int, f: float, S: int, n_keyframes: int, seed: int,
     return out
 
 
+def make_stream(W: int, H: int, f: float, n_frames: int, seed: int, noise_sigma: float = 2.0,
+                step: float = 0.01, yaw_deg: float = 0.15):
+    """A continuous camera stream through one scene (for the sequence driver): frame k sits
+    step * k metres along a sideways heading and is turned yaw_deg * k about the camera's y axis.
+    Returns (images (n, H, W) uint8, R (n, 3, 3), T (n, 3), K)."""
+    cam = Camera(W, H, f)
+    rng = np.random.default_rng(seed)
+    R0 = rodrigues(_unit(rng), np.deg2rad(5.0) * rng.uniform())
+    T0 = rng.normal(0.0, 0.5, size=3)
+    scene = Scene(cam, int(rng.integers(1 << 31)), R0, T0)
+    heading = R0 @ np.array([1.0, 0.0, 0.0])
+    imgs, Rs, Ts = [], [], []
+    for k in range(n_frames):
+        R = R0 @ rodrigues(np.array([0.0, 1.0, 0.0]), np.deg2rad(yaw_deg) * k)
+        T = T0 + heading * step * k
+        img, _ = scene.render(R, T, rng, noise_sigma)
+        imgs.append(img)
+        Rs.append(R)
+        Ts.append(T)
+    return np.stack(imgs), np.stack(Rs), np.stack(Ts), cam.K
+
+
 def make_frameset(W: int, H: int, f: float, S: int, seed: int, noise_sigma: float = 2.0) -> FrameSet:
     return make_sequence(W, H, f, S, 1, seed, noise_sigma)[0]
 

@@ -1,0 +1,107 @@
+"""The headless sequence driver (pm_sequence, in place of evaluate.cc) end to end on a synthetic
+TUM-style stream written to disk: its depth files are compared bit-for-bit with the same keyframe
+schedule (oracle/sequence.py) driven through the Python StereoMapper, with the pyramid and
+colour steps checked against oracle/imgproc.py."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import imgproc as oip
+from oracle import sequence as oseq
+from probabilistic_mapping_b200 import _lib, scene, sequence
+from probabilistic_mapping_b200.mapper import StereoMapper
+
+pytestmark = pytest.mark.gpu
+
+W, H, F, N = 160, 120, 130.0, 27
+
+
+@pytest.fixture(scope="module")
+def stream(tmp_path_factory, pm_lib):
+    from probabilistic_mapping_b200 import build
+    build.build_cli()
+    root = str(tmp_path_factory.mktemp("seq"))
+    imgs, R, T, K = scene.make_stream(W, H, F, N, seed=5)
+    il, pl = sequence.write_tum(root, imgs, R, T)
+    images = [tuple(l.split()) for l in open(il) if not l.startswith("#")]
+    poses = [l.split() for l in open(pl) if not l.startswith("#")]
+    return dict(root=root, il=il, pl=pl, imgs=imgs, images=images, poses=poses)
+
+
+def python_run(st, case, downsample=0):
+    """evaluate.cc's keyframe loop through the Python StereoMapper, on the oracle's schedule."""
+    kfs, _ = oseq.schedule(st["images"], [(p[0],) for p in st["poses"]])
+    fx, fy, cx, cy = F, F, W / 2.0, H / 2.0
+    for _ in range(downsample):
+        fx, fy, cx, cy = fx / 2, fy / 2, (cx + 0.5) / 2.0 - 0.5, (cy + 0.5) / 2.0 - 0.5
+    K = np.array([[fx, 0, cx], [0, fy, cy], [0, 0, 1.0]])
+
+    def frame(i):
+        img = st["imgs"][i]
+        for _ in range(downsample):
+            img = oip.pyr_down(img)
+        return img
+
+    def pose(i):
+        p = [float(v) for v in st["poses"][i][1:]]
+        return sequence.quat_to_rot(p[3], p[4], p[5], p[6]), np.array(p[:3])
+
+    w, h = W >> downsample, H >> downsample
+    m = StereoMapper(w, h, 64, fusion_variant=_lib.PM_FUSION_CPU_PATH, max_sources=3)
+    m.initIntrinsic(K, 0.02 * fx, np.float32(1.0 / (0.15 * 160.0)))
+    out = {}
+    for ref, rp, src in kfs:
+        Rl, Tl = pose(rp)
+        m.initReference(frame(ref))
+        for s, sp in src:
+            Rr, Tr = pose(sp)
+            m.update(frame(s), Rl, Tl, Rr, Tr)
+        if case >= 3:
+            d, _ = m.outputFusion(Rl, Tl, fx, fy, cx, cy, want_variance=False)
+        else:
+            d = m.outputCase(case)
+        for _ in range(downsample):
+            d = oip.depth_up2(d)
+        out[st["images"][ref][0]] = d
+    m.close()
+    return out
+
+
+def cli_run(st, tmp, case, downsample=0, fmt="pfm", color=True):
+    os.makedirs(tmp, exist_ok=True)
+    res = sequence.run(st["il"], st["pl"], tmp, root=st["root"], case=case, downsample=downsample,
+                       fx=repr(F), fy=repr(F), cx=repr(W / 2.0), cy=repr(H / 2.0), format=fmt, color=color)
+    return res[-1]
+
+
+def read_ppm(path):
+    data = open(path, "rb").read()
+    parts = data.split(b"\n", 3)
+    w, h = (int(v) for v in parts[1].split())
+    rgb = np.frombuffer(parts[3], np.uint8, count=w * h * 3).reshape(h, w, 3)
+    return rgb[..., ::-1]
+
+
+@pytest.mark.parametrize("case,downsample", [(3, 0), (3, 1), (0, 0), (1, 1)])
+def test_driver_matches_python_loop(stream, tmp_path, case, downsample):
+    summary = cli_run(stream, str(tmp_path), case, downsample)
+    want = python_run(stream, case, downsample)
+    assert summary["keyframes"] == len(want) == 5 and summary["warnings"] == 0
+    assert (summary["width"], summary["height"]) == (W, H)
+    nonzero = 0
+    for stamp, d in want.items():
+        got = sequence.read_pfm(os.path.join(str(tmp_path), f"depth_{stamp}.pfm"))
+        assert got.shape == (H, W)
+        assert (got.view(np.uint32) == d.view(np.uint32)).all(), stamp
+        nonzero += int(((d > 0) & (d < 100)).sum())
+        level, bgr = oip.colorize(oip.range_mask(d, 0.2, 20.0))
+        np.testing.assert_array_equal(read_ppm(os.path.join(str(tmp_path), f"color_{stamp}.ppm")), bgr)
+    assert nonzero > 0
+
+
+def test_driver_npy_output(stream, tmp_path):
+    cli_run(stream, str(tmp_path), 2, 0, fmt="npy", color=False)
+    want = python_run(stream, 2)
+    for stamp, d in want.items():
+        np.testing.assert_array_equal(np.load(os.path.join(str(tmp_path), f"depth_{stamp}.npy")), d)
