@@ -134,7 +134,8 @@ def case_argmin(vol: np.ndarray, rho0: float, drho: float) -> tuple[np.ndarray, 
     """outputFusionCPU's CASE 0 / CASE 1 winner-take-all (stereo_mapper.cpp:636-660, 680-704)
     over an (H, W, D) float volume: the first plane holding a value below 100000 that no earlier
     plane undercuts; 10000 when that minimum is below FLOAT_EPS, 0 at the first and last plane,
-    else 1 / (rho0 + d * drho) in float32.  Returns (depth, plane)."""
+    else 1 / fma(d, drho, rho0) in float32 (the reference has rho0 = 0, where the fused and the
+    plain product agree).  Returns (depth, plane)."""
     vol = np.asarray(vol, np.float32)
     H, W, D = vol.shape
     v = np.where(np.isnan(vol), np.float32(np.inf), vol)
@@ -143,7 +144,7 @@ def case_argmin(vol: np.ndarray, rho0: float, drho: float) -> tuple[np.ndarray, 
     mn = np.take_along_axis(v, idx[..., None], 2)[..., 0]
     idx = np.where(np.isinf(mn), 0, idx)           # nothing below 100000: plane 0
     mn64 = np.where(np.isinf(mn), 100000.0, mn.astype(np.float64))
-    rho = (np.float32(rho0) + idx.astype(np.float32) * np.float32(drho)).astype(np.float32)
+    rho = _fma_f32(idx.astype(np.float32), np.float32(drho), np.float32(rho0))   # one rounding
     with np.errstate(divide="ignore"):
         dep = (np.float32(1.0) / rho).astype(np.float32)
     dep = np.where((idx == 0) | (idx == D - 1), np.float32(0.0), dep)

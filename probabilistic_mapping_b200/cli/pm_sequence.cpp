@@ -277,7 +277,14 @@ int main(int argc, char** argv) {
         Pose p;
         if (r.size() < 8 || !parse_stamp(r[0], p.t)) { std::fprintf(stderr, "pm_sequence: bad pose line\n"); return 2; }
         double* v[7] = {&p.tx, &p.ty, &p.tz, &p.qx, &p.qy, &p.qz, &p.qw};
-        for (int i = 0; i < 7; ++i) *v[i] = std::atof(r[1 + i].c_str());
+        for (int i = 0; i < 7; ++i) {
+            char* end = nullptr;
+            *v[i] = std::strtod(r[1 + i].c_str(), &end);
+            if (end == r[1 + i].c_str() || *end != '\0' || !std::isfinite(*v[i])) {
+                std::fprintf(stderr, "pm_sequence: bad pose value '%s'\n", r[1 + i].c_str());
+                return 2;
+            }
+        }
         P.push_back(p);
     }
     if (a.associate >= 0.0) {   // restamp: each image gets its nearest pose within the tolerance

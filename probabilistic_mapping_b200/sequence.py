@@ -91,8 +91,8 @@ def write_tum(root: str, images, R, T, t0: float = 1000.0, dt: float = 1.0 / 30.
             fi.write(f"{st} {name}\n")
         for k in range(len(R)):
             st = pose_stamps[k] if pose_stamps is not None else f"{t0 + k * dt:.6f}"
-            q = rot_to_quat(R[k])
-            fp.write(f"{st} {T[k][0]!r} {T[k][1]!r} {T[k][2]!r} {q[0]!r} {q[1]!r} {q[2]!r} {q[3]!r}\n")
+            vals = [float(v) for v in T[k]] + list(rot_to_quat(R[k]))
+            fp.write(st + "".join(f" {v!r}" for v in vals) + "\n")
     return il, pl
 
 
