@@ -7,7 +7,7 @@ against the previous keyframe's state.  Workload: 640x480, 128 inverse-depth pla
 [0.1, 2.0] 1/m, 5 sources, f = 520, seeded synthetic scenes (six textured planes).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--form batched|plain] [--precision fp16|fp32] [--batch B]
+                  [--form batched|plain|mixed] [--precision fp16|fp32] [--batch B] [--lanes L]
 
 Default (the headline): the FP16 form, B sequences batched (one CUDA-graph launch per step for
 all B), against the plain FP32 form (one StereoMapper, one map after the other) measured in the
@@ -267,7 +267,7 @@ def run_batched(args, rank, world, precision: str, B: int, host_io: bool, clocks
                tau_so=TAU, uniqueness_ratio=UNIQ, cost_mode=1 if args.cost_mode == "corrected" else 0,
                precision=prec, device=dev)
     seqs = [scene.make_sequence(W, H, F_PX, S, 2, seed=2000 + 97 * rank + i) for i in range(B)]
-    b = StereoBatch([cfg] * B, S, lanes=0, host_io=host_io, autotune=True)
+    b = StereoBatch([cfg] * B, S, lanes=0, host_io=host_io, autotune=True, priority=args.priority)
     for i in range(B):
         b.init_intrinsic(i, seqs[i][0].K, drho)
 
@@ -305,6 +305,101 @@ def run_batched(args, rank, world, precision: str, B: int, host_io: bool, clocks
     return t, (sampler.summary() if sampler else None), tuning
 
 
+# The mixed batch: 48 sequences, 16 at each size, 4 sources (the batching form's workload).
+MIXED = [(320, 240, 64, 260.0), (640, 480, 128, 520.0), (1280, 720, 192, 1040.0)]
+MIXED_PER_SHAPE, MIXED_S = 16, 4
+
+
+def run_mixed(args, rank, world, precision: str, host_io: bool, clocks: bool):
+    """This rank's shard (balanced by voxels x sources) of the 48-sequence mixed batch in one
+    pm_batch; each step is one CUDA-graph launch that maps every sequence of the shard.  Two
+    seeded scenes per size are shared by that size's sequences (the inputs only need the size)."""
+    import torch
+    from probabilistic_mapping_b200 import _lib, scene
+    from probabilistic_mapping_b200.batch import StereoBatch
+    from probabilistic_mapping_b200.shard import shard_sequences
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    prec = _lib.PM_PREC_FP16 if precision == "fp16" else _lib.PM_PREC_FP32
+    cfgs, shapes = [], []
+    for k, (w, h, d, f) in enumerate(MIXED):
+        rho0, _ = scene.plane_range(d)
+        for _ in range(MIXED_PER_SHAPE):
+            cfgs.append(dict(width=w, height=h, num_planes=d, rho0=rho0, intensity_scale=1 / 255, num_paths=PATHS,
+                             p1=P1, p2=P2, tau_so=TAU, uniqueness_ratio=UNIQ,
+                             cost_mode=1 if args.cost_mode == "corrected" else 0, precision=prec, device=dev))
+            shapes.append(k)
+    mine = shard_sequences(cfgs, world, MIXED_S)[rank]
+    scenes = {k: [scene.make_sequence(w, h, f, MIXED_S, 2, seed=3000 + 10 * k + j) for j in range(2)]
+              for k, (w, h, d, f) in enumerate(MIXED) if any(shapes[i] == k for i in mine)}
+    b = StereoBatch([cfgs[i] for i in mine], MIXED_S, lanes=args.lanes, host_io=host_io, autotune=True,
+                    priority=args.priority)
+    seqs = []
+    for j, i in enumerate(mine):
+        seqs.append(scenes[shapes[i]][i % 2])
+        b.init_intrinsic(j, seqs[-1][0].K, scene.plane_range(MIXED[shapes[i]][2])[1])
+
+    def feed(step):
+        k = step % 2
+        for j, sq in enumerate(seqs):
+            fs = sq[k]
+            if step < 2:
+                b.set_frame(j, 0, fs.ref)
+                for s in range(MIXED_S):
+                    b.set_frame(j, 1 + s, fs.srcs[s])
+            b.set_poses(j, fs.R_ref, fs.T_ref, list(fs.R_srcs), list(fs.T_srcs))
+
+    for i in range(args.warmup):
+        feed(i)
+        b.run()
+    b.synchronize()
+    stream = torch.cuda.ExternalStream(b.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(dev) if clocks else None
+    if sampler:
+        sampler.__enter__()
+    e0.record(stream)
+    for i in range(args.steps):
+        feed(args.warmup + i)
+        b.run()
+    e1.record(stream)
+    b.synchronize()
+    if sampler:
+        sampler.__exit__(None, None, None)
+    t = e0.elapsed_time(e1)
+    b.close()
+    t = max_over_ranks([t], world)[0]
+    h2d = sum(cfgs[i]["width"] * cfgs[i]["height"] * (MIXED_S + 1) for i in mine)
+    d2h = sum(cfgs[i]["width"] * cfgs[i]["height"] * 8 for i in mine)
+    return t, (sampler.summary() if sampler else None), len(mine), h2d, d2h
+
+
+def mixed_main(args, rank, world):
+    precision = args.precision or "fp16"
+    t, clocks, n_mine, _, _ = run_mixed(args, rank, world, precision, host_io=False, clocks=True)
+    te, _, _, h2d, d2h = run_mixed(args, rank, world, precision, host_io=True, clocks=False)
+    total = len(MIXED) * MIXED_PER_SHAPE
+    value = total * args.steps / (t / 1000.0)
+    e2e = total * args.steps / (te / 1000.0)
+    if rank == 0:
+        vox = sum(w * h * d for w, h, d, _ in MIXED) * MIXED_PER_SHAPE
+        line = {"metric": "depth maps/s, 48-sequence mixed batch (16 each at 320x240x64, 640x480x128, "
+                          "1280x720x192), 4 sources", "value": value, "unit": "depth maps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f16" if precision == "fp16" else "f32",
+                "data": "synthetic",
+                "config": {"workload": f"48 sequences, {MIXED_S} sources, {PATHS}-path SGM, fusion step, "
+                                       f"{precision}, lanes={args.lanes}", "global_batch": total, "seq_len": 0,
+                           "parallelism": f"sequence shards x{world}, balanced by voxels x sources",
+                           "l2": "per-map working sets exceed the 126 MB L2"},
+                "voxels_per_s": vox * args.steps / (t / 1000.0),
+                "sequences_on_rank0": n_mine,
+                "e2e": {"value": e2e, "unit": "depth maps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "note": "rank 0's shard bytes"},
+                "clocks": clocks}
+        print(json.dumps(line))
+
+
 def cpu_baseline_sample(threads: int | None = None, maps: int = 1):
     """FP64 oracle (all host threads) on full-size depth maps of the same workload."""
     import oracle
@@ -340,7 +435,12 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--form", choices=["batched", "plain"], default="batched")
+    ap.add_argument("--form", choices=["batched", "plain", "mixed"], default="batched",
+                    help="batched: B sequences of the headline workload; plain: one map after the other; "
+                         "mixed: the 48-sequence three-size batch, sharded over ranks")
+    ap.add_argument("--lanes", type=int, default=0, help="volume sets per size in the mixed batch (0: one each)")
+    ap.add_argument("--priority", type=int, default=1, choices=[0, 1],
+                    help="batched forms: SGM kernels at the greatest launch priority (1) or not (0)")
     ap.add_argument("--precision", choices=["fp32", "fp16"], default=None,
                     help="precision of the measured form (default: fp16 batched, fp32 plain)")
     ap.add_argument("--batch", type=int, default=16, help="sequences per batch (batched form)")
@@ -379,6 +479,12 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
+    if args.form == "mixed":
+        mixed_main(args, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.precision is None:
         args.precision = "fp16" if args.form == "batched" else "fp32"
     # the plain FP32 form, always measured: the baseline of the batched form's speed-up and the

@@ -199,6 +199,8 @@ typedef struct pm_batch pm_batch;
 #define PM_BATCH_HOST_IO 1  /* frames in and fused depth/variance out through batch-owned pinned
                                host buffers, copied inside the graph; else device buffers */
 #define PM_BATCH_AUTOTUNE 2 /* time the SGM schedules for each distinct shape at creation */
+#define PM_BATCH_PRIORITY 4 /* SGM kernels at the device's greatest launch priority, so they
+                               overlap the other sequences' cost kernels */
 PM_API pm_status pm_batch_create(const pm_config* cfgs, int num_sequences, int num_sources, int lanes, int flags,
                                  pm_batch** out);
 PM_API void pm_batch_destroy(pm_batch* b);

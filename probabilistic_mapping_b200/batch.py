@@ -22,7 +22,8 @@ def _addr(x):
 class StereoBatch:
     """configs: list of dicts of pm_config fields, each with width, height and num_planes."""
 
-    def __init__(self, configs, num_sources: int, lanes: int = 0, host_io: bool = True, autotune: bool = False):
+    def __init__(self, configs, num_sources: int, lanes: int = 0, host_io: bool = True, autotune: bool = False,
+                 priority: bool = False):
         self.lib = load()
         n = len(configs)
         arr = (_lib.PmConfig * n)()
@@ -38,7 +39,8 @@ class StereoBatch:
             self.shapes.append((H, W))
         self.S = num_sources
         self.host_io = host_io
-        flags = (_lib.PM_BATCH_HOST_IO if host_io else 0) | (_lib.PM_BATCH_AUTOTUNE if autotune else 0)
+        flags = ((_lib.PM_BATCH_HOST_IO if host_io else 0) | (_lib.PM_BATCH_AUTOTUNE if autotune else 0) |
+                 (_lib.PM_BATCH_PRIORITY if priority else 0))
         b = ctypes.c_void_p()
         check(self.lib.pm_batch_create(arr, n, num_sources, lanes, flags, ctypes.byref(b)), None, "pm_batch_create")
         self.b = b

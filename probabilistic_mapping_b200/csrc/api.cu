@@ -29,8 +29,7 @@ struct pm_mapper {
 
     uint8_t* d_u8 = nullptr;    // upload staging, W*H bytes
     float* d_ref = nullptr;     // scaled reference image
-    float4* d_srcq = nullptr;   // FP32: max_sources source frames in the quad layout
-    void* d_srcq16 = nullptr;                     // FP16 form, exact sampler: FP16 quads
+    float4* d_srcq = nullptr;   // max_sources source frames in the quad layout (FP16 form: FP16-rounded values)
     void* d_srch[kMaxSources] = {};               // FP16 form, texture sampler: pitched FP16 frames
     size_t srch_pitch = 0;
     cudaTextureObject_t tex[kMaxSources] = {};    // FP16 form: one texture object per slot
@@ -250,8 +249,7 @@ pm_status upload_image(pm_mapper* h, const uint8_t* img, size_t pitch, float* ds
     if (slot >= 0 && half && h->cfg.sampler == PM_SAMPLER_TEXTURE)
         PM_CK(h, launch_to_half(W, H, dev, pitch, h->d_srch[slot], h->srch_pitch, sc, h->stream));
     else if (slot >= 0 && half)
-        PM_CK(h, launch_to_quad_half(W, H, dev, pitch, (char*)h->d_srcq16 + (size_t)slot * 8 * W * H, sc,
-                                     h->stream));
+        PM_CK(h, launch_to_quad_half(W, H, dev, pitch, h->d_srcq + (size_t)slot * W * H, sc, h->stream));
     else if (slot >= 0)
         PM_CK(h, launch_to_quad(W, H, dev, pitch, h->d_srcq + (size_t)slot * W * H, sc, h->stream));
     else if (half)
@@ -273,8 +271,6 @@ pm_status evaluate_cost(pm_mapper* h, bool into_state) {
     if (c.precision == PM_PREC_FP16 && c.sampler == PM_SAMPLER_TEXTURE) {
         a.use_tex = 1;
         for (int s = 0; s < h->nsrc; ++s) a.tex[s] = h->tex[s];
-    } else if (c.precision == PM_PREC_FP16) {
-        a.srcq16 = h->d_srcq16;
     }
     for (int s = 0; s < h->nsrc; ++s)
         for (int i = 0; i < 12; ++i) a.hom[s][i] = h->homs[12 * s + i];
@@ -339,7 +335,6 @@ void release(pm_mapper* h) {
     cudaFree(h->d_u8);
     cudaFree(h->d_ref);
     cudaFree(h->d_srcq);
-    cudaFree(h->d_srcq16);
     for (int s = 0; s < kMaxSources; ++s) {
         if (h->tex[s]) cudaDestroyTextureObject(h->tex[s]);
         cudaFree(h->d_srch[s]);
@@ -424,8 +419,7 @@ pm_status pm_create(const pm_config* cfg, pm_mapper** out) {
     h->own_stream = ok;
     const bool half = cfg->precision == PM_PREC_FP16;
     ok = ok && alloc((void**)&h->d_u8, N) && alloc((void**)&h->d_ref, 4 * N) &&
-         (half || alloc((void**)&h->d_srcq, 16 * N * cfg->max_sources)) &&
-         (!half || cfg->sampler == PM_SAMPLER_TEXTURE || alloc(&h->d_srcq16, 8 * N * cfg->max_sources)) &&
+         ((half && cfg->sampler == PM_SAMPLER_TEXTURE) || alloc((void**)&h->d_srcq, 16 * N * cfg->max_sources)) &&
          alloc(&h->d_cost, esz * V) &&
          alloc((void**)&h->d_depth, 4 * N) &&
          alloc((void**)&h->d_idx, 4 * N) && alloc((void**)&h->d_ztable, 8 * N) &&

@@ -13,7 +13,10 @@
 // memory of a large batch.  Two graph instances alternate by step parity over double-buffered
 // parameter blocks and frame buffers, so the host prepares step t+1 while step t runs.
 // An optional autotuner times the SGM schedules (scanlines per block of the path-pair kernel,
-// concurrent or serial path pairs) for each distinct shape and keeps the fastest.
+// concurrent or serial path pairs) for each distinct shape and keeps the fastest.  With
+// PM_BATCH_PRIORITY the SGM kernels carry the device's greatest launch priority, so the block
+// dispatcher hands freed SM slots to one sequence's latency-bound SGM before the queued blocks
+// of another sequence's cost kernel, and the two overlap instead of running back to back.
 #include <cuda_fp16.h>
 
 #include <cstdarg>
@@ -59,7 +62,6 @@ struct Seq {
     // persistent device state
     float* d_ref = nullptr;
     float4* d_srcq = nullptr;
-    void* d_srcq16 = nullptr;
     float* d_depth = nullptr;
     int32_t* d_idx = nullptr;
     float* d_state[2][4] = {};
@@ -93,6 +95,7 @@ struct pm_batch {
     int S = 0;
     int flags = 0;
     int device = 0;
+    int sgm_priority = 0;   // launch priority of the SGM kernels (PM_BATCH_PRIORITY)
     cudaStream_t run = nullptr;
     cudaEvent_t root = nullptr;
     cudaEvent_t launched[2] = {};
@@ -160,7 +163,6 @@ void free_batch(pm_batch* b) {
         }
         cudaFree(q.d_ref);
         cudaFree(q.d_srcq);
-        cudaFree(q.d_srcq16);
         cudaFree(q.d_depth);
         cudaFree(q.d_idx);
         for (auto& s : q.d_state)
@@ -181,7 +183,7 @@ void free_batch(pm_batch* b) {
     if (b->run) cudaStreamDestroy(b->run);
 }
 
-SgmLaunch sgm_launch(const Seq& q, const LaneBufs& l) {
+SgmLaunch sgm_launch(const Seq& q, const LaneBufs& l, int priority) {
     SgmLaunch a;
     std::memset(&a, 0, sizeof a);
     const pm_config& c = q.cfg;
@@ -204,6 +206,7 @@ SgmLaunch sgm_launch(const Seq& q, const LaneBufs& l) {
     a.order = q.order;
     a.pair_warps = q.pair_warps;
     a.serial_pairs = q.serial_pairs;
+    a.priority = priority;
     return a;
 }
 
@@ -228,7 +231,7 @@ cudaError_t enqueue_seq(pm_batch* b, int i, int k) {
     if (e) return e;
     for (int s = 0; s < S; ++s) {
         const uint8_t* f = q.d_frames[k] + (1 + s) * N;
-        e = half ? launch_to_quad_half(W, H, f, W, (char*)q.d_srcq16 + (size_t)s * 8 * N, sc, m)
+        e = half ? launch_to_quad_half(W, H, f, W, q.d_srcq + (size_t)s * N, sc, m)
                  : launch_to_quad(W, H, f, W, q.d_srcq + (size_t)s * N, sc, m);
         if (e) return e;
     }
@@ -238,8 +241,7 @@ cudaError_t enqueue_seq(pm_batch* b, int i, int k) {
     CostLaunch a;
     std::memset(&a, 0, sizeof a);
     a.ref = q.d_ref;
-    a.srcq = half ? nullptr : q.d_srcq;
-    a.srcq16 = half ? q.d_srcq16 : nullptr;
+    a.srcq = q.d_srcq;
     a.W = W;
     a.H = H;
     a.D = c.num_planes;
@@ -251,7 +253,7 @@ cudaError_t enqueue_seq(pm_batch* b, int i, int k) {
     a.cost = l.cost;
     a.cost_half = half;
     if ((e = launch_cost(a, m))) return e;
-    const SgmLaunch g = sgm_launch(q, l);
+    const SgmLaunch g = sgm_launch(q, l, b->sgm_priority);
     if ((e = launch_sgm(g, kCombineFilter, m, &q.side))) return e;
     if ((e = cudaEventRecord(q.lane_free, m))) return e;
     // fusion (stereo_mapper.cpp:111-244) with the step's pose, flags and state index from d_par
@@ -296,7 +298,9 @@ pm_status build_graphs(pm_batch* b) {
             return bfail(b, PM_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : ee));
         }
         b->graph[k] = g;
-        PB_CK(b, cudaGraphInstantiate(&b->exec[k], g, 0));
+        // with PM_BATCH_PRIORITY the SGM nodes keep their own (higher) priority
+        PB_CK(b, cudaGraphInstantiateWithFlags(&b->exec[k], g,
+                                               b->sgm_priority ? cudaGraphInstantiateFlagUseNodePriority : 0));
     }
     b->built = true;
     return PM_OK;
@@ -331,7 +335,7 @@ pm_status autotune(pm_batch* b) {
             for (int serial = 0; serial < 2 && e == cudaSuccess; ++serial) {
                 q.pair_warps = w;
                 q.serial_pairs = serial;
-                const SgmLaunch g = sgm_launch(q, l);
+                const SgmLaunch g = sgm_launch(q, l, 0);
                 e = launch_sgm(g, kCombineFilter, b->run, &q.side);   // warm-up
                 if (e == cudaSuccess) e = cudaEventRecord(t0, b->run);
                 for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = launch_sgm(g, kCombineFilter, b->run, &q.side);
@@ -377,6 +381,10 @@ pm_status pm_batch_create(const pm_config* cfgs, int n, int num_sources, int lan
     b->flags = flags;
     b->device = cfgs[0].device;
     DevGuard dg(b->device);
+    if (flags & PM_BATCH_PRIORITY) {
+        int least = 0, greatest = 0;
+        if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess) b->sgm_priority = greatest;
+    }
     cudaError_t first_err = cudaSuccess;
     auto note = [&](cudaError_t e) {
         if (e != cudaSuccess && first_err == cudaSuccess) first_err = e;
@@ -414,7 +422,6 @@ pm_status pm_batch_create(const pm_config* cfgs, int n, int num_sources, int lan
             if (!ok) break;
         }
         q.lane = pool[lanes == 0 ? j : j % lanes];
-        const bool half = q.cfg.precision == PM_PREC_FP16;
         const size_t N = q.N;
         for (int k = 0; k < 2 && ok; ++k) {
             ok = note(cudaMallocHost((void**)&q.h_par[k], sizeof(float) * q.par_floats)) &&
@@ -426,7 +433,7 @@ pm_status pm_batch_create(const pm_config* cfgs, int n, int num_sources, int lan
             if (ok) std::memset(q.h_par[k], 0, sizeof(float) * q.par_floats);
         }
         ok = ok && alloc((void**)&q.d_ref, 4 * N) &&
-             (half ? alloc(&q.d_srcq16, 8 * N * q.S) : alloc((void**)&q.d_srcq, 16 * N * q.S)) &&
+             alloc((void**)&q.d_srcq, 16 * N * q.S) &&
              alloc((void**)&q.d_depth, 4 * N) && alloc((void**)&q.d_idx, 4 * N) &&
              alloc((void**)&q.d_ztable, 8 * N) && alloc((void**)&q.d_table, 4 * N) &&
              alloc((void**)&q.d_fused, 4 * N) && alloc((void**)&q.d_var, 4 * N);

@@ -51,22 +51,23 @@ __global__ void __launch_bounds__(256) to_half_kernel(int W, int H, const uint8_
     }
 }
 
-// FP16 quads for the FP16 form's exact sampler: the layout of to_quad_kernel in halves.
+// Quads for the FP16 form's sampler: the layout of to_quad_kernel with every value rounded to
+// FP16 (the form's image precision), held in FP32 lanes so that a sample needs no conversion.
 __global__ void __launch_bounds__(256) to_quad_half_kernel(int W, int H, const uint8_t* __restrict__ src,
-                                                           size_t pitch, uint2* __restrict__ dst, float scale) {
+                                                           size_t pitch, float4* __restrict__ dst, float scale) {
     const int y = blockIdx.y;
     const uint8_t* r0 = src + (size_t)y * pitch;
     const uint8_t* r1 = r0 + pitch;
     const bool has1 = (y + 1) < H;
-    uint2* out = dst + (size_t)y * W;
+    float4* out = dst + (size_t)y * W;
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < W; x += gridDim.x * blockDim.x) {
         const bool hasx = (x + 1) < W;
-        const float a = __fmul_rn((float)r0[x], scale);                             // I(x, y)
-        const float b = has1 ? __fmul_rn((float)r1[x], scale) : 0.0f;               // I(x, y+1)
-        const float c = hasx ? __fmul_rn((float)r0[x + 1], scale) : 0.0f;           // I(x+1, y)
-        const float d = (has1 && hasx) ? __fmul_rn((float)r1[x + 1], scale) : 0.0f; // I(x+1, y+1)
-        const __half2 lo = __floats2half2_rn(a, b), hi = __floats2half2_rn(c, d);
-        out[x] = make_uint2(*reinterpret_cast<const unsigned*>(&lo), *reinterpret_cast<const unsigned*>(&hi));
+        float4 q;
+        q.x = __half2float(__float2half_rn(__fmul_rn((float)r0[x], scale)));                     // I(x, y)
+        q.y = has1 ? __half2float(__float2half_rn(__fmul_rn((float)r1[x], scale))) : 0.0f;         // I(x, y+1)
+        q.z = hasx ? __half2float(__float2half_rn(__fmul_rn((float)r0[x + 1], scale))) : 0.0f;     // I(x+1, y)
+        q.w = (has1 && hasx) ? __half2float(__float2half_rn(__fmul_rn((float)r1[x + 1], scale))) : 0.0f;
+        out[x] = q;
     }
 }
 
@@ -114,10 +115,10 @@ cudaError_t launch_to_float_h(int W, int H, const uint8_t* src, size_t src_pitch
     return cudaGetLastError();
 }
 
-cudaError_t launch_to_quad_half(int W, int H, const uint8_t* src, size_t src_pitch, void* dst, float scale,
+cudaError_t launch_to_quad_half(int W, int H, const uint8_t* src, size_t src_pitch, float4* dst, float scale,
                                 cudaStream_t s) {
     const dim3 grid((W + 255) / 256, H);
-    to_quad_half_kernel<<<grid, 256, 0, s>>>(W, H, src, src_pitch, reinterpret_cast<uint2*>(dst), scale);
+    to_quad_half_kernel<<<grid, 256, 0, s>>>(W, H, src, src_pitch, dst, scale);
     return cudaGetLastError();
 }
 

@@ -68,8 +68,10 @@ __device__ __forceinline__ float2 shfl_down2(float2 v) {
     return f2(__shfl_down_sync(kFull, v.x, 1), __shfl_down_sync(kFull, v.y, 1));
 }
 
-// Source access: plain float rows, the quad layout (one 16-byte load per bilinear sample), or
-// (FP16 form) a texture object over an FP16 image, filtered by the texture unit.
+// Source access: plain float rows, the quad layout (one 16-byte load per bilinear sample; in the
+// FP16 form its values are rounded to FP16 but kept in FP32 lanes, since a per-sample conversion
+// costs more issue slots than the wider loads cost bandwidth in this issue-bound kernel), or (FP16
+// form) a texture object over an FP16 image, filtered by the texture unit.
 enum { kPlain = 0, kQuad = 1, kTex = 2, kQuadH = 3 };
 template <int SAMP> struct Src;
 template <> struct Src<kPlain> {
@@ -85,8 +87,8 @@ template <> struct Src<kTex> {
     cudaTextureObject_t t;
     int W, H;
 };
-template <> struct Src<kQuadH> {   // FP16 quads: (I(x,y), I(x,y+1)) and (I(x+1,y), I(x+1,y+1)) as half2
-    const uint2* __restrict__ q;
+template <> struct Src<kQuadH> {   // FP16 form: quads of FP16-rounded values in FP32 lanes
+    const float4* __restrict__ q;
     int W, H;
     unsigned off;
 };
@@ -134,18 +136,11 @@ __device__ __forceinline__ float2 sample2(const Src<SAMP>& src, const WarpConst&
         const unsigned i0 = __float_as_uint(tv.x) * (unsigned)src.W + __float_as_uint(tu.x) - src.off;
         const unsigned i1 = __float_as_uint(tv.y) * (unsigned)src.W + __float_as_uint(tu.y) - src.off;
         float2 lo0, hi0, lo1, hi1;
-        if constexpr (SAMP == kQuad) {
+        {
             const float4 t0 = __ldg(src.q + (ok0 ? i0 : 0u));
             const float4 t1 = __ldg(src.q + (ok1 ? i1 : 0u));
             lo0 = f2(t0.x, t0.y); hi0 = f2(t0.z, t0.w);
             lo1 = f2(t1.x, t1.y); hi1 = f2(t1.z, t1.w);
-        } else {
-            const uint2 t0 = __ldg(src.q + (ok0 ? i0 : 0u));
-            const uint2 t1 = __ldg(src.q + (ok1 ? i1 : 0u));
-            lo0 = __half22float2(*reinterpret_cast<const __half2*>(&t0.x));
-            hi0 = __half22float2(*reinterpret_cast<const __half2*>(&t0.y));
-            lo1 = __half22float2(*reinterpret_cast<const __half2*>(&t1.x));
-            hi1 = __half22float2(*reinterpret_cast<const __half2*>(&t1.y));
         }
         // (top, bot) = fma(a, (I(x+1,y), I(x+1,y+1)) - (I(x,y), I(x,y+1)), (I(x,y), I(x,y+1)))
         const float2 p0 = __ffma2_rn(f2(a.x, a.x), sub2(hi0, lo0), lo0);
@@ -183,7 +178,10 @@ __device__ __forceinline__ Hom load_hom(const CostLaunch& a, int s) {
 // this library writes has cnt = 0 exactly where last < 0.  Both divisions are a
 // reciprocal-multiply with one FMA correction (RN(1/9) and the exact Newton reciprocal of
 // cnt+1), equal to IEEE division for divisors up to 33 and dividends 0 or >= 1e-30 (the
-// exhaustive check of pm_debug_check_arith); outside that the pair takes IEEE division.
+// exhaustive check of pm_debug_check_arith); outside that the pair takes IEEE division.  A pass
+// that starts from initReference (INC false) folds at most kMaxSources sources, so its divisors
+// never exceed 33 and only the dividends are tested.
+template <bool INC>
 __device__ __forceinline__ void fold2(float2& acc, float2& cn, float2 tmp, float r9) {
     const float2 r9p = f2(r9, r9);
     const float2 n1 = __fadd2_rn(cn, f2(1.0f, 1.0f));
@@ -194,7 +192,7 @@ __device__ __forceinline__ void fold2(float2& acc, float2& cn, float2 tmp, float
     const float2 r = rcp_warp2(n1);
     const float2 p0 = __fmul2_rn(num, r);
     float2 q = __ffma2_rn(__ffma2_rn(p0, nn1, num), r, p0);
-    const bool fast = n1.x <= 33.0f && n1.y <= 33.0f && !(tmp.x != 0.0f && tmp.x < 1e-30f) &&
+    const bool fast = (!INC || (n1.x <= 33.0f && n1.y <= 33.0f)) && !(tmp.x != 0.0f && tmp.x < 1e-30f) &&
                       !(tmp.y != 0.0f && tmp.y < 1e-30f) && !(num.x != 0.0f && num.x < 1e-30f) &&
                       !(num.y != 0.0f && num.y < 1e-30f);
     if (!fast) {
@@ -207,7 +205,7 @@ __device__ __forceinline__ void fold2(float2& acc, float2& cn, float2 tmp, float
 }
 
 // MODE 0: reference sample set (calc_cost.cu:83-199); MODE 1: corrected 3x3 patch.
-template <int MODE, bool HALF, int SAMP>
+template <int MODE, bool HALF, int SAMP, bool INC>
 __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* const refp = reinterpret_cast<float2*>(smem_raw + Smem::REF);
@@ -233,7 +231,7 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
     for (int e = tid; e < NPIX * PCB; e += NT) {
         const int p = e / PCB, k = e - p * PCB;
         float c0 = -1.0f, n0 = 0.0f;
-        if (a.incremental) {
+        if (INC) {
             const int o = p / TXU, i = p - o * TXU;
             const int gx = x0 + i, gy = y0 + o;
             if (gx < W && gy < H) {
@@ -257,14 +255,11 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
 
     for (int s = 0; s < a.nsrc; ++s) {
         Src<SAMP> src;
-        if constexpr (SAMP == kQuad) {
+        if constexpr (SAMP == kQuad || SAMP == kQuadH) {
             src.q = a.srcq + (size_t)s * W * H;
             src.off = 0x4B400000u * (unsigned)(W + 1);
         } else if constexpr (SAMP == kTex) {
             src.t = a.tex[s];
-        } else if constexpr (SAMP == kQuadH) {
-            src.q = reinterpret_cast<const uint2*>(a.srcq16) + (size_t)s * W * H;
-            src.off = 0x4B400000u * (unsigned)(W + 1);
         } else {
             src.p = a.srcs + (size_t)s * W * H;
         }
@@ -282,7 +277,7 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
         // columns (L / R); row r (down) is computed in the iteration
         float2 Su = f2(0.0f, 0.0f), Sc = Su, Lu = Su, Lc = Su, Ru = Su, Rc = Su;
         float hxc = 0.0f;
-#pragma unroll 1
+#pragma unroll   // unrolled, the rolling row registers are renamed instead of copied
         for (int r = 0; r < TY + 2; ++r) {
             float hx, hy, hz;
             homog(h, x, y0 - 1 + r, hx, hy, hz);
@@ -330,7 +325,7 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
                 float2* const ap = accp + o * (TXU * SP / 2);
                 float2* const cp = cntp + o * (TXU * SP / 2);
                 float2 av = *ap, nv = *cp;
-                fold2(av, nv, f2(tx, ty), r9);
+                fold2<INC>(av, nv, f2(tx, ty), r9);
                 *ap = av;
                 *cp = nv;
             }
@@ -370,7 +365,7 @@ __global__ void __launch_bounds__(256) invalid_kernel(const void* cost, long npi
 
 template <int MODE, bool HALF, int SAMP>
 cudaError_t launch_t(const CostLaunch& a, dim3 grid, cudaStream_t s) {
-    auto kern = cost_kernel<MODE, HALF, SAMP>;
+    auto kern = a.incremental ? cost_kernel<MODE, HALF, SAMP, true> : cost_kernel<MODE, HALF, SAMP, false>;
     if (Smem::BYTES > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Smem::BYTES);
         if (e != cudaSuccess) return e;
@@ -381,9 +376,14 @@ cudaError_t launch_t(const CostLaunch& a, dim3 grid, cudaStream_t s) {
 
 template <int MODE, bool HALF>
 cudaError_t launch_q(const CostLaunch& a, dim3 grid, cudaStream_t s) {
-    if (a.use_tex) return launch_t<MODE, HALF, kTex>(a, grid, s);
-    if (a.srcq16) return launch_t<MODE, HALF, kQuadH>(a, grid, s);
-    return a.srcq ? launch_t<MODE, HALF, kQuad>(a, grid, s) : launch_t<MODE, HALF, kPlain>(a, grid, s);
+    // FP16 volumes come from the FP16 form's samplers, FP32 volumes from the exact FP32 ones
+    if constexpr (HALF) {
+        if (a.use_tex) return launch_t<MODE, true, kTex>(a, grid, s);
+        return a.srcq ? launch_t<MODE, true, kQuadH>(a, grid, s) : cudaErrorInvalidValue;
+    } else {
+        if (a.use_tex) return cudaErrorInvalidValue;
+        return a.srcq ? launch_t<MODE, false, kQuad>(a, grid, s) : launch_t<MODE, false, kPlain>(a, grid, s);
+    }
 }
 
 }  // namespace

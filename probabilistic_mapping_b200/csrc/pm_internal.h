@@ -17,10 +17,11 @@ constexpr float kCaseInf = 10000.0f; // no-overlap value of the CASE 0/1 debug o
 struct CostLaunch {
     const float* ref;      // W*H scaled reference image
     const float* srcs;     // nsrc consecutive W*H scaled source images (used when srcq is null)
-    const float4* srcq;    // nsrc consecutive W*H quad images (2x2 bilinear footprints)
-    // FP16 form: sources as FP16 quads (srcq16, 8 bytes per pixel), or, when use_tex is set,
-    // through these texture objects (FP16 pitched images, linear filtering, zero border)
-    const void* srcq16;
+    // nsrc consecutive W*H quad images (2x2 bilinear footprints); in the FP16 form (cost_half)
+    // their values are rounded to FP16
+    const float4* srcq;
+    // FP16 form with use_tex: the sources through these texture objects (FP16 pitched images,
+    // linear filtering, zero border)
     unsigned long long tex[kMaxSources];
     int use_tex;
     int W, H, D, nsrc;
@@ -63,6 +64,7 @@ struct SgmLaunch {
     PlaneOrder order;
     int pair_warps;        // scanlines per block of the path-pair kernel: 2, 4 or 8 (0: 4)
     int serial_pairs;      // 1: run the path pairs one after another on the caller's stream
+    int priority;          // launch priority of the pair and combine kernels (0: the stream's)
 };
 // Side streams for the concurrent path pairs: pairs 0..2 fork from the caller's stream and join
 // back before the combine kernel.
@@ -92,8 +94,8 @@ cudaError_t launch_to_float(int W, int H, const uint8_t* src, size_t src_pitch, 
 // uint8 -> scaled FP16 image with a byte pitch (the FP16 form's texture storage).
 cudaError_t launch_to_half(int W, int H, const uint8_t* src, size_t src_pitch, void* dst, size_t dst_pitch,
                            float scale, cudaStream_t s);
-// uint8 -> FP16 quads (the quad layout in halves, 8 bytes per pixel): the FP16 form's exact sampler.
-cudaError_t launch_to_quad_half(int W, int H, const uint8_t* src, size_t src_pitch, void* dst, float scale,
+// uint8 -> quads of FP16-rounded values in FP32 lanes: the FP16 form's exact sampler.
+cudaError_t launch_to_quad_half(int W, int H, const uint8_t* src, size_t src_pitch, float4* dst, float scale,
                                 cudaStream_t s);
 // uint8 -> scaled float image whose values are rounded to FP16 (the FP16 form's reference image).
 cudaError_t launch_to_float_h(int W, int H, const uint8_t* src, size_t src_pitch, float* dst, float scale,

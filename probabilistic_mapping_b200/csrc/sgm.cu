@@ -439,6 +439,28 @@ __global__ void __launch_bounds__(128) case_kernel(const void* __restrict__ vol,
 // pair p = paths (2p, 2p+1) runs as one sgm_pair_kernel along direction kDirs[2p].
 const int kDirs[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1}, {-1, 1}, {1, -1}};
 
+// A launch with an explicit priority attribute (recorded into graph nodes under capture), or a
+// plain launch at the stream's priority.
+template <typename... Args>
+cudaError_t launch_with_priority(void (*kern)(Args...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                 int priority, Args... args) {
+    if (priority == 0) {
+        kern<<<grid, block, smem, s>>>(args...);
+        return cudaGetLastError();
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributePriority;
+    attr[0].val.priority = priority;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 template <int PPL, bool HALF, int NW>
 cudaError_t launch_pair_nw(const SgmLaunch& a, int pair, cudaStream_t s) {
     const size_t smem = (size_t)NW * PF * Ring<PPL, HALF>::STAGE_B;
@@ -449,8 +471,8 @@ cudaError_t launch_pair_nw(const SgmLaunch& a, int pair, cudaStream_t s) {
     }
     const int dx = kDirs[2 * pair][0], dy = kDirs[2 * pair][1];
     const int nch = num_chains(dx, dy, a.W, a.H);
-    kern<<<(nch + NW - 1) / NW, NW * 32, smem, s>>>(a, dx, dy, 2 * pair);
-    return cudaGetLastError();
+    return launch_with_priority(kern, dim3((nch + NW - 1) / NW), dim3(NW * 32), smem, s, a.priority, a, dx, dy,
+                                2 * pair);
 }
 
 // scanlines (warps) per block: a.pair_warps in {2, 4, 8}, 4 when unset
@@ -472,13 +494,11 @@ cudaError_t launch_combine(const SgmLaunch& a, int mode, cudaStream_t s) {
     const long blocks_needed = (npix + 7) / 8;   // 8 warps per block
     const int blocks = (int)(blocks_needed < (long)sms * 8 ? blocks_needed : (long)sms * 8);
     const bool eight = a.num_paths == 8;
-    if (mode == kCombineFilter && eight) combine_kernel<PPL, kCombineFilter, 8><<<blocks, 256, 0, s>>>(a);
-    else if (mode == kCombineFilter) combine_kernel<PPL, kCombineFilter, 4><<<blocks, 256, 0, s>>>(a);
-    else if (mode == kCombineArgmin && eight) combine_kernel<PPL, kCombineArgmin, 8><<<blocks, 256, 0, s>>>(a);
-    else if (mode == kCombineArgmin) combine_kernel<PPL, kCombineArgmin, 4><<<blocks, 256, 0, s>>>(a);
-    else if (eight) combine_kernel<PPL, kCombineStore, 8><<<blocks, 256, 0, s>>>(a);
-    else combine_kernel<PPL, kCombineStore, 4><<<blocks, 256, 0, s>>>(a);
-    return cudaGetLastError();
+    void (*kern)(SgmLaunch);
+    if (mode == kCombineFilter) kern = eight ? combine_kernel<PPL, kCombineFilter, 8> : combine_kernel<PPL, kCombineFilter, 4>;
+    else if (mode == kCombineArgmin) kern = eight ? combine_kernel<PPL, kCombineArgmin, 8> : combine_kernel<PPL, kCombineArgmin, 4>;
+    else kern = eight ? combine_kernel<PPL, kCombineStore, 8> : combine_kernel<PPL, kCombineStore, 4>;
+    return launch_with_priority(kern, dim3(blocks), dim3(256), 0, s, a.priority, a);
 }
 
 // Path pairs p = 0 .. num_paths/2 - 1: pairs 0..np-2 run on their own side streams when `side`
