@@ -10,8 +10,9 @@ against the previous keyframe's state.  Workload: 640x480, 128 inverse-depth pla
                   [--form batched|plain|mixed] [--precision fp16|fp32] [--batch B] [--lanes L]
 
 Default (the headline): the FP16 form, B sequences batched (one CUDA-graph launch per step for
-all B), against the plain FP32 form (one StereoMapper, one map after the other) measured in the
-same run.  `value` is depth maps/s with inputs resident in HBM; `e2e` is the same through the
+all B), sources sampled by the texture unit from FP32 texels of FP16-rounded values (as the
+reference's own textures: 8-bit bilinear weights), against the plain FP32 form (one
+StereoMapper, one map after the other, exact bilinear weights) measured in the same run.  `value` is depth maps/s with inputs resident in HBM; `e2e` is the same through the
 public C ABI with pinned host frames and outputs copied inside the timed region.  Under
 torchrun every rank maps its own sequences (no collective on the data path) and the slowest
 rank's time is used.
@@ -38,6 +39,7 @@ PATHS = 8
 # and FP64 rounding would disagree.
 P1, P2, TAU, UNIQ = 0.003, 0.01, 3.5 / 255.0, 0.95
 N_KEYFRAMES = 4
+SAMPLERS = {"exact": 0, "texture": 1, "texture_f32": 2}   # PM_SAMPLER_* of the FP16 form
 
 
 def peaks():
@@ -129,12 +131,13 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
-def make_mapper(precision: int, device: int, cost_mode: int = 0):
+def make_mapper(precision: int, device: int, cost_mode: int = 0, sampler: int = 0):
     from probabilistic_mapping_b200 import scene
     from probabilistic_mapping_b200.mapper import StereoMapper
     rho0, drho = scene.plane_range(D)
     m = StereoMapper(W, H, D, rho0=rho0, intensity_scale=1 / 255, num_paths=PATHS, p1=P1, p2=P2, tau_so=TAU,
-                     uniqueness_ratio=UNIQ, cost_mode=cost_mode, precision=precision, device=device)
+                     uniqueness_ratio=UNIQ, cost_mode=cost_mode, precision=precision, device=device,
+                     sampler=sampler if precision == 1 else 0)
     return m, drho
 
 
@@ -174,7 +177,7 @@ def run_ours(args, rank, world, precision: str = "fp32", passes=("dev", "e2e", "
     K = seq[0].K
     fx, fy, cx, cy = K[0, 0], K[1, 1], K[0, 2], K[1, 2]
     prec = 1 if precision == "fp16" else 0
-    m, drho = make_mapper(prec, dev, 1 if args.cost_mode == "corrected" else 0)
+    m, drho = make_mapper(prec, dev, 1 if args.cost_mode == "corrected" else 0, SAMPLERS[args.sampler])
     m.initIntrinsic(K, 0.0, drho)
     stream = torch.cuda.Stream(device=dev)
     m.set_stream(stream.cuda_stream)
@@ -265,7 +268,7 @@ def run_batched(args, rank, world, precision: str, B: int, host_io: bool, clocks
     prec = _lib.PM_PREC_FP16 if precision == "fp16" else _lib.PM_PREC_FP32
     cfg = dict(width=W, height=H, num_planes=D, rho0=rho0, intensity_scale=1 / 255, num_paths=PATHS, p1=P1, p2=P2,
                tau_so=TAU, uniqueness_ratio=UNIQ, cost_mode=1 if args.cost_mode == "corrected" else 0,
-               precision=prec, device=dev)
+               precision=prec, device=dev, sampler=SAMPLERS[args.sampler] if prec == _lib.PM_PREC_FP16 else 0)
     seqs = [scene.make_sequence(W, H, F_PX, S, 2, seed=2000 + 97 * rank + i) for i in range(B)]
     b = StereoBatch([cfg] * B, S, lanes=0, host_io=host_io, autotune=True, priority=args.priority)
     for i in range(B):
@@ -327,7 +330,8 @@ def run_mixed(args, rank, world, precision: str, host_io: bool, clocks: bool):
         for _ in range(MIXED_PER_SHAPE):
             cfgs.append(dict(width=w, height=h, num_planes=d, rho0=rho0, intensity_scale=1 / 255, num_paths=PATHS,
                              p1=P1, p2=P2, tau_so=TAU, uniqueness_ratio=UNIQ,
-                             cost_mode=1 if args.cost_mode == "corrected" else 0, precision=prec, device=dev))
+                             cost_mode=1 if args.cost_mode == "corrected" else 0, precision=prec, device=dev,
+                             sampler=SAMPLERS[args.sampler] if prec == _lib.PM_PREC_FP16 else 0))
             shapes.append(k)
     mine = shard_sequences(cfgs, world, MIXED_S)[rank]
     scenes = {k: [scene.make_sequence(w, h, f, MIXED_S, 2, seed=3000 + 10 * k + j) for j in range(2)]
@@ -389,7 +393,8 @@ def mixed_main(args, rank, world):
                 "scaling": "strong", "vs_baseline": None, "dtype": "f16" if precision == "fp16" else "f32",
                 "data": "synthetic",
                 "config": {"workload": f"48 sequences, {MIXED_S} sources, {PATHS}-path SGM, fusion step, "
-                                       f"{precision}, lanes={args.lanes}", "global_batch": total, "seq_len": 0,
+                                       f"{precision}" + (f" {args.sampler} sampler" if precision == "fp16" else "")
+                                       + f", lanes={args.lanes}", "global_batch": total, "seq_len": 0,
                            "parallelism": f"sequence shards x{world}, balanced by voxels x sources",
                            "l2": "per-map working sets exceed the 126 MB L2"},
                 "voxels_per_s": vox * args.steps / (t / 1000.0),
@@ -439,6 +444,8 @@ def main():
                     help="batched: B sequences of the headline workload; plain: one map after the other; "
                          "mixed: the 48-sequence three-size batch, sharded over ranks")
     ap.add_argument("--lanes", type=int, default=0, help="volume sets per size in the mixed batch (0: one each)")
+    ap.add_argument("--sampler", choices=list(SAMPLERS), default="texture_f32",
+                    help="FP16 form: source sampling (exact FP32 bilinear, or the texture unit from FP16 / FP32 texels)")
     ap.add_argument("--priority", type=int, default=1, choices=[0, 1],
                     help="batched forms: SGM kernels at the greatest launch priority (1) or not (0)")
     ap.add_argument("--precision", choices=["fp32", "fp16"], default=None,
@@ -532,6 +539,7 @@ def main():
             "config": {"workload": f"{W}x{H}, {D} planes, {S} sources, {PATHS}-path SGM, uniqueness {UNIQ}, "
                                    f"fusion step; {args.precision} {args.form} form"
                                    + (f", {B} sequences per CUDA-graph launch" if args.form == "batched" else "")
+                                   + (f", {args.sampler} sampler" if args.precision == "fp16" else "")
                                    + f", {args.cost_mode} cost samples",
                        "global_batch": world * B, "seq_len": 0, "parallelism": f"replicas x{world}",
                        "l2": "per-map working set (cost + path volumes, >1 GB) exceeds the 126 MB L2"},

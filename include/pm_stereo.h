@@ -51,9 +51,12 @@ typedef int pm_status;
 #define PM_PREC_FP16 1 /* FP16 cost volume, FP32 SGM accumulators and fusion */
 
 /* How the FP16 form samples source frames (the FP32 form always uses exact bilinear weights). */
-#define PM_SAMPLER_EXACT 0   /* FP16 images, bilinear weights and interpolation in FP32 */
-#define PM_SAMPLER_TEXTURE 1 /* FP16 images filtered by the texture unit (8-bit weights, as the
-                                reference's own textures, calc_cost.cu:226-237) */
+#define PM_SAMPLER_EXACT 0   /* FP16-rounded images, bilinear weights and interpolation in FP32 */
+#define PM_SAMPLER_TEXTURE 1 /* FP16 texels filtered by the texture unit (8-bit weights, as the
+                                reference's own textures, calc_cost.cu:226-237; the unit filters
+                                FP16 texels at reduced precision) */
+#define PM_SAMPLER_TEXTURE_F32 2 /* FP16-rounded images in FP32 texels: the texture unit's 8-bit
+                                    weights with FP32 filtering, at the speed of PM_SAMPLER_TEXTURE */
 
 #define PM_FUSION_GPU 0      /* StereoMapper::outputFusion + depth_fusion.cu kernels */
 #define PM_FUSION_CPU_PATH 1 /* the constants and masks of outputFusionCPU, run on the GPU */
@@ -157,6 +160,9 @@ typedef struct pm_buffers {
     const int32_t* wta_index; /* W*H winner-take-all plane index */
     const float* wta_depth;   /* W*H */
     const int32_t* table;  /* W*H propagation table of the last fusion step */
+    const float* cost_offset; /* FP16 form: W*H; the half volume holds cost - cost_offset[pixel],
+                                 the pixel's smallest measured cost (0 when some plane of the pixel
+                                 is unmeasured); NULL in the FP32 form */
 } pm_buffers;
 PM_API pm_status pm_get_buffers(pm_mapper* h, pm_buffers* out);
 PM_API pm_status pm_debug_store_sgm(pm_mapper* h, int enable);

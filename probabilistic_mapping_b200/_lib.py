@@ -24,6 +24,7 @@ PM_PREC_FP32 = 0
 PM_PREC_FP16 = 1
 PM_SAMPLER_EXACT = 0
 PM_SAMPLER_TEXTURE = 1
+PM_SAMPLER_TEXTURE_F32 = 2
 PM_BATCH_HOST_IO = 1
 PM_BATCH_AUTOTUNE = 2
 PM_BATCH_PRIORITY = 4
@@ -60,7 +61,7 @@ class PmDiffConfig(ctypes.Structure):
 
 class PmBuffers(ctypes.Structure):
     _fields_ = [("cost", ctypes.c_void_p), ("sgm", ctypes.c_void_p), ("wta_index", ctypes.c_void_p),
-                ("wta_depth", ctypes.c_void_p), ("table", ctypes.c_void_p)]
+                ("wta_depth", ctypes.c_void_p), ("table", ctypes.c_void_p), ("cost_offset", ctypes.c_void_p)]
 
 
 # Every exported entry point with its argument types; also the list the load test checks.

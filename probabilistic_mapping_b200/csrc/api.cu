@@ -30,7 +30,7 @@ struct pm_mapper {
     uint8_t* d_u8 = nullptr;    // upload staging, W*H bytes
     float* d_ref = nullptr;     // scaled reference image
     float4* d_srcq = nullptr;   // max_sources source frames in the quad layout (FP16 form: FP16-rounded values)
-    void* d_srch[kMaxSources] = {};               // FP16 form, texture sampler: pitched FP16 frames
+    void* d_srch[kMaxSources] = {};               // FP16 form, texture samplers: pitched FP16 or FP32 texels
     size_t srch_pitch = 0;
     cudaTextureObject_t tex[kMaxSources] = {};    // FP16 form: one texture object per slot
     int nsrc = 0;               // queued (not yet folded) sources
@@ -41,6 +41,8 @@ struct pm_mapper {
     bool has_state = false;     // cost/cnt hold a folded running state
 
     void* d_cost = nullptr;     // W*H*D float or half
+    float* d_off = nullptr;     // FP16 form: per-pixel shift of the half volume (W*H)
+    float* d_boff = nullptr;    // FP16 form: block offsets before the rebase (W*H*D/16)
     float* d_cnt = nullptr;     // allocated on the first fold
     float* d_part[8] = {};      // SGM: one volume per path (num_paths of them)
     SgmStreams side{};          // concurrent path groups
@@ -190,9 +192,9 @@ pm_status check_config(const pm_config* c, pm_mapper* h) {
         return fail(h, PM_ERR_INVALID_ARGUMENT, "unknown precision %d", c->precision);
     if (c->precision == PM_PREC_FP16 && c->num_planes % 64)
         return fail(h, PM_ERR_INVALID_ARGUMENT, "FP16 volumes need num_planes to be a multiple of 64");
-    if (c->sampler != PM_SAMPLER_EXACT && c->sampler != PM_SAMPLER_TEXTURE)
+    if (c->sampler != PM_SAMPLER_EXACT && c->sampler != PM_SAMPLER_TEXTURE && c->sampler != PM_SAMPLER_TEXTURE_F32)
         return fail(h, PM_ERR_INVALID_ARGUMENT, "unknown sampler %d", c->sampler);
-    if (c->sampler == PM_SAMPLER_TEXTURE && c->precision != PM_PREC_FP16)
+    if (c->sampler != PM_SAMPLER_EXACT && c->precision != PM_PREC_FP16)
         return fail(h, PM_ERR_INVALID_ARGUMENT, "the texture sampler belongs to the FP16 form");
     if (c->fusion_variant != PM_FUSION_GPU && c->fusion_variant != PM_FUSION_CPU_PATH)
         return fail(h, PM_ERR_INVALID_ARGUMENT, "unknown fusion_variant %d", c->fusion_variant);
@@ -248,6 +250,8 @@ pm_status upload_image(pm_mapper* h, const uint8_t* img, size_t pitch, float* ds
     const bool half = h->cfg.precision == PM_PREC_FP16;
     if (slot >= 0 && half && h->cfg.sampler == PM_SAMPLER_TEXTURE)
         PM_CK(h, launch_to_half(W, H, dev, pitch, h->d_srch[slot], h->srch_pitch, sc, h->stream));
+    else if (slot >= 0 && half && h->cfg.sampler == PM_SAMPLER_TEXTURE_F32)
+        PM_CK(h, launch_to_float_h_pitched(W, H, dev, pitch, (float*)h->d_srch[slot], h->srch_pitch, sc, h->stream));
     else if (slot >= 0 && half)
         PM_CK(h, launch_to_quad_half(W, H, dev, pitch, h->d_srcq + (size_t)slot * W * H, sc, h->stream));
     else if (slot >= 0)
@@ -268,13 +272,15 @@ pm_status evaluate_cost(pm_mapper* h, bool into_state) {
     a.ref = h->d_ref;
     a.srcq = h->d_srcq;
     a.nsrc = h->nsrc;
-    if (c.precision == PM_PREC_FP16 && c.sampler == PM_SAMPLER_TEXTURE) {
+    if (c.precision == PM_PREC_FP16 && c.sampler != PM_SAMPLER_EXACT) {
         a.use_tex = 1;
         for (int s = 0; s < h->nsrc; ++s) a.tex[s] = h->tex[s];
     }
     for (int s = 0; s < h->nsrc; ++s)
         for (int i = 0; i < 12; ++i) a.hom[s][i] = h->homs[12 * s + i];
     a.cost = h->d_cost;
+    a.offset = h->d_off;
+    a.block_offset = h->d_boff;
     if (into_state || h->has_state) {
         if (!h->d_cnt) PM_CK(h, cudaMalloc(&h->d_cnt, sizeof(float) * (size_t)c.width * c.height * c.num_planes));
         a.cnt = h->d_cnt;
@@ -295,6 +301,7 @@ pm_status run_sgm_filter(pm_mapper* h) {
     SgmLaunch a;
     fill_sgm_launch(c, h->order, a);
     a.cost = h->d_cost;
+    a.offset = h->d_off;
     a.ref = h->d_ref;
     for (int r = 0; r < c.num_paths; ++r) a.part[r] = h->d_part[r];
     a.total = h->store_sgm ? h->d_part[0] : nullptr;   // combine reads part[0] of a pixel before writing it
@@ -340,6 +347,8 @@ void release(pm_mapper* h) {
         cudaFree(h->d_srch[s]);
     }
     cudaFree(h->d_cost);
+    cudaFree(h->d_off);
+    cudaFree(h->d_boff);
     cudaFree(h->d_cnt);
     for (auto* p : h->d_part) cudaFree(p);
     cudaFree(h->d_depth);
@@ -419,33 +428,18 @@ pm_status pm_create(const pm_config* cfg, pm_mapper** out) {
     h->own_stream = ok;
     const bool half = cfg->precision == PM_PREC_FP16;
     ok = ok && alloc((void**)&h->d_u8, N) && alloc((void**)&h->d_ref, 4 * N) &&
-         ((half && cfg->sampler == PM_SAMPLER_TEXTURE) || alloc((void**)&h->d_srcq, 16 * N * cfg->max_sources)) &&
-         alloc(&h->d_cost, esz * V) &&
+         ((half && cfg->sampler != PM_SAMPLER_EXACT) || alloc((void**)&h->d_srcq, 16 * N * cfg->max_sources)) &&
+         alloc(&h->d_cost, esz * V) && (!half || (alloc((void**)&h->d_off, 4 * N) && alloc((void**)&h->d_boff, 4 * N * (cfg->num_planes / 16)))) &&
          alloc((void**)&h->d_depth, 4 * N) &&
          alloc((void**)&h->d_idx, 4 * N) && alloc((void**)&h->d_ztable, 8 * N) &&
          alloc((void**)&h->d_table, 4 * N) && alloc((void**)&h->d_fused, 4 * N) &&
          alloc((void**)&h->d_var, 4 * N);
-    // FP16 form: per-slot pitched FP16 images sampled through texture objects (linear filter,
-    // zero border, unnormalised coordinates: the reference's texture setup, calc_cost.cu:226-237)
-    for (int s = 0; half && cfg->sampler == PM_SAMPLER_TEXTURE && s < cfg->max_sources && ok; ++s) {
-        ok = note(cudaMallocPitch(&h->d_srch[s], &h->srch_pitch, sizeof(__half) * cfg->width, cfg->height));
-        if (!ok) break;
-        cudaResourceDesc rd;
-        std::memset(&rd, 0, sizeof rd);
-        rd.resType = cudaResourceTypePitch2D;
-        rd.res.pitch2D.devPtr = h->d_srch[s];
-        rd.res.pitch2D.desc = cudaCreateChannelDescHalf();
-        rd.res.pitch2D.width = cfg->width;
-        rd.res.pitch2D.height = cfg->height;
-        rd.res.pitch2D.pitchInBytes = h->srch_pitch;
-        cudaTextureDesc td;
-        std::memset(&td, 0, sizeof td);
-        td.addressMode[0] = td.addressMode[1] = cudaAddressModeBorder;
-        td.filterMode = cudaFilterModeLinear;
-        td.readMode = cudaReadModeElementType;
-        td.normalizedCoords = 0;
-        ok = note(cudaCreateTextureObject(&h->tex[s], &rd, &td, nullptr));
-    }
+    // FP16 form: per-slot pitched images (FP16 texels, or FP16-rounded values in FP32 texels)
+    // sampled through texture objects (linear filter, zero border, unnormalised coordinates: the
+    // reference's texture setup, calc_cost.cu:226-237)
+    for (int s = 0; half && cfg->sampler != PM_SAMPLER_EXACT && s < cfg->max_sources && ok; ++s)
+        ok = note(make_source_texture(cfg->width, cfg->height, cfg->sampler == PM_SAMPLER_TEXTURE_F32, &h->d_srch[s],
+                                      &h->srch_pitch, &h->tex[s]));
     for (int r = 0; r < cfg->num_paths && ok; ++r) ok = alloc((void**)&h->d_part[r], 4 * V);
     if (ok && cfg->fusion_variant == PM_FUSION_CPU_PATH) {
         if (cfg->width >= 65536 || cfg->height >= 65536) ok = note(cudaErrorInvalidValue);
@@ -579,10 +573,11 @@ pm_status pm_output_case(pm_mapper* h, int output_case, float* result, size_t pi
     SgmLaunch a;
     fill_sgm_launch(c, h->order, a);
     if (output_case == PM_CASE_RAW_ARGMIN) {   // stereo_mapper.cpp:628-662
-        PM_CK(h, launch_case_argmin(h->d_cost, a.cost_half, c.width, c.height, c.num_planes, a.fp, h->d_fused,
+        PM_CK(h, launch_case_argmin(h->d_cost, a.cost_half, h->d_off, c.width, c.height, c.num_planes, a.fp, h->d_fused,
                                     sizeof(float) * (size_t)c.width, h->d_idx, h->stream));
     } else {                                   // stereo_mapper.cpp:668-706
         a.cost = h->d_cost;
+        a.offset = h->d_off;
         a.ref = h->d_ref;
         for (int r = 0; r < c.num_paths; ++r) a.part[r] = h->d_part[r];
         a.depth = h->d_fused;
@@ -720,6 +715,7 @@ pm_status pm_set_state(pm_mapper* h, const float* alpha, const float* beta, cons
 pm_status pm_get_buffers(pm_mapper* h, pm_buffers* out) {
     if (!h || !out) return PM_ERR_INVALID_ARGUMENT;
     out->cost = h->d_cost;
+    out->cost_offset = h->d_off;
     out->sgm = h->d_part[0];
     out->wta_index = h->d_idx;
     out->wta_depth = h->d_depth;

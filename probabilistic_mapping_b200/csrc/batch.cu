@@ -41,6 +41,8 @@ namespace {
 // Large buffers one sequence needs only while its cost volume and SGM are in flight.
 struct LaneBufs {
     void* cost = nullptr;
+    float* off = nullptr;    // FP16 volumes: the per-pixel shift (see CostLaunch::offset)
+    float* boff = nullptr;   // FP16 volumes: block offsets before the rebase
     float* part[8] = {};
     int last_user = -1;   // sequence index that used this set last in the capture order
 };
@@ -62,6 +64,10 @@ struct Seq {
     // persistent device state
     float* d_ref = nullptr;
     float4* d_srcq = nullptr;
+    // FP16 form with a texture sampler: pitched source images and their texture objects
+    void* d_srch[kMaxSources] = {};
+    size_t srch_pitch = 0;
+    cudaTextureObject_t tex[kMaxSources] = {};
     float* d_depth = nullptr;
     int32_t* d_idx = nullptr;
     float* d_state[2][4] = {};
@@ -151,6 +157,8 @@ void free_batch(pm_batch* b) {
     }
     for (auto& l : b->lanes) {
         cudaFree(l.cost);
+        cudaFree(l.off);
+        cudaFree(l.boff);
         for (auto* p : l.part) cudaFree(p);
     }
     for (auto& q : b->seqs) {
@@ -163,6 +171,10 @@ void free_batch(pm_batch* b) {
         }
         cudaFree(q.d_ref);
         cudaFree(q.d_srcq);
+        for (int s = 0; s < kMaxSources; ++s) {
+            if (q.tex[s]) cudaDestroyTextureObject(q.tex[s]);
+            cudaFree(q.d_srch[s]);
+        }
         cudaFree(q.d_depth);
         cudaFree(q.d_idx);
         for (auto& s : q.d_state)
@@ -188,6 +200,7 @@ SgmLaunch sgm_launch(const Seq& q, const LaneBufs& l, int priority) {
     std::memset(&a, 0, sizeof a);
     const pm_config& c = q.cfg;
     a.cost = l.cost;
+    a.offset = l.off;
     a.cost_half = c.precision == PM_PREC_FP16;
     a.ref = q.d_ref;
     for (int r = 0; r < c.num_paths; ++r) a.part[r] = l.part[r];
@@ -231,8 +244,13 @@ cudaError_t enqueue_seq(pm_batch* b, int i, int k) {
     if (e) return e;
     for (int s = 0; s < S; ++s) {
         const uint8_t* f = q.d_frames[k] + (1 + s) * N;
-        e = half ? launch_to_quad_half(W, H, f, W, q.d_srcq + (size_t)s * N, sc, m)
-                 : launch_to_quad(W, H, f, W, q.d_srcq + (size_t)s * N, sc, m);
+        if (c.sampler == PM_SAMPLER_TEXTURE)
+            e = launch_to_half(W, H, f, W, q.d_srch[s], q.srch_pitch, sc, m);
+        else if (c.sampler == PM_SAMPLER_TEXTURE_F32)
+            e = launch_to_float_h_pitched(W, H, f, W, (float*)q.d_srch[s], q.srch_pitch, sc, m);
+        else
+            e = half ? launch_to_quad_half(W, H, f, W, q.d_srcq + (size_t)s * N, sc, m)
+                     : launch_to_quad(W, H, f, W, q.d_srcq + (size_t)s * N, sc, m);
         if (e) return e;
     }
     // the lane's volumes are free once the previous sequence in this lane has finished its SGM
@@ -242,6 +260,12 @@ cudaError_t enqueue_seq(pm_batch* b, int i, int k) {
     std::memset(&a, 0, sizeof a);
     a.ref = q.d_ref;
     a.srcq = q.d_srcq;
+    if (c.sampler != PM_SAMPLER_EXACT) {
+        a.use_tex = 1;
+        for (int s = 0; s < S; ++s) a.tex[s] = q.tex[s];
+    }
+    a.offset = l.off;
+    a.block_offset = l.boff;
     a.W = W;
     a.H = H;
     a.D = c.num_planes;
@@ -372,8 +396,7 @@ pm_status pm_batch_create(const pm_config* cfgs, int n, int num_sources, int lan
         return PM_ERR_INVALID_ARGUMENT;
     for (int i = 0; i < n; ++i) {
         if (validate_config(&cfgs[i]) != PM_OK) return PM_ERR_INVALID_ARGUMENT;
-        if (cfgs[i].sampler != PM_SAMPLER_EXACT || cfgs[i].fusion_variant != PM_FUSION_GPU ||
-            cfgs[i].device != cfgs[0].device)
+        if (cfgs[i].fusion_variant != PM_FUSION_GPU || cfgs[i].device != cfgs[0].device)
             return PM_ERR_UNSUPPORTED;
     }
     pm_batch* b = new pm_batch();
@@ -417,6 +440,9 @@ pm_status pm_batch_create(const pm_config* cfgs, int n, int num_sources, int lan
             LaneBufs l;
             const size_t esz = q.cfg.precision == PM_PREC_FP16 ? 2 : 4;
             ok = alloc(&l.cost, esz * q.V);
+            if (ok && esz == 2)
+                ok = alloc((void**)&l.off, 4 * q.N) && note(cudaMemset(l.off, 0, 4 * q.N)) &&
+                     alloc((void**)&l.boff, 4 * q.N * (q.cfg.num_planes / 16));
             for (int r = 0; r < q.cfg.num_paths && ok; ++r) ok = alloc((void**)&l.part[r], 4 * q.V);
             b->lanes.push_back(l);
             if (!ok) break;
@@ -433,12 +459,15 @@ pm_status pm_batch_create(const pm_config* cfgs, int n, int num_sources, int lan
             if (ok) std::memset(q.h_par[k], 0, sizeof(float) * q.par_floats);
         }
         ok = ok && alloc((void**)&q.d_ref, 4 * N) &&
-             alloc((void**)&q.d_srcq, 16 * N * q.S) &&
+             (q.cfg.sampler != PM_SAMPLER_EXACT || alloc((void**)&q.d_srcq, 16 * N * q.S)) &&
              alloc((void**)&q.d_depth, 4 * N) && alloc((void**)&q.d_idx, 4 * N) &&
              alloc((void**)&q.d_ztable, 8 * N) && alloc((void**)&q.d_table, 4 * N) &&
              alloc((void**)&q.d_fused, 4 * N) && alloc((void**)&q.d_var, 4 * N);
         for (int s = 0; s < 2 && ok; ++s)
             for (int k = 0; k < 4 && ok; ++k) ok = alloc((void**)&q.d_state[s][k], 4 * N);
+        for (int s = 0; q.cfg.sampler != PM_SAMPLER_EXACT && s < q.S && ok; ++s)
+            ok = note(make_source_texture(q.cfg.width, q.cfg.height, q.cfg.sampler == PM_SAMPLER_TEXTURE_F32,
+                                          &q.d_srch[s], &q.srch_pitch, &q.tex[s]));
         for (int s = 0; s < 4 && ok; ++s) ok = note(cudaStreamCreateWithFlags(&q.st[s], cudaStreamNonBlocking));
         if (ok) {
             for (int s = 0; s < 3; ++s) q.side.stream[s] = q.st[1 + s];

@@ -7,6 +7,8 @@
 //                    taken in bytes; the reference received a byte step and indexed with it in
 //                    floats (stereo_mapper.cpp:149-152 vs convert.cu:16-21), which reads past
 //                    the end of the source for every row after the first quarter.
+#include <cstring>
+
 #include "pm_device.cuh"
 
 namespace pm {
@@ -46,7 +48,9 @@ __global__ void __launch_bounds__(256) to_half_kernel(int W, int H, const uint8_
     const uint8_t* row = src + (size_t)y * pitch;
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < W; x += gridDim.x * blockDim.x) {
         const __half v = __float2half_rn(__fmul_rn((float)row[x], scale));
-        if (as_float) reinterpret_cast<float*>(dst)[(size_t)y * W + x] = __half2float(v);
+        if (as_float)   // FP16-rounded values in float lanes, pitched (dst_pitch 0: packed rows)
+            reinterpret_cast<float*>(reinterpret_cast<char*>(dst) + (size_t)y * (dst_pitch ? dst_pitch : 4 * (size_t)W))[x] =
+                __half2float(v);
         else reinterpret_cast<__half*>(reinterpret_cast<char*>(dst) + (size_t)y * dst_pitch)[x] = v;
     }
 }
@@ -108,6 +112,13 @@ cudaError_t launch_to_half(int W, int H, const uint8_t* src, size_t src_pitch, v
     return cudaGetLastError();
 }
 
+cudaError_t launch_to_float_h_pitched(int W, int H, const uint8_t* src, size_t src_pitch, float* dst,
+                                     size_t dst_pitch, float scale, cudaStream_t s) {
+    const dim3 grid((W + 255) / 256, H);
+    to_half_kernel<<<grid, 256, 0, s>>>(W, H, src, src_pitch, reinterpret_cast<__half*>(dst), dst_pitch, scale, 1);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_to_float_h(int W, int H, const uint8_t* src, size_t src_pitch, float* dst, float scale,
                               cudaStream_t s) {
     const dim3 grid((W + 255) / 256, H);
@@ -120,6 +131,29 @@ cudaError_t launch_to_quad_half(int W, int H, const uint8_t* src, size_t src_pit
     const dim3 grid((W + 255) / 256, H);
     to_quad_half_kernel<<<grid, 256, 0, s>>>(W, H, src, src_pitch, dst, scale);
     return cudaGetLastError();
+}
+
+cudaError_t make_source_texture(int W, int H, bool f32, void** buf, size_t* pitch, unsigned long long* tex) {
+    cudaError_t e = cudaMallocPitch(buf, pitch, (f32 ? 4 : 2) * (size_t)W, (size_t)H);
+    if (e != cudaSuccess) return e;
+    cudaResourceDesc rd;
+    std::memset(&rd, 0, sizeof rd);
+    rd.resType = cudaResourceTypePitch2D;
+    rd.res.pitch2D.devPtr = *buf;
+    rd.res.pitch2D.desc = f32 ? cudaCreateChannelDesc<float>() : cudaCreateChannelDescHalf();
+    rd.res.pitch2D.width = W;
+    rd.res.pitch2D.height = H;
+    rd.res.pitch2D.pitchInBytes = *pitch;
+    cudaTextureDesc td;
+    std::memset(&td, 0, sizeof td);
+    td.addressMode[0] = td.addressMode[1] = cudaAddressModeBorder;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    cudaTextureObject_t t = 0;
+    e = cudaCreateTextureObject(&t, &rd, &td, nullptr);
+    *tex = t;
+    return e;
 }
 
 cudaError_t launch_convert(int W, int H, const float* in, float* out, int flag, size_t pitch, cudaStream_t s) {

@@ -237,6 +237,7 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
             if (gx < W && gy < H) {
                 const size_t g = ((size_t)gy * W + gx) * D + d0 + k;
                 c0 = load_cost<HALF>(a.cost, g);
+                if constexpr (HALF) c0 = __fadd_rn(c0, a.offset[(size_t)gy * W + gx]);
                 n0 = a.cnt[g];
             }
         }
@@ -338,14 +339,44 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
 
     // store contiguous plane runs of the volume (plane-innermost layout)
     __syncthreads();
-    for (int e = tid; e < NPIX * PCB; e += NT) {
-        const int p = e / PCB, k = e - p * PCB;
-        const int o = p / TXU, i = p - o * TXU;
-        const int gx = x0 + i, gy = y0 + o;
-        if (gx < W && gy < H) {
-            const size_t g = ((size_t)gy * W + gx) * D + d0 + k;
-            store_cost<HALF>(a.cost, g, accs[p * SP + k]);
-            if (a.cnt) a.cnt[g] = cnts[p * SP + k];
+    if constexpr (HALF) {
+        // per pixel and 16-plane block: the smallest measured cost of the block (0 when none is
+        // measured) is stored beside the block, and the half volume holds the differences
+        __shared__ float s_off[NPIX];
+        for (int p = tid; p < NPIX; p += NT) {
+            float m = inf_f();
+#pragma unroll
+            for (int k = 0; k < PCB; ++k) {
+                const float v = accs[p * SP + k];
+                m = v >= 0.0f ? fminf(m, v) : m;
+            }
+            m = m == inf_f() ? 0.0f : m;
+            s_off[p] = m;
+            const int o = p / TXU, i = p - o * TXU;
+            const int gx = x0 + i, gy = y0 + o;
+            if (gx < W && gy < H) a.block_offset[((size_t)gy * W + gx) * (D / PCB) + blockIdx.z] = m;
+        }
+        __syncthreads();
+        for (int e = tid; e < NPIX * PCB; e += NT) {
+            const int p = e / PCB, k = e - p * PCB;
+            const int o = p / TXU, i = p - o * TXU;
+            const int gx = x0 + i, gy = y0 + o;
+            if (gx < W && gy < H) {
+                const size_t g = ((size_t)gy * W + gx) * D + d0 + k;
+                store_cost<true>(a.cost, g, __fsub_rn(accs[p * SP + k], s_off[p]));
+                if (a.cnt) a.cnt[g] = cnts[p * SP + k];
+            }
+        }
+    } else {
+        for (int e = tid; e < NPIX * PCB; e += NT) {
+            const int p = e / PCB, k = e - p * PCB;
+            const int o = p / TXU, i = p - o * TXU;
+            const int gx = x0 + i, gy = y0 + o;
+            if (gx < W && gy < H) {
+                const size_t g = ((size_t)gy * W + gx) * D + d0 + k;
+                store_cost<false>(a.cost, g, accs[p * SP + k]);
+                if (a.cnt) a.cnt[g] = cnts[p * SP + k];
+            }
         }
     }
 }
@@ -361,6 +392,31 @@ __global__ void __launch_bounds__(256) invalid_kernel(const void* cost, long npi
     for (int d = lane; d < D; d += 32) neg |= load_cost<HALF>(cost, (size_t)pix * D + d) < 0.0f;
     const bool any = __any_sync(kFull, neg);
     if (lane == 0) invalid[pix] = any ? 1 : 0;
+}
+
+// Moves every 16-plane block of a pixel from its own offset to the pixel's: the smallest block
+// offset, or 0 when some plane is unmeasured (negative).  One warp per pixel, lane l holding
+// planes [l*PPL, (l+1)*PPL), rewritten in place.
+template <int PPL>
+__global__ void __launch_bounds__(256) rebase_kernel(__half* __restrict__ cost, const float* __restrict__ boff,
+                                                     float* __restrict__ off, long npix, int D) {
+    const long pix = (long)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (pix >= npix) return;
+    const int nb = D >> 4;
+    const float* bo = boff + (size_t)pix * nb;
+    __half* c = cost + (size_t)pix * D + lane * PPL;
+    float v[PPL];
+    bool neg = false;
+#pragma unroll
+    for (int j = 0; j < PPL; ++j) {
+        v[j] = __half2float(c[j]);
+        neg |= v[j] < 0.0f;
+    }
+    const float g = __any_sync(kFull, neg) ? 0.0f : warp_min_f32(lane < nb ? __ldg(bo + lane) : inf_f());
+#pragma unroll
+    for (int j = 0; j < PPL; ++j) c[j] = __float2half_rn(__fadd_rn(v[j], __fsub_rn(__ldg(bo + ((lane * PPL + j) >> 4)), g)));
+    if (lane == 0) off[pix] = g;
 }
 
 template <int MODE, bool HALF, int SAMP>
@@ -390,11 +446,26 @@ cudaError_t launch_q(const CostLaunch& a, dim3 grid, cudaStream_t s) {
 
 cudaError_t launch_cost(const CostLaunch& a, cudaStream_t s) {
     if (a.nsrc > kMaxSources || a.D % PCB || a.W < 1 || a.H < 1) return cudaErrorInvalidValue;
+    if (a.cost_half && (!a.offset || !a.block_offset || (a.D / 32) % 2)) return cudaErrorInvalidValue;
     const dim3 grid((a.W + TXU - 1) / TXU, (a.H + TY - 1) / TY, a.D / PCB);
     cudaError_t e;
     if (a.mode == 0) e = a.cost_half ? launch_q<0, true>(a, grid, s) : launch_q<0, false>(a, grid, s);
     else e = a.cost_half ? launch_q<1, true>(a, grid, s) : launch_q<1, false>(a, grid, s);
-    if (e != cudaSuccess || !a.invalid) return e;
+    if (e != cudaSuccess) return e;
+    if (a.cost_half) {
+        const long np = (long)a.W * a.H;
+        const unsigned blocks = (unsigned)((np + 7) / 8);
+        __half* c = static_cast<__half*>(a.cost);
+        switch (a.D / 32) {
+            case 2: rebase_kernel<2><<<blocks, 256, 0, s>>>(c, a.block_offset, a.offset, np, a.D); break;
+            case 4: rebase_kernel<4><<<blocks, 256, 0, s>>>(c, a.block_offset, a.offset, np, a.D); break;
+            case 6: rebase_kernel<6><<<blocks, 256, 0, s>>>(c, a.block_offset, a.offset, np, a.D); break;
+            case 8: rebase_kernel<8><<<blocks, 256, 0, s>>>(c, a.block_offset, a.offset, np, a.D); break;
+            default: return cudaErrorInvalidValue;
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (!a.invalid) return cudaSuccess;
     const long npix = (long)a.W * a.H;
     if (a.cost_half) invalid_kernel<true><<<(unsigned)((npix + 7) / 8), 256, 0, s>>>(a.cost, npix, a.D, a.invalid);
     else invalid_kernel<false><<<(unsigned)((npix + 7) / 8), 256, 0, s>>>(a.cost, npix, a.D, a.invalid);

@@ -31,6 +31,14 @@ struct CostLaunch {
     const float* hom_dev;  // batched form: the homographies (nsrc x 12) in device memory, or nullptr
     void* cost;            // W*H*D float, or __half when cost_half
     int cost_half;
+    // FP16 volumes hold cost - offset[pixel], offset = the pixel's smallest measured cost (0 when
+    // some plane is unmeasured, i.e. for a pixel the SGM treats as invalid), so that the values
+    // near the minimum keep FP16's relative precision.  The SGM recurrences are unchanged by a
+    // per-pixel shift; the winner-take-all adds it back once per path.  The kernel first writes
+    // each 16-plane block relative to its own minimum (block_offset); a rebase pass then moves
+    // every block to the pixel's offset.
+    float* offset;         // W*H (cost_half only)
+    float* block_offset;   // W*H*(D/16) scratch (cost_half only)
     float* cnt;            // running count (incremental mode) or nullptr
     uint8_t* invalid;      // W*H, 1 where a plane was never measured (optional)
     int incremental;       // start from (cost, cnt) in memory instead of (-1, 0)
@@ -55,6 +63,7 @@ struct SgmLaunch {
     const float* ref;      // W*H scaled reference image (path gradient D1, sgm.cu:75)
     float* part[8];        // W*H*D volume of each path (num_paths of them), reference path order
     float* total;          // W*H*D complete sum (may alias part[0]); nullptr: not stored
+    const float* offset;   // W*H per-pixel shift of an FP16 cost volume (see CostLaunch), or nullptr
     int W, H, D, num_paths;
     float p1, p2, tau, q1, q2;
     FilterParams fp;
@@ -79,9 +88,9 @@ enum CombineMode { kCombineStore = 0, kCombineFilter = 1, kCombineArgmin = 2 };
 // registers and writes depth/index with the winner-take-all filter (kCombineFilter) or the debug
 // argmin (kCombineArgmin); kCombineStore only writes `total`.  side == nullptr runs everything on s.
 cudaError_t launch_sgm(const SgmLaunch& a, int mode, cudaStream_t s, const SgmStreams* side);
-// The debug argmin over a float (half = 0) or __half (half = 1) W*H*D volume.
-cudaError_t launch_case_argmin(const void* vol, int half, int W, int H, int D, const FilterParams& fp, float* depth,
-                               size_t pitch, int32_t* index, cudaStream_t s);
+// The debug argmin over a float (half = 0) or __half (half = 1, shifted by offset) W*H*D volume.
+cudaError_t launch_case_argmin(const void* vol, int half, const float* offset, int W, int H, int D,
+                               const FilterParams& fp, float* depth, size_t pitch, int32_t* index, cudaStream_t s);
 cudaError_t launch_filter(const float* sum, int W, int H, int D, const FilterParams& fp,
                           const PlaneOrder& order, float* depth, size_t pitch, int32_t* index,
                           cudaStream_t s);
@@ -95,6 +104,9 @@ cudaError_t launch_to_float(int W, int H, const uint8_t* src, size_t src_pitch, 
 cudaError_t launch_to_half(int W, int H, const uint8_t* src, size_t src_pitch, void* dst, size_t dst_pitch,
                            float scale, cudaStream_t s);
 // uint8 -> quads of FP16-rounded values in FP32 lanes: the FP16 form's exact sampler.
+// uint8 -> FP16-rounded values in pitched float rows (the FP16 form's FP32-texel textures).
+cudaError_t launch_to_float_h_pitched(int W, int H, const uint8_t* src, size_t src_pitch, float* dst,
+                                     size_t dst_pitch, float scale, cudaStream_t s);
 cudaError_t launch_to_quad_half(int W, int H, const uint8_t* src, size_t src_pitch, float4* dst, float scale,
                                 cudaStream_t s);
 // uint8 -> scaled float image whose values are rounded to FP16 (the FP16 form's reference image).
@@ -102,6 +114,10 @@ cudaError_t launch_to_float_h(int W, int H, const uint8_t* src, size_t src_pitch
                               cudaStream_t s);
 cudaError_t launch_to_quad(int W, int H, const uint8_t* src, size_t src_pitch, float4* dst,
                            float scale, cudaStream_t s);
+// A pitched W x H source image (FP16 texels, or FP32 texels when f32) and its texture object:
+// linear filtering, zero border, unnormalised coordinates (the reference's texture setup,
+// calc_cost.cu:226-237).
+cudaError_t make_source_texture(int W, int H, bool f32, void** buf, size_t* pitch, unsigned long long* tex);
 cudaError_t launch_convert(int W, int H, const float* in, float* out, int flag, size_t pitch_bytes,
                            cudaStream_t s);
 

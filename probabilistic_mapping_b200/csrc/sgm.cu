@@ -367,6 +367,12 @@ __global__ void __launch_bounds__(256) combine_kernel(const SgmLaunch a) {
             else
                 o[j] = s4;
         }
+        if (a.offset) {   // every path carries the FP16 volume's per-pixel shift once
+            const float sh = __fmul_rn((float)NP, __ldg(a.offset + pix));
+#pragma unroll
+            for (int j = 0; j < PPL; ++j) o[j] = __fadd_rn(o[j], sh);
+        }
+
         if (a.total) store_planes<PPL>(a.total + (size_t)pix * D + lane * PPL, o);
         if constexpr (MODE != kCombineStore) {
             float depth;
@@ -411,17 +417,18 @@ __global__ void __launch_bounds__(128) filter_kernel(const float* __restrict__ s
 
 // CASE 0 of outputFusionCPU: the debug argmin straight on the plane-sweep cost volume.
 template <int PPL, bool HALF>
-__global__ void __launch_bounds__(128) case_kernel(const void* __restrict__ vol, int W, int H, int D,
-                                                   const FilterParams fp, float* depth, size_t pitch,
-                                                   int32_t* index) {
+__global__ void __launch_bounds__(128) case_kernel(const void* __restrict__ vol, const float* __restrict__ offset,
+                                                   int W, int H, int D, const FilterParams fp, float* depth,
+                                                   size_t pitch, int32_t* index) {
     const int lane = threadIdx.x & 31;
     const long pix = (long)blockIdx.x * 4 + (threadIdx.x >> 5);
     if (pix >= (long)W * H) return;
     float s[PPL];
     if constexpr (HALF) {
         const __half* p = static_cast<const __half*>(vol) + (size_t)pix * D + lane * PPL;
+        const float off = __ldg(offset + pix);
 #pragma unroll
-        for (int j = 0; j < PPL; ++j) s[j] = __half2float(p[j]);
+        for (int j = 0; j < PPL; ++j) s[j] = __fadd_rn(__half2float(p[j]), off);
     } else {
         load_planes<PPL>(s, static_cast<const float*>(vol) + (size_t)pix * D + lane * PPL);
     }
@@ -575,19 +582,20 @@ cudaError_t launch_filter(const float* sum, int W, int H, int D, const FilterPar
 }
 
 template <int PPL, bool HALF>
-cudaError_t launch_case_t(const void* vol, int W, int H, int D, const FilterParams& fp, float* depth, size_t pitch,
-                          int32_t* index, cudaStream_t s) {
+cudaError_t launch_case_t(const void* vol, const float* offset, int W, int H, int D, const FilterParams& fp,
+                          float* depth, size_t pitch, int32_t* index, cudaStream_t s) {
     const long n = (long)W * H;
-    case_kernel<PPL, HALF><<<(unsigned)((n + 3) / 4), 128, 0, s>>>(vol, W, H, D, fp, depth, pitch, index);
+    case_kernel<PPL, HALF><<<(unsigned)((n + 3) / 4), 128, 0, s>>>(vol, offset, W, H, D, fp, depth, pitch, index);
     return cudaGetLastError();
 }
 
-cudaError_t launch_case_argmin(const void* vol, int half, int W, int H, int D, const FilterParams& fp, float* depth,
-                               size_t pitch, int32_t* index, cudaStream_t s) {
+cudaError_t launch_case_argmin(const void* vol, int half, const float* offset, int W, int H, int D,
+                               const FilterParams& fp, float* depth, size_t pitch, int32_t* index, cudaStream_t s) {
+    if (half && !offset) return cudaErrorInvalidValue;
     switch (D / 32) {
 #define PM_CASE_PPL(P) \
-        case P: return half ? launch_case_t<P, true>(vol, W, H, D, fp, depth, pitch, index, s) \
-                            : launch_case_t<P, false>(vol, W, H, D, fp, depth, pitch, index, s);
+        case P: return half ? launch_case_t<P, true>(vol, offset, W, H, D, fp, depth, pitch, index, s) \
+                            : launch_case_t<P, false>(vol, offset, W, H, D, fp, depth, pitch, index, s);
         PM_CASE_PPL(1) PM_CASE_PPL(2) PM_CASE_PPL(3) PM_CASE_PPL(4)
         PM_CASE_PPL(5) PM_CASE_PPL(6) PM_CASE_PPL(7) PM_CASE_PPL(8)
 #undef PM_CASE_PPL

@@ -1,7 +1,7 @@
 """The batched form against separate StereoMapper runs.
 
-A batch of sequences with different shapes, precisions, path counts and cost modes (two of them
-sharing one lane of cost/path volumes) is stepped over several keyframes; after every step each
+A batch of sequences with different shapes, precisions, samplers, path counts and cost modes (two
+of them sharing one lane of cost/path volumes) is stepped over several keyframes; after every step each
 sequence's fused depth and variance must equal, bit for bit, what a StereoMapper fed the same
 frames and poses returns: the batch runs the same kernels, with the per-step values read from
 device memory instead of kernel parameters.
@@ -24,6 +24,7 @@ SEQS = [
     dict(width=128, height=96, num_planes=128, precision=1, cost_mode=1, num_paths=8),
     dict(width=96, height=64, num_planes=64, precision=0, cost_mode=0, num_paths=4),
     dict(width=96, height=64, num_planes=64, precision=0, cost_mode=0, num_paths=8),   # shares seq 0's lane
+    dict(width=128, height=96, num_planes=64, precision=1, cost_mode=0, num_paths=8, sampler=2),  # FP32 texels
 ]
 
 

@@ -2,7 +2,7 @@
 against the oracle: CASE 0 is the argmin of the plane-sweep cost, CASE 1 the argmin of the SGM
 sum, both bit-exact against oracle/imgproc.case_argmin on the FP32 oracle's volumes (the same op
 order as the kernels); CASE 2 is pm_output.  The FP16 form's CASE 0 is checked against the
-argmin of its own FP16 cost volume."""
+argmin of its own FP16 cost volume plus its per-pixel offsets."""
 import numpy as np
 import pytest
 
@@ -61,8 +61,13 @@ def test_case0_fp16_volume():
     b = m.buffers()
     vol = torch.empty(H * W * D, dtype=torch.float16, device="cuda")
     torch.cuda.synchronize()
+    off = torch.empty(H * W, dtype=torch.float32, device="cuda")
     err, = rt.cudaMemcpy(vol.data_ptr(), b.cost, vol.numel() * 2, rt.cudaMemcpyKind.cudaMemcpyDeviceToDevice)
     assert err == rt.cudaError_t.cudaSuccess
-    want, _ = oip.case_argmin(vol.float().cpu().numpy().reshape(H, W, D), rho0, drho)
+    err, = rt.cudaMemcpy(off.data_ptr(), b.cost_offset, off.numel() * 4, rt.cudaMemcpyKind.cudaMemcpyDeviceToDevice)
+    assert err == rt.cudaError_t.cudaSuccess
+    # the half volume holds cost - offset[pixel]; the kernel adds it back in FP32
+    full = vol.float().reshape(H * W, D) + off[:, None]
+    want, _ = oip.case_argmin(full.cpu().numpy().reshape(H, W, D), rho0, drho)
     assert (got.view(np.uint32) == want.view(np.uint32)).all()
     m.close()
