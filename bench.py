@@ -158,12 +158,13 @@ def algorithmic_bytes(e: int):
 FLOP_PER_VOXEL_SOURCE = 144
 
 
-def cost_kernel_work(e: int):
+def cost_kernel_work(e: int, texels: bool = False):
     """Algorithmic flop and bytes of one cost-kernel launch (all S sources folded at once): the
-    volume written once (e V), the reference image and the S source quads read once."""
+    volume written once (e V), the reference image and the S source images read once (16-byte
+    quads for the exact sampler, 4-byte texels for the texture sampler)."""
     N = W * H
     V = N * D
-    return FLOP_PER_VOXEL_SOURCE * V * S, e * V + 4 * N + 16 * N * S
+    return FLOP_PER_VOXEL_SOURCE * V * S, e * V + 4 * N + (4 if texels else 16) * N * S
 
 
 def run_ours(args, rank, world, precision: str = "fp32", passes=("dev", "e2e", "stage")):
@@ -523,14 +524,14 @@ def main():
     peak_hbm, sm_mhz, peak_kind = peaks()
     peak_fp32 = fp32_peak_tflops(sm_mhz)
     cost_ms, sgm_ms = float(stage_ms[0]), float(stage_ms[1])
-    cost_flop, cost_bytes = cost_kernel_work(e)
+    cost_flop, cost_bytes = cost_kernel_work(e, e == 2 and args.sampler != "exact")
     cost_tflops = cost_flop / (cost_ms / 1000.0) / 1e12 if cost_ms > 0 else None
     cost_gbs = cost_bytes / (cost_ms / 1000.0) / 1e9 if cost_ms > 0 else None
     sgm_gbs = sgm_bytes / (sgm_ms / 1000.0) / 1e9 if sgm_ms > 0 else None
     map_s = 1.0 / (value / world)   # seconds per map per GPU
-    # to_float (reference) + to_quad (S sources), cost, one kernel per opposite-path pair,
-    # combine + winner-take-all, fusion transform + update
-    launches_per_map = 1 + S + 1 + PATHS // 2 + 1 + 2
+    # to_float (reference) + one conversion per source, cost (+ the FP16 volume's rebase), one
+    # kernel per opposite-path pair, combine + winner-take-all, fusion transform + update
+    launches_per_map = 1 + S + 1 + (1 if e == 2 else 0) + PATHS // 2 + 1 + 2
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "depth maps/s", "n_gpus": world, "steps": args.steps,
@@ -547,9 +548,12 @@ def main():
                            "unit": "depth maps/s"},
             "speedup_vs_plain_fp32": value / plain_value,
             # the dominant kernel (cost_kernel, ~2/3 of a map) is FP32-ALU-bound, not HBM-bound
-            "roofline": {"bound": "fp32", "kernel": "cost_kernel", "achieved": cost_tflops, "peak": peak_fp32,
+            "roofline": {"bound": "fp32", "kernel": "cost_kernel" + (" (stage time includes the FP16 rebase pass)"
+                                                                    if e == 2 else ""),
+                         "achieved": cost_tflops, "peak": peak_fp32,
                          "unit": "TFLOP/s", "frac": (cost_tflops / peak_fp32) if cost_tflops else None,
-                         "traffic": ncu_traffic("cost_kernel") if e == 4 else None, "ms_per_launch": cost_ms,
+                         "traffic": ncu_traffic("cost_kernel" if e == 4 else "cost_kernel_fp16"),
+                         "ms_per_launch": cost_ms,
                          "algorithmic_flop_per_launch": cost_flop, "algorithmic_bytes_per_launch": cost_bytes,
                          "hbm_achieved_gbs": cost_gbs, "hbm_frac": (cost_gbs / peak_hbm) if cost_gbs else None,
                          "precision": args.precision,
