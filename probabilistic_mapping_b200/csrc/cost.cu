@@ -181,9 +181,24 @@ __device__ __forceinline__ Hom load_hom(const CostLaunch& a, int s) {
 // exhaustive check of pm_debug_check_arith); outside that the pair takes IEEE division.  A pass
 // that starts from initReference (INC false) folds at most kMaxSources sources, so its divisors
 // never exceed 33 and only the dividends are tested.
-template <bool INC>
+//
+// The FP16 form (APPROX) stores the result in FP16, so it folds with one multiply by RN(1/9)
+// and the hardware reciprocal estimate of cnt+1 (relative error ~1e-7, far below FP16's
+// 4.9e-4) instead of the correctly rounded divisions.
+template <bool INC, bool APPROX>
 __device__ __forceinline__ void fold2(float2& acc, float2& cn, float2 tmp, float r9) {
     const float2 r9p = f2(r9, r9);
+    if constexpr (APPROX) {
+        const float2 n1 = __fadd2_rn(cn, f2(1.0f, 1.0f));
+        float2 r;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r.x) : "f"(n1.x));
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r.y) : "f"(n1.y));
+        const float2 q = __fmul2_rn(__ffma2_rn(cn, acc, __fmul2_rn(tmp, r9p)), r);
+        const bool v0 = tmp.x == tmp.x, v1 = tmp.y == tmp.y;
+        acc = f2(v0 ? q.x : acc.x, v1 ? q.y : acc.y);
+        cn = f2(v0 ? n1.x : cn.x, v1 ? n1.y : cn.y);
+        return;
+    }
     const float2 n1 = __fadd2_rn(cn, f2(1.0f, 1.0f));
     const float2 nn1 = __ffma2_rn(cn, f2(-1.0f, -1.0f), f2(-1.0f, -1.0f));   // -(cnt + 1), exact
     const float2 q0 = __fmul2_rn(tmp, r9p);
@@ -326,7 +341,7 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
                 float2* const ap = accp + o * (TXU * SP / 2);
                 float2* const cp = cntp + o * (TXU * SP / 2);
                 float2 av = *ap, nv = *cp;
-                fold2<INC>(av, nv, f2(tx, ty), r9);
+                fold2<INC, HALF>(av, nv, f2(tx, ty), r9);
                 *ap = av;
                 *cp = nv;
             }
