@@ -36,12 +36,12 @@ def make_configs():
     return out
 
 
-@pytest.mark.parametrize("host_io,autotune", [(True, False), (False, True)])
-def test_batch_matches_separate_mappers(host_io, autotune):
+@pytest.mark.parametrize("host_io,autotune,priority", [(True, False, False), (False, True, True)])
+def test_batch_matches_separate_mappers(host_io, autotune, priority):
     cfgs = make_configs()
     seqs = [scene.make_sequence(c["width"], c["height"], 0.8 * c["width"], S, 3, seed=50 + i)
             for i, c in enumerate(cfgs)]
-    b = StereoBatch(cfgs, S, lanes=1, host_io=host_io, autotune=autotune)
+    b = StereoBatch(cfgs, S, lanes=1, host_io=host_io, autotune=autotune, priority=priority)
     mappers = []
     for i, c in enumerate(cfgs):
         W, H, D = c["width"], c["height"], c["num_planes"]
