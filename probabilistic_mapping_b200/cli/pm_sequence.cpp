@@ -176,7 +176,8 @@ std::string json_str(const std::string& s) {
 struct Args {
     std::string images, poses, root, out = ".", format = "pfm";
     int planes = 64, paths = 4, downsample = 0, agg = 3, interval = 6, out_case = 0, device = 0;
-    int precision = PM_PREC_FP32, cost_mode = PM_COST_REFERENCE, color = 0, dry = 0, limit = -1;
+    int precision = PM_PREC_FP32, cost_mode = PM_COST_REFERENCE, sampler = PM_SAMPLER_EXACT, color = 0, dry = 0;
+    int limit = -1;
     double fx = 481.2017, fy = -480.0002, cx = 319.5, cy = 239.5;   // ICL-NUIM (evaluate.cc:36-39)
     double min_depth = 0.2, max_depth = 20.0, associate = -1.0;     // evaluate.cc:27-28
 };
@@ -187,7 +188,8 @@ void usage() {
                  "  [--case N (0 raw-cost argmin, 1 SGM argmin, 2 filtered depth, >=3 fused; default 0)]\n"
                  "  [--planes 64] [--paths 4|8] [--fx F --fy F --cx F --cy F] [--downsample 0]\n"
                  "  [--agg 3] [--interval 6] [--min-depth 0.2] [--max-depth 20] [--format pfm|npy]\n"
-                 "  [--color] [--precision fp32|fp16] [--cost reference|corrected] [--associate SECONDS]\n"
+                 "  [--color] [--precision fp32|fp16] [--sampler exact|texture|texture_f32 (fp16)]\n"
+                 "  [--cost reference|corrected] [--associate SECONDS]\n"
                  "  [--limit N] [--device 0] [--dry-run]\n");
 }
 
@@ -221,6 +223,13 @@ bool parse_args(int argc, char** argv, Args& a) {
         else if (k == "--associate") a.associate = std::atof(v);
         else if (k == "--precision") a.precision = std::string(v) == "fp16" ? PM_PREC_FP16 : PM_PREC_FP32;
         else if (k == "--cost") a.cost_mode = std::string(v) == "corrected" ? PM_COST_CORRECTED : PM_COST_REFERENCE;
+        else if (k == "--sampler") {
+            const std::string m = v;
+            if (m == "exact") a.sampler = PM_SAMPLER_EXACT;
+            else if (m == "texture") a.sampler = PM_SAMPLER_TEXTURE;
+            else if (m == "texture_f32") a.sampler = PM_SAMPLER_TEXTURE_F32;
+            else return false;
+        }
         else return false;
     }
     return !a.images.empty() && !a.poses.empty() && a.agg > 0 && a.interval > 0 && a.downsample >= 0 &&
@@ -404,6 +413,7 @@ int main(int argc, char** argv) {
             pm_config_default(&c, W, H, a.planes);
             c.num_paths = a.paths;
             c.precision = a.precision;
+            c.sampler = a.precision == PM_PREC_FP16 ? a.sampler : PM_SAMPLER_EXACT;
             c.cost_mode = a.cost_mode;
             c.fusion_variant = PM_FUSION_CPU_PATH;   // outputFusionCPU (evaluate.cc:260)
             c.device = a.device;

@@ -100,6 +100,34 @@ def test_driver_matches_python_loop(stream, tmp_path, case, downsample):
     assert nonzero > 0
 
 
+def test_driver_fp16_texture(stream, tmp_path):
+    """The FP16 form with the texture sampler through the driver: same files as the Python loop
+    with the same configuration."""
+    os.makedirs(str(tmp_path), exist_ok=True)
+    sequence.run(stream["il"], stream["pl"], str(tmp_path), root=stream["root"], case=3, fx=repr(F), fy=repr(F),
+                 cx=repr(W / 2.0), cy=repr(H / 2.0), precision="fp16", sampler="texture_f32")
+    kfs, _ = oseq.schedule(stream["images"], [(p[0],) for p in stream["poses"]])
+    K = np.array([[F, 0, W / 2.0], [0, F, H / 2.0], [0, 0, 1.0]])
+    m = StereoMapper(W, H, 64, fusion_variant=_lib.PM_FUSION_CPU_PATH, max_sources=3,
+                     precision=_lib.PM_PREC_FP16, sampler=_lib.PM_SAMPLER_TEXTURE_F32)
+    m.initIntrinsic(K, 0.02 * F, np.float32(1.0 / (0.15 * 160.0)))
+
+    def pose(i):
+        p = [float(v) for v in stream["poses"][i][1:]]
+        return sequence.quat_to_rot(p[3], p[4], p[5], p[6]), np.array(p[:3])
+
+    for ref, rp, src in kfs:
+        Rl, Tl = pose(rp)
+        m.initReference(stream["imgs"][ref])
+        for s, sp in src:
+            Rr, Tr = pose(sp)
+            m.update(stream["imgs"][s], Rl, Tl, Rr, Tr)
+        d, _ = m.outputFusion(Rl, Tl, F, F, W / 2.0, H / 2.0, want_variance=False)
+        got = sequence.read_pfm(os.path.join(str(tmp_path), f"depth_{stream['images'][ref][0]}.pfm"))
+        assert (got.view(np.uint32) == d.view(np.uint32)).all()
+    m.close()
+
+
 def test_driver_npy_output(stream, tmp_path):
     cli_run(stream, str(tmp_path), 2, 0, fmt="npy", color=False)
     want = python_run(stream, 2)
