@@ -410,28 +410,48 @@ __global__ void __launch_bounds__(256) invalid_kernel(const void* cost, long npi
 }
 
 // Moves every 16-plane block of a pixel from its own offset to the pixel's: the smallest block
-// offset, or 0 when some plane is unmeasured (negative).  One warp per pixel, lane l holding
-// planes [l*PPL, (l+1)*PPL), rewritten in place.
+// offset, or 0 when some plane is unmeasured (negative).  One warp per RB consecutive pixels, lane
+// l holding planes [l*PPL, (l+1)*PPL) of each as PPL/2 half pairs, rewritten in place; all RB
+// pixels are loaded before any is reduced, to keep more bytes in flight.
+constexpr int RB = 4;
+
 template <int PPL>
-__global__ void __launch_bounds__(256) rebase_kernel(__half* __restrict__ cost, const float* __restrict__ boff,
+__global__ void __launch_bounds__(256) rebase_kernel(__half2* __restrict__ cost, const float* __restrict__ boff,
                                                      float* __restrict__ off, long npix, int D) {
-    const long pix = (long)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const long pix0 = ((long)blockIdx.x * 8 + (threadIdx.x >> 5)) * RB;
     const int lane = threadIdx.x & 31;
-    if (pix >= npix) return;
     const int nb = D >> 4;
-    const float* bo = boff + (size_t)pix * nb;
-    __half* c = cost + (size_t)pix * D + lane * PPL;
-    float v[PPL];
-    bool neg = false;
+    __half2 h[RB][PPL / 2];
+    float bl[RB];
 #pragma unroll
-    for (int j = 0; j < PPL; ++j) {
-        v[j] = __half2float(c[j]);
-        neg |= v[j] < 0.0f;
+    for (int r = 0; r < RB; ++r) {
+        const long pix = pix0 + r < npix ? pix0 + r : npix - 1;   // a repeated last pixel is rewritten identically
+        const __half2* c = cost + ((size_t)pix * D + lane * PPL) / 2;
+#pragma unroll
+        for (int j = 0; j < PPL / 2; ++j) h[r][j] = c[j];
+        bl[r] = lane < nb ? __ldg(boff + (size_t)pix * nb + lane) : inf_f();
     }
-    const float g = __any_sync(kFull, neg) ? 0.0f : warp_min_f32(lane < nb ? __ldg(bo + lane) : inf_f());
 #pragma unroll
-    for (int j = 0; j < PPL; ++j) c[j] = __float2half_rn(__fadd_rn(v[j], __fsub_rn(__ldg(bo + ((lane * PPL + j) >> 4)), g)));
-    if (lane == 0) off[pix] = g;
+    for (int r = 0; r < RB; ++r) {
+        if (pix0 + r >= npix) break;   // warp-uniform
+        const long pix = pix0 + r;
+        bool neg = false;
+#pragma unroll
+        for (int j = 0; j < PPL / 2; ++j) {
+            const float2 v = __half22float2(h[r][j]);
+            neg |= v.x < 0.0f || v.y < 0.0f;
+        }
+        const float g = __any_sync(kFull, neg) ? 0.0f : warp_min_f32(bl[r]);
+        __half2* c = cost + ((size_t)pix * D + lane * PPL) / 2;
+#pragma unroll
+        for (int j = 0; j < PPL / 2; ++j) {
+            const float2 v = __half22float2(h[r][j]);
+            const float s0 = __fsub_rn(__shfl_sync(kFull, bl[r], (lane * PPL + 2 * j) >> 4), g);
+            const float s1 = __fsub_rn(__shfl_sync(kFull, bl[r], (lane * PPL + 2 * j + 1) >> 4), g);
+            c[j] = __floats2half2_rn(__fadd_rn(v.x, s0), __fadd_rn(v.y, s1));
+        }
+        if (lane == 0) off[pix] = g;
+    }
 }
 
 template <int MODE, bool HALF, int SAMP>
@@ -469,8 +489,8 @@ cudaError_t launch_cost(const CostLaunch& a, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     if (a.cost_half) {
         const long np = (long)a.W * a.H;
-        const unsigned blocks = (unsigned)((np + 7) / 8);
-        __half* c = static_cast<__half*>(a.cost);
+        const unsigned blocks = (unsigned)((np + 8 * RB - 1) / (8 * RB));
+        __half2* c = static_cast<__half2*>(a.cost);
         switch (a.D / 32) {
             case 2: rebase_kernel<2><<<blocks, 256, 0, s>>>(c, a.block_offset, a.offset, np, a.D); break;
             case 4: rebase_kernel<4><<<blocks, 256, 0, s>>>(c, a.block_offset, a.offset, np, a.D); break;
