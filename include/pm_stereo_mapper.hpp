@@ -53,6 +53,15 @@ public:
         check(pm_output_fusion(h_, depth, depth_pitch, variance, variance_pitch, R, t, fx, fy, cx, cy),
               "outputFusion");
     }
+    // StereoMapper::outputFusionCPU (stereo_mapper.cpp:625-820): with CASE >= 3 the fused map of a
+    // mapper created with fusion_variant = PM_FUSION_CPU_PATH, else the CASE 0/1/2 debug output.
+    void outputFusionCPU(float* depth, size_t depth_pitch, const double R[9], const double t[3], float fx,
+                         float fy, float cx, float cy, int output_case = 3) {
+        if (output_case >= 3)
+            check(pm_output_fusion(h_, depth, depth_pitch, nullptr, 0, R, t, fx, fy, cx, cy), "outputFusionCPU");
+        else
+            check(pm_output_case(h_, output_case, depth, depth_pitch), "outputFusionCPU");
+    }
     void wtaDepth(float* depth, size_t pitch_bytes) { check(pm_get_wta_depth(h_, depth, pitch_bytes), "wtaDepth"); }
     void setStream(void* cuda_stream) { check(pm_set_stream(h_, cuda_stream), "setStream"); }
     void synchronize() { check(pm_synchronize(h_), "synchronize"); }

@@ -71,7 +71,7 @@ struct SgmLaunch {
     size_t depth_pitch;
     int32_t* index;        // W*H (optional)
     PlaneOrder order;
-    int pair_warps;        // scanlines per block of the path-pair kernel: 2, 4 or 8 (0: 4)
+    int pair_warps;        // scanlines per block of the path-pair kernel: 2, 4 or 8 (0: 2)
     int serial_pairs;      // 1: run the path pairs one after another on the caller's stream
     int priority;          // launch priority of the pair and combine kernels (0: the stream's)
 };

@@ -482,13 +482,15 @@ cudaError_t launch_pair_nw(const SgmLaunch& a, int pair, cudaStream_t s) {
                                 2 * pair);
 }
 
-// scanlines (warps) per block: a.pair_warps in {2, 4, 8}, 4 when unset
+// scanlines (warps) per block: a.pair_warps in {2, 4, 8}, 2 when unset (the batched form's
+// autotuner picks 2 for the 640x480x128 map too: smaller blocks spread one map's few scanlines
+// over more SMs)
 template <int PPL, bool HALF>
 cudaError_t launch_pair(const SgmLaunch& a, int pair, cudaStream_t s) {
     switch (a.pair_warps) {
-        case 2: return launch_pair_nw<PPL, HALF, 2>(a, pair, s);
+        case 4: return launch_pair_nw<PPL, HALF, 4>(a, pair, s);
         case 8: return launch_pair_nw<PPL, HALF, 8>(a, pair, s);
-        default: return launch_pair_nw<PPL, HALF, 4>(a, pair, s);
+        default: return launch_pair_nw<PPL, HALF, 2>(a, pair, s);
     }
 }
 

@@ -43,6 +43,13 @@ int main(int argc, char** argv) {
                 std::printf("non-finite depth\n");
                 return 1;
             }
+        // the CASE 2 debug output of outputFusionCPU is the filtered depth itself
+        std::vector<float> case2(W * H);
+        m.outputFusionCPU(case2.data(), W * sizeof(float), I, T0, 50, 50, 32, 24, 2);
+        if (std::memcmp(case2.data(), depth.data(), depth.size() * sizeof(float)) != 0) {
+            std::printf("CASE 2 differs from output\n");
+            return 1;
+        }
     }
     std::printf("ok\n");
     return 0;
