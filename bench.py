@@ -147,9 +147,11 @@ def algorithmic_bytes(e: int):
     N = W * H
     V = N * D
     b_alg = (S + 1) * N + 3 * e * V + 8 * V + 60 * N
-    # every path reads C and the reference image and writes its FP32 path volume; the combine
-    # reads the path volumes and writes depth and index
-    sgm_pass = PATHS * (e * V + 4 * V + 4 * N) + PATHS * 4 * V + 8 * N
+    # every path reads C and the reference image; each opposite-path pair stores one FP32 volume
+    # and adds into it once (a read and a write); the combine reads the pair volumes and writes
+    # depth and index
+    pairs = PATHS // 2
+    sgm_pass = PATHS * (e * V + 4 * N) + pairs * (4 * V + 8 * V) + pairs * 4 * V + 8 * N
     return b_alg, sgm_pass
 
 

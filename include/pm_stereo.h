@@ -291,10 +291,11 @@ PM_API pm_status pm_stage_calc_cost(const pm_config* cfg, const float* ref, cons
                              const float* homs, float* cost, float* cnt, uint8_t* invalid,
                              void* stream);
 
-/* sgm2 (sgm.cu:115-135): out := sum over cfg->num_paths paths; out needs no clearing.  Each
- * path is aggregated into its own volume (out holds path 0, scratch the other num_paths - 1:
- * (num_paths - 1)*W*H*D floats), opposite paths pairwise in one kernel, and the volumes are
- * added as (P0 + P1) + (P2 + P3) [+ ((P4 + P5) + (P6 + P7))], paths in the reference's order. */
+/* sgm2 (sgm.cu:115-135): out := sum over cfg->num_paths paths; out needs no clearing.  Opposite
+ * paths run pairwise in one kernel and each pair is aggregated into its own volume (out holds
+ * pair 0, scratch the other num_paths/2 - 1: (num_paths/2 - 1)*W*H*D floats; a larger scratch,
+ * such as the num_paths - 1 volumes earlier versions used, is fine), and the sum is
+ * (P0 + P1) + (P2 + P3) [+ ((P4 + P5) + (P6 + P7))], paths in the reference's order. */
 PM_API pm_status pm_stage_sgm(const pm_config* cfg, const float* cost, const float* ref, float* out,
                        float* scratch, void* stream);
 
@@ -302,8 +303,8 @@ PM_API pm_status pm_stage_sgm(const pm_config* cfg, const float* cost, const flo
 PM_API pm_status pm_stage_filter(const pm_config* cfg, const float* sgm, float* depth, size_t pitch_bytes,
                           int32_t* index, void* stream);
 
-/* sgm2 + filter_cost fused: the combine kernel adds the path volumes in registers and runs the
- * winner-take-all; `scratch` holds the num_paths path volumes (num_paths*W*H*D floats). */
+/* sgm2 + filter_cost fused: the combine kernel adds the pair volumes in registers and runs the
+ * winner-take-all; `scratch` holds the num_paths/2 pair volumes ((num_paths/2)*W*H*D floats). */
 PM_API pm_status pm_stage_sgm_filter(const pm_config* cfg, const float* cost, const float* ref,
                               float* scratch, float* depth, size_t pitch_bytes, int32_t* index,
                               void* stream);

@@ -44,7 +44,7 @@ struct pm_mapper {
     float* d_off = nullptr;     // FP16 form: per-pixel shift of the half volume (W*H)
     float* d_boff = nullptr;    // FP16 form: block offsets before the rebase (W*H*D/16)
     float* d_cnt = nullptr;     // allocated on the first fold
-    float* d_part[8] = {};      // SGM: one volume per path (num_paths of them)
+    float* d_part[4] = {};      // SGM: one volume per opposite-path pair (num_paths / 2 of them)
     SgmStreams side{};          // concurrent path groups
     bool have_side = false;
     float* d_depth = nullptr;   // WTA depth, linear
@@ -303,7 +303,7 @@ pm_status run_sgm_filter(pm_mapper* h) {
     a.cost = h->d_cost;
     a.offset = h->d_off;
     a.ref = h->d_ref;
-    for (int r = 0; r < c.num_paths; ++r) a.part[r] = h->d_part[r];
+    for (int r = 0; r < c.num_paths / 2; ++r) a.part[r] = h->d_part[r];
     a.total = h->store_sgm ? h->d_part[0] : nullptr;   // combine reads part[0] of a pixel before writing it
     a.depth = h->d_depth;
     a.depth_pitch = sizeof(float) * (size_t)c.width;
@@ -440,7 +440,7 @@ pm_status pm_create(const pm_config* cfg, pm_mapper** out) {
     for (int s = 0; half && cfg->sampler != PM_SAMPLER_EXACT && s < cfg->max_sources && ok; ++s)
         ok = note(make_source_texture(cfg->width, cfg->height, cfg->sampler == PM_SAMPLER_TEXTURE_F32, &h->d_srch[s],
                                       &h->srch_pitch, &h->tex[s]));
-    for (int r = 0; r < cfg->num_paths && ok; ++r) ok = alloc((void**)&h->d_part[r], 4 * V);
+    for (int r = 0; r < cfg->num_paths / 2 && ok; ++r) ok = alloc((void**)&h->d_part[r], 4 * V);
     if (ok && cfg->fusion_variant == PM_FUSION_CPU_PATH) {
         if (cfg->width >= 65536 || cfg->height >= 65536) ok = note(cudaErrorInvalidValue);
         ok = ok && alloc((void**)&h->d_cmask, N) && alloc((void**)&h->d_corig, 4 * N) &&
@@ -579,7 +579,7 @@ pm_status pm_output_case(pm_mapper* h, int output_case, float* result, size_t pi
         a.cost = h->d_cost;
         a.offset = h->d_off;
         a.ref = h->d_ref;
-        for (int r = 0; r < c.num_paths; ++r) a.part[r] = h->d_part[r];
+        for (int r = 0; r < c.num_paths / 2; ++r) a.part[r] = h->d_part[r];
         a.depth = h->d_fused;
         a.depth_pitch = sizeof(float) * (size_t)c.width;
         a.index = h->d_idx;
@@ -829,7 +829,7 @@ pm_status pm_stage_sgm(const pm_config* cfg, const float* cost, const float* ref
     a.ref = ref;
     const size_t V = (size_t)cfg->width * cfg->height * cfg->num_planes;
     a.part[0] = out;   // the combine kernel reads part[0] of a pixel before it writes the total there
-    for (int r = 1; r < cfg->num_paths; ++r) a.part[r] = scratch + (r - 1) * V;
+    for (int r = 1; r < cfg->num_paths / 2; ++r) a.part[r] = scratch + (r - 1) * V;
     a.total = out;
     return launch_sgm(a, kCombineStore, (cudaStream_t)stream, nullptr) == cudaSuccess ? PM_OK : PM_ERR_CUDA;
 }
@@ -861,7 +861,7 @@ pm_status pm_stage_sgm_filter(const pm_config* cfg, const float* cost, const flo
     a.cost = cost;
     a.ref = ref;
     const size_t V = (size_t)cfg->width * cfg->height * cfg->num_planes;
-    for (int r = 0; r < cfg->num_paths; ++r) a.part[r] = scratch + r * V;
+    for (int r = 0; r < cfg->num_paths / 2; ++r) a.part[r] = scratch + r * V;
     a.total = nullptr;
     a.depth = depth;
     a.depth_pitch = pitch;

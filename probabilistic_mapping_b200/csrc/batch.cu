@@ -43,7 +43,7 @@ struct LaneBufs {
     void* cost = nullptr;
     float* off = nullptr;    // FP16 volumes: the per-pixel shift (see CostLaunch::offset)
     float* boff = nullptr;   // FP16 volumes: block offsets before the rebase
-    float* part[8] = {};
+    float* part[4] = {};
     int last_user = -1;   // sequence index that used this set last in the capture order
 };
 
@@ -203,7 +203,7 @@ SgmLaunch sgm_launch(const Seq& q, const LaneBufs& l, int priority) {
     a.offset = l.off;
     a.cost_half = c.precision == PM_PREC_FP16;
     a.ref = q.d_ref;
-    for (int r = 0; r < c.num_paths; ++r) a.part[r] = l.part[r];
+    for (int r = 0; r < c.num_paths / 2; ++r) a.part[r] = l.part[r];
     a.W = c.width;
     a.H = c.height;
     a.D = c.num_planes;
@@ -443,7 +443,7 @@ pm_status pm_batch_create(const pm_config* cfgs, int n, int num_sources, int lan
             if (ok && esz == 2)
                 ok = alloc((void**)&l.off, 4 * q.N) && note(cudaMemset(l.off, 0, 4 * q.N)) &&
                      alloc((void**)&l.boff, 4 * q.N * (q.cfg.num_planes / 16));
-            for (int r = 0; r < q.cfg.num_paths && ok; ++r) ok = alloc((void**)&l.part[r], 4 * q.V);
+            for (int r = 0; r < q.cfg.num_paths / 2 && ok; ++r) ok = alloc((void**)&l.part[r], 4 * q.V);
             b->lanes.push_back(l);
             if (!ok) break;
         }

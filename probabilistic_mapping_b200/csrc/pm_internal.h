@@ -61,7 +61,7 @@ struct SgmLaunch {
     const void* cost;      // W*H*D float or __half
     int cost_half;
     const float* ref;      // W*H scaled reference image (path gradient D1, sgm.cu:75)
-    float* part[8];        // W*H*D volume of each path (num_paths of them), reference path order
+    float* part[4];        // W*H*D volume of each opposite-path pair (num_paths / 2 of them): P_2p + P_2p+1
     float* total;          // W*H*D complete sum (may alias part[0]); nullptr: not stored
     const float* offset;   // W*H per-pixel shift of an FP16 cost volume (see CostLaunch), or nullptr
     int W, H, D, num_paths;
@@ -84,9 +84,9 @@ struct SgmStreams {
 };
 // What the combine kernel does with the summed path volumes.
 enum CombineMode { kCombineStore = 0, kCombineFilter = 1, kCombineArgmin = 2 };
-// Runs the opposite-path pairs (each path into part[r]), then adds the path volumes pairwise in
-// registers and writes depth/index with the winner-take-all filter (kCombineFilter) or the debug
-// argmin (kCombineArgmin); kCombineStore only writes `total`.  side == nullptr runs everything on s.
+// Runs the opposite-path pairs (pair p into part[p]), then adds the pair volumes in registers
+// and writes depth/index with the winner-take-all filter (kCombineFilter) or the debug argmin
+// (kCombineArgmin); kCombineStore only writes `total`.  side == nullptr runs everything on s.
 cudaError_t launch_sgm(const SgmLaunch& a, int mode, cudaStream_t s, const SgmStreams* side);
 // The debug argmin over a float (half = 0) or __half (half = 1, shifted by offset) W*H*D volume.
 cudaError_t launch_case_argmin(const void* vol, int half, const float* offset, int W, int H, int D,

@@ -11,13 +11,16 @@
 //     cp.async into a per-lane shared-memory ring PF steps ahead of the recurrence;
 //   * opposite paths run as pairs: one warp walks a scanline from both ends at once, so it keeps
 //     two independent recurrences in flight; the pairs (L/R, T/B and the two diagonals) run
-//     concurrently on separate streams, and every path writes its own volume (no
-//     read-modify-write between passes);
-//   * a pixel-parallel combine kernel (one warp per pixel, full occupancy) adds the path volumes
-//     pairwise, (P0 + P1) + (P2 + P3) [+ ((P4 + P5) + (P6 + P7))], in registers and runs the
+//     concurrently on separate streams.  Each pair owns one volume: the path that reaches a pixel
+//     first stores its values there and the other adds its own with a vector reduction, so the
+//     volume ends up holding P_2p + P_2p+1 (float addition is commutative, so this is the same
+//     sum in either order);
+//   * a pixel-parallel combine kernel (one warp per pixel, full occupancy) adds the pair volumes,
+//     (P0 + P1) + (P2 + P3) [+ ((P4 + P5) + (P6 + P7))], in registers and runs the
 //     winner-take-all directly, so the complete sum need not be written.  The FP32 result
 //     therefore differs from the reference's sequential path order only by rounding; the CPU
-//     oracle replays this exact order.
+//     oracle replays this exact order.  (The reduction unit flushes subnormal sums to zero; path
+//     values are costs plus penalties, never below 2^-126 unless exactly 0.)
 #include <climits>
 #include <vector>
 
@@ -215,6 +218,24 @@ __device__ __forceinline__ void load_slice(float (&cv)[PPL], const unsigned char
     }
 }
 
+// Adds v to p[0..PPL) in global memory with vector float reductions (no result returned).
+template <int PPL> __device__ __forceinline__ void red_planes(float* p, const float (&v)[PPL]) {
+    if constexpr (PPL % 4 == 0) {
+#pragma unroll
+        for (int j = 0; j < PPL; j += 4)
+            asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p + j), "f"(v[j]), "f"(v[j + 1]),
+                         "f"(v[j + 2]), "f"(v[j + 3])
+                         : "memory");
+    } else if constexpr (PPL % 2 == 0) {
+#pragma unroll
+        for (int j = 0; j < PPL; j += 2)
+            asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p + j), "f"(v[j]), "f"(v[j + 1]) : "memory");
+    } else {
+#pragma unroll
+        for (int j = 0; j < PPL; ++j) asm volatile("red.global.add.f32 [%0], %1;" ::"l"(p + j), "f"(v[j]) : "memory");
+    }
+}
+
 // Recurrence state of one path along one scanline.
 template <int PPL> struct PathState {
     float L[PPL];
@@ -268,9 +289,11 @@ __device__ __forceinline__ void path_step(const SgmLaunch& a, PathState<PPL>& s,
 }
 
 // A pair of opposite paths along the same scanlines: warp c takes scanline c of direction
-// (dx, dy) and walks it from both ends at once, the forward path into part[slot] and the
-// backward one into part[slot + 1].  The two recurrences are independent, so each warp keeps two
-// dependency chains in flight.  The cost slices and reference pixels of both ends are streamed
+// (dx, dy) and walks it from both ends at once into the pair's volume part[slot / 2]: while the
+// two ends have not met, each stores its pixel's path values; after they have, each adds its
+// values to what the other end stored there; at the meeting pixel of an odd chain the two are
+// added in registers.  The two recurrences are independent, so each warp keeps two dependency
+// chains in flight.  The cost slices and reference pixels of both ends are streamed
 // PF steps ahead with cp.async into a per-warp shared ring.
 template <int PPL, bool HALF, int NW>
 __global__ void __launch_bounds__(NW * 32) sgm_pair_kernel(const SgmLaunch a, int dx, int dy, int slot) {
@@ -290,8 +313,7 @@ __global__ void __launch_bounds__(NW * 32) sgm_pair_kernel(const SgmLaunch a, in
 
     unsigned char* const wbase = ring + (size_t)warp * PF * STAGE_B;
     const CT* __restrict__ cost = reinterpret_cast<const CT*>(a.cost);
-    float* const outf = a.part[slot];
-    float* const outb = a.part[slot + 1];
+    float* const out = a.part[slot >> 1];
 
     auto issue = [&](unsigned char* sb, int k) {
         const long qf = pf0 + k * step, qb = pb0 - k * step;
@@ -325,8 +347,20 @@ __global__ void __launch_bounds__(NW * 32) sgm_pair_kernel(const SgmLaunch a, in
         float of[PPL], ob[PPL];
         path_step<PPL>(a, fs, cf, If, k == 0, incl, lane, of);
         path_step<PPL>(a, bs, cb, Ib, k == 0, incl, lane, ob);
-        store_planes<PPL>(outf + (size_t)(pf0 + k * step) * D + lane * PPL, of);
-        store_planes<PPL>(outb + (size_t)(pb0 - k * step) * D + lane * PPL, ob);
+        float* const qf = out + (size_t)(pf0 + k * step) * D + lane * PPL;
+        float* const qb = out + (size_t)(pb0 - k * step) * D + lane * PPL;
+        const int other = ch.n - 1 - k;   // the step at which the other end visits this pixel
+        if (k < other) {                  // first visits (warp-uniform)
+            store_planes<PPL>(qf, of);
+            store_planes<PPL>(qb, ob);
+        } else if (k > other) {           // second visits: the first ones were this thread's stores
+            red_planes<PPL>(qf, of);
+            red_planes<PPL>(qb, ob);
+        } else {                          // both ends on the same pixel
+#pragma unroll
+            for (int j = 0; j < PPL; ++j) of[j] = __fadd_rn(of[j], ob[j]);
+            store_planes<PPL>(qf, of);
+        }
         // refill this stage (consumed above) with step k + PF
         if (k + PF < ch.n) issue(sb, k + PF);
         cp_async_commit();
@@ -335,10 +369,10 @@ __global__ void __launch_bounds__(NW * 32) sgm_pair_kernel(const SgmLaunch a, in
     cp_async_wait<0>();
 }
 
-// Sum of the path volumes in the pairwise order (P0 + P1) + (P2 + P3) [+ ((P4 + P5) + (P6 + P7))],
-// then the winner-take-all filter (MODE kCombineFilter), the debug argmin (kCombineArgmin) or
-// only a store of the sum (kCombineStore).  One warp per pixel, grid-stride; the next pixel's
-// path slices are loaded before the current one is reduced.
+// Sum of the NP pair volumes (each P_2p + P_2p+1) in the order (P0 + P1) + (P2 + P3)
+// [+ ((P4 + P5) + (P6 + P7))], then the winner-take-all filter (MODE kCombineFilter), the debug
+// argmin (kCombineArgmin) or only a store of the sum (kCombineStore).  One warp per pixel,
+// grid-stride; the next pixel's slices are loaded before the current one is reduced.
 template <int PPL, int MODE, int NP>
 __global__ void __launch_bounds__(256) combine_kernel(const SgmLaunch a) {
     const int lane = threadIdx.x & 31;
@@ -361,14 +395,13 @@ __global__ void __launch_bounds__(256) combine_kernel(const SgmLaunch a) {
         float o[PPL];
 #pragma unroll
         for (int j = 0; j < PPL; ++j) {
-            const float s4 = __fadd_rn(__fadd_rn(cur[0][j], cur[1][j]), __fadd_rn(cur[2][j], cur[3][j]));
-            if constexpr (NP == 8)
-                o[j] = __fadd_rn(s4, __fadd_rn(__fadd_rn(cur[4][j], cur[5][j]), __fadd_rn(cur[6][j], cur[7][j])));
+            if constexpr (NP == 4)
+                o[j] = __fadd_rn(__fadd_rn(cur[0][j], cur[1][j]), __fadd_rn(cur[2][j], cur[3][j]));
             else
-                o[j] = s4;
+                o[j] = __fadd_rn(cur[0][j], cur[1][j]);
         }
         if (a.offset) {   // every path carries the FP16 volume's per-pixel shift once
-            const float sh = __fmul_rn((float)NP, __ldg(a.offset + pix));
+            const float sh = __fmul_rn((float)(2 * NP), __ldg(a.offset + pix));
 #pragma unroll
             for (int j = 0; j < PPL; ++j) o[j] = __fadd_rn(o[j], sh);
         }
@@ -504,9 +537,9 @@ cudaError_t launch_combine(const SgmLaunch& a, int mode, cudaStream_t s) {
     const int blocks = (int)(blocks_needed < (long)sms * 8 ? blocks_needed : (long)sms * 8);
     const bool eight = a.num_paths == 8;
     void (*kern)(SgmLaunch);
-    if (mode == kCombineFilter) kern = eight ? combine_kernel<PPL, kCombineFilter, 8> : combine_kernel<PPL, kCombineFilter, 4>;
-    else if (mode == kCombineArgmin) kern = eight ? combine_kernel<PPL, kCombineArgmin, 8> : combine_kernel<PPL, kCombineArgmin, 4>;
-    else kern = eight ? combine_kernel<PPL, kCombineStore, 8> : combine_kernel<PPL, kCombineStore, 4>;
+    if (mode == kCombineFilter) kern = eight ? combine_kernel<PPL, kCombineFilter, 4> : combine_kernel<PPL, kCombineFilter, 2>;
+    else if (mode == kCombineArgmin) kern = eight ? combine_kernel<PPL, kCombineArgmin, 4> : combine_kernel<PPL, kCombineArgmin, 2>;
+    else kern = eight ? combine_kernel<PPL, kCombineStore, 4> : combine_kernel<PPL, kCombineStore, 2>;
     return launch_with_priority(kern, dim3(blocks), dim3(256), 0, s, a.priority, a);
 }
 
