@@ -107,9 +107,13 @@ def test_sgm_and_filter_bit_exact(pm_lib, D, paths, compat, uniq):
     rf, _ = upload_images(pm_lib, fs, p.intensity_scale)
     dcost = torch.from_numpy(cost).cuda()
     out = torch.empty_like(dcost)
-    part = torch.empty((p.num_paths - 1,) + tuple(dcost.shape), dtype=torch.float32, device="cuda")
+    # the documented minimum scratch (num_paths/2 - 1 pair volumes) followed by a guard volume
+    npairs = p.num_paths // 2
+    part = torch.full((npairs,) + tuple(dcost.shape), 7.0, dtype=torch.float32, device="cuda")
     cfg = config(p)
     assert pm_lib.pm_stage_sgm(ctypes.byref(cfg), vp(dcost), vp(rf), vp(out), vp(part), None) == 0
+    torch.cuda.synchronize()
+    assert (part[npairs - 1] == 7.0).all(), "pm_stage_sgm wrote past its scratch"
     depth = torch.empty((p.H, p.W), dtype=torch.float32, device="cuda")
     idx = torch.empty((p.H, p.W), dtype=torch.int32, device="cuda")
     assert pm_lib.pm_stage_filter(ctypes.byref(cfg), vp(out), vp(depth), 4 * p.W, vp(idx), None) == 0
@@ -124,7 +128,7 @@ def test_sgm_and_filter_bit_exact(pm_lib, D, paths, compat, uniq):
     p.sum_order = 1
     np.testing.assert_allclose(seq_sum, want_sum, rtol=2e-6, atol=1e-6)
     # fused last path + filter gives the same depth and index
-    scratch = torch.empty((p.num_paths,) + tuple(dcost.shape), dtype=torch.float32, device="cuda")
+    scratch = torch.full((npairs + 1,) + tuple(dcost.shape), 7.0, dtype=torch.float32, device="cuda")
     depth2 = torch.zeros((p.H, p.W + 3), dtype=torch.float32, device="cuda")   # pitched output
     idx2 = torch.empty((p.H, p.W), dtype=torch.int32, device="cuda")
     assert pm_lib.pm_stage_sgm_filter(ctypes.byref(cfg), vp(dcost), vp(rf), vp(scratch), vp(depth2),
@@ -132,6 +136,7 @@ def test_sgm_and_filter_bit_exact(pm_lib, D, paths, compat, uniq):
     torch.cuda.synchronize()
     assert (idx2.cpu().numpy() == want_idx).all()
     assert (bits(depth2.cpu().numpy()[:, :p.W]) == bits(want_depth)).all()
+    assert (scratch[npairs] == 7.0).all(), "pm_stage_sgm_filter wrote past its scratch"
     # every decision branch of filter_cost.cu:37-52 is exercised
     assert (want_depth == 1000.0).any() and (want_depth == 0).any() and ((want_depth > 0) & (want_depth < 1000)).any()
 
