@@ -395,6 +395,7 @@ int main(int argc, char** argv) {
     std::vector<float> h_depth;
     std::vector<uint8_t> h_bgr;
     double sum_ms = 0.0;
+    std::vector<double> times;
     int rc;
     for (size_t n = 0; n < kfs.size(); ++n) {
         const Keyframe& k = kfs[n];
@@ -405,8 +406,7 @@ int main(int argc, char** argv) {
         if ((rc = load(k.ref, slots[0])) != 0) return rc;
         for (int i = 0; i < a.agg; ++i)
             if ((rc = load(k.src[i], slots[(size_t)i + 1])) != 0) return rc;
-        const auto t0 = std::chrono::steady_clock::now();
-        if (!h) {
+        if (!h) {   // the reference constructs its StereoMapper at start-up, outside the timed interval
             W = slots[0].W;
             H = slots[0].H;
             pm_config c;
@@ -430,6 +430,7 @@ int main(int argc, char** argv) {
         }
         for (const DevFrame& s : slots)
             if (s.W != W || s.H != H) { std::fprintf(stderr, "pm_sequence: frames differ in size\n"); return 2; }
+        const auto t0 = std::chrono::steady_clock::now();   // evaluate.cc:244 (tc_sgm)
         CK_PM(h, pm_init_reference(h, slots[0].data, (size_t)W));
         for (int i = 0; i < a.agg; ++i) {
             double Rr[9], Tr[3];
@@ -454,7 +455,9 @@ int main(int argc, char** argv) {
         h_depth.resize((size_t)w * hh);
         CK_CUDA(cudaMemcpyAsync(h_depth.data(), cur, 4 * (size_t)w * hh, cudaMemcpyDeviceToHost, stream));
         CK_CUDA(cudaStreamSynchronize(stream));
-        sum_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        sum_ms += ms;
+        times.push_back(ms);
         const std::string stem = a.out + "/depth_" + F[k.ref].t.text;
         const std::string dpath = stem + "." + a.format;
         if ((a.format == "pfm" ? pm_write_pfm(dpath.c_str(), w, hh, h_depth.data(), 0)
@@ -476,9 +479,14 @@ int main(int argc, char** argv) {
             }
         }
     }
+    std::vector<double> sorted = times;
+    std::sort(sorted.begin(), sorted.end());
+    // the mean is the reference's "AVERAE CAL TIME" (evaluate.cc:268-270); the first keyframe also
+    // pays the one-time loading of the library's kernels
     std::printf("{\"keyframes\": %zu, \"warnings\": %d, \"case\": %d, \"width\": %d, \"height\": %d, "
-                "\"mean_ms_per_keyframe\": %.3f}\n",
-                kfs.size(), warnings, a.out_case, W << a.downsample, H << a.downsample, sum_ms / kfs.size());
+                "\"mean_ms_per_keyframe\": %.3f, \"median_ms_per_keyframe\": %.3f, \"first_ms\": %.3f}\n",
+                kfs.size(), warnings, a.out_case, W << a.downsample, H << a.downsample, sum_ms / kfs.size(),
+                sorted[sorted.size() / 2], times[0]);
     pm_destroy(h);
     for (DevFrame& s : slots) {
         cudaFree(s.buf[0]);

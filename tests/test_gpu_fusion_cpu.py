@@ -50,3 +50,52 @@ def test_cpu_variant_sequence_matches_oracle(mode):
         nonzero += int((got != 0).sum())
     assert nonzero > 0
     m.close()
+
+
+def test_fusion_step_times_640x480():
+    """Measurement: the fusion step of both variants on the GPU (stage timer) at 640x480, next to
+    the sequential restatement of outputFusionCPU on the host (the reference runs it as
+    single-threaded CPU loops).  With PM_REPORT_DIR set the numbers go to
+    $PM_REPORT_DIR/fusion_640x480.json."""
+    import json
+    import os
+    import time
+    W, H, D, S = 640, 480, 64, 3
+    seq = scene.make_sequence(W, H, 520.0, S, 3, seed=71)
+    rho0, drho = scene.plane_range(D)
+    K = seq[0].K
+    cam = (K[0, 0], K[1, 1], K[0, 2], K[1, 2])
+    report = {}
+    for name, variant in (("gpu_variant", _lib.PM_FUSION_GPU), ("cpu_variant", _lib.PM_FUSION_CPU_PATH)):
+        m = StereoMapper(W, H, D, fusion_variant=variant, rho0=rho0, intensity_scale=1 / 255, p1=0.003, p2=0.01,
+                         tau_so=3.5 / 255)
+        m.initIntrinsic(K, 0.0, drho)
+        m.enable_stage_timing(True)
+        times = []
+        for k, fs in enumerate(seq):
+            m.initReference(fs.ref)
+            for s in range(S):
+                m.update(fs.srcs[s], fs.R_ref, fs.T_ref, fs.R_srcs[s], fs.T_srcs[s])
+            m.outputFusion(fs.R_ref, fs.T_ref, *cam)
+            if k > 0:
+                times.append(float(m.stage_times()[2]))
+        report[name + "_ms"] = min(times)
+        if variant == _lib.PM_FUSION_CPU_PATH:
+            # the host restatement on the same inputs: the state before the last step and its WTA depth
+            state = {n: np.zeros((2, W * H), np.float32) for n in ("alpha", "beta", "mu", "sigma")}
+            state["table"] = np.zeros((2, W * H), np.uint32)
+            for n, v in zip(("alpha", "beta", "mu", "sigma"), m.get_state()):
+                state[n][0] = v
+            depth = m.wta_depth().reshape(-1).copy()
+            rel = oracle.relative_pose(seq[2].R_ref, seq[2].T_ref, seq[1].R_ref, seq[1].T_ref)
+            t0 = time.perf_counter()
+            oracle.fuse_cpu(W, H, rel, np.array(cam, np.float32), 0, depth, state)
+            report["host_sequential_ms"] = 1000 * (time.perf_counter() - t0)
+        m.close()
+    print(json.dumps(report))
+    out = os.environ.get("PM_REPORT_DIR")
+    if out:
+        os.makedirs(out, exist_ok=True)
+        with open(os.path.join(out, "fusion_640x480.json"), "w") as f:
+            json.dump(report, f, indent=1)
+    assert all(v > 0 for v in report.values())

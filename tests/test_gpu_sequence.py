@@ -133,3 +133,27 @@ def test_driver_npy_output(stream, tmp_path):
     want = python_run(stream, 2)
     for stamp, d in want.items():
         np.testing.assert_array_equal(np.load(os.path.join(str(tmp_path), f"depth_{stamp}.npy")), d)
+
+
+def test_driver_time_per_keyframe_640x480(tmp_path_factory):
+    """Measurement: the driver's mean time per keyframe (initReference, three updates, the CPU
+    fusion variant, copy-out; the interval evaluate.cc:244-269 times) at 640x480 with the
+    reference's 64 planes and 4 paths, FP32 and FP16 with the texture sampler.  With
+    PM_REPORT_DIR set the numbers go to $PM_REPORT_DIR/driver_640x480.json."""
+    import json
+    root = str(tmp_path_factory.mktemp("seq640"))
+    imgs, R, T, _ = scene.make_stream(640, 480, 520.0, 25, seed=6, step=0.02)
+    il, pl = sequence.write_tum(root, imgs, R, T)
+    report = {}
+    for name, opts in (("fp32", {}), ("fp16_texture_f32", dict(precision="fp16", sampler="texture_f32"))):
+        out = os.path.join(root, name)
+        os.makedirs(out)
+        res = sequence.run(il, pl, out, root=root, case=3, fx="520.0", fy="520.0", cx="320.0", cy="240.0", **opts)
+        report[name] = res[-1]
+    print(json.dumps(report))
+    rep = os.environ.get("PM_REPORT_DIR")
+    if rep:
+        os.makedirs(rep, exist_ok=True)
+        with open(os.path.join(rep, "driver_640x480.json"), "w") as f:
+            json.dump(report, f, indent=1)
+    assert all(r["keyframes"] == 4 and r["mean_ms_per_keyframe"] > 0 for r in report.values())
