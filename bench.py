@@ -131,13 +131,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
+def sampler_name(args, precision) -> str:
+    """The source sampler of a form: --sampler for the FP16 form, --fp32-sampler for the FP32 one."""
+    return args.sampler if precision in ("fp16", 1) else args.fp32_sampler
+
+
 def make_mapper(precision: int, device: int, cost_mode: int = 0, sampler: int = 0):
     from probabilistic_mapping_b200 import scene
     from probabilistic_mapping_b200.mapper import StereoMapper
     rho0, drho = scene.plane_range(D)
     m = StereoMapper(W, H, D, rho0=rho0, intensity_scale=1 / 255, num_paths=PATHS, p1=P1, p2=P2, tau_so=TAU,
                      uniqueness_ratio=UNIQ, cost_mode=cost_mode, precision=precision, device=device,
-                     sampler=sampler if precision == 1 else 0)
+                     sampler=sampler)
     return m, drho
 
 
@@ -180,7 +185,7 @@ def run_ours(args, rank, world, precision: str = "fp32", passes=("dev", "e2e", "
     K = seq[0].K
     fx, fy, cx, cy = K[0, 0], K[1, 1], K[0, 2], K[1, 2]
     prec = 1 if precision == "fp16" else 0
-    m, drho = make_mapper(prec, dev, 1 if args.cost_mode == "corrected" else 0, SAMPLERS[args.sampler])
+    m, drho = make_mapper(prec, dev, 1 if args.cost_mode == "corrected" else 0, SAMPLERS[sampler_name(args, prec)])
     m.initIntrinsic(K, 0.0, drho)
     stream = torch.cuda.Stream(device=dev)
     m.set_stream(stream.cuda_stream)
@@ -271,7 +276,7 @@ def run_batched(args, rank, world, precision: str, B: int, host_io: bool, clocks
     prec = _lib.PM_PREC_FP16 if precision == "fp16" else _lib.PM_PREC_FP32
     cfg = dict(width=W, height=H, num_planes=D, rho0=rho0, intensity_scale=1 / 255, num_paths=PATHS, p1=P1, p2=P2,
                tau_so=TAU, uniqueness_ratio=UNIQ, cost_mode=1 if args.cost_mode == "corrected" else 0,
-               precision=prec, device=dev, sampler=SAMPLERS[args.sampler] if prec == _lib.PM_PREC_FP16 else 0)
+               precision=prec, device=dev, sampler=SAMPLERS[sampler_name(args, prec)])
     seqs = [scene.make_sequence(W, H, F_PX, S, 2, seed=2000 + 97 * rank + i) for i in range(B)]
     b = StereoBatch([cfg] * B, S, lanes=0, host_io=host_io, autotune=True, priority=args.priority)
     for i in range(B):
@@ -334,7 +339,7 @@ def run_mixed(args, rank, world, precision: str, host_io: bool, clocks: bool):
             cfgs.append(dict(width=w, height=h, num_planes=d, rho0=rho0, intensity_scale=1 / 255, num_paths=PATHS,
                              p1=P1, p2=P2, tau_so=TAU, uniqueness_ratio=UNIQ,
                              cost_mode=1 if args.cost_mode == "corrected" else 0, precision=prec, device=dev,
-                             sampler=SAMPLERS[args.sampler] if prec == _lib.PM_PREC_FP16 else 0))
+                             sampler=SAMPLERS[sampler_name(args, prec)]))
             shapes.append(k)
     mine = shard_sequences(cfgs, world, MIXED_S)[rank]
     scenes = {k: [scene.make_sequence(w, h, f, MIXED_S, 2, seed=3000 + 10 * k + j) for j in range(2)]
@@ -396,7 +401,7 @@ def mixed_main(args, rank, world):
                 "scaling": "strong", "vs_baseline": None, "dtype": "f16" if precision == "fp16" else "f32",
                 "data": "synthetic",
                 "config": {"workload": f"48 sequences, {MIXED_S} sources, {PATHS}-path SGM, fusion step, "
-                                       f"{precision}" + (f" {args.sampler} sampler" if precision == "fp16" else "")
+                                       f"{precision} {sampler_name(args, precision)} sampler"
                                        + f", lanes={args.lanes}", "global_batch": total, "seq_len": 0,
                            "parallelism": f"sequence shards x{world}, balanced by voxels x sources",
                            "l2": "per-map working sets exceed the 126 MB L2"},
@@ -449,6 +454,9 @@ def main():
     ap.add_argument("--lanes", type=int, default=0, help="volume sets per size in the mixed batch (0: one each)")
     ap.add_argument("--sampler", choices=list(SAMPLERS), default="texture_f32",
                     help="FP16 form: source sampling (exact FP32 bilinear, or the texture unit from FP16 / FP32 texels)")
+    ap.add_argument("--fp32-sampler", choices=["exact", "texture_f32"], default="exact",
+                    help="FP32 form: exact FP32 bilinear (bit-exact against the FP32 oracle) or the texture "
+                         "unit on FP32 texels (the reference's own sampler)")
     ap.add_argument("--priority", type=int, default=1, choices=[0, 1],
                     help="batched forms: SGM kernels at the greatest launch priority (1) or not (0)")
     ap.add_argument("--precision", choices=["fp32", "fp16"], default=None,
@@ -526,7 +534,7 @@ def main():
     peak_hbm, sm_mhz, peak_kind = peaks()
     peak_fp32 = fp32_peak_tflops(sm_mhz)
     cost_ms, sgm_ms = float(stage_ms[0]), float(stage_ms[1])
-    cost_flop, cost_bytes = cost_kernel_work(e, e == 2 and args.sampler != "exact")
+    cost_flop, cost_bytes = cost_kernel_work(e, sampler_name(args, args.precision) != "exact")
     cost_tflops = cost_flop / (cost_ms / 1000.0) / 1e12 if cost_ms > 0 else None
     cost_gbs = cost_bytes / (cost_ms / 1000.0) / 1e9 if cost_ms > 0 else None
     sgm_gbs = sgm_bytes / (sgm_ms / 1000.0) / 1e9 if sgm_ms > 0 else None
@@ -542,7 +550,7 @@ def main():
             "config": {"workload": f"{W}x{H}, {D} planes, {S} sources, {PATHS}-path SGM, uniqueness {UNIQ}, "
                                    f"fusion step; {args.precision} {args.form} form"
                                    + (f", {B} sequences per CUDA-graph launch" if args.form == "batched" else "")
-                                   + (f", {args.sampler} sampler" if args.precision == "fp16" else "")
+                                   + f", {sampler_name(args, args.precision)} sampler"
                                    + f", {args.cost_mode} cost samples",
                        "global_batch": world * B, "seq_len": 0, "parallelism": f"replicas x{world}",
                        "l2": "per-map working set (cost + path volumes, >1 GB) exceeds the 126 MB L2"},
@@ -554,7 +562,8 @@ def main():
                                                                     if e == 2 else ""),
                          "achieved": cost_tflops, "peak": peak_fp32,
                          "unit": "TFLOP/s", "frac": (cost_tflops / peak_fp32) if cost_tflops else None,
-                         "traffic": ncu_traffic("cost_kernel" if e == 4 else "cost_kernel_fp16"),
+                         "traffic": ncu_traffic("cost_kernel" if e == 4 and args.fp32_sampler == "exact"
+                                                else "cost_kernel_fp16" if e == 2 else None),
                          "ms_per_launch": cost_ms,
                          "algorithmic_flop_per_launch": cost_flop, "algorithmic_bytes_per_launch": cost_bytes,
                          "hbm_achieved_gbs": cost_gbs, "hbm_frac": (cost_gbs / peak_hbm) if cost_gbs else None,

@@ -50,13 +50,17 @@ typedef int pm_status;
 #define PM_PREC_FP32 0 /* plain form: FP32 images, cost volume and aggregation */
 #define PM_PREC_FP16 1 /* FP16 cost volume, FP32 SGM accumulators and fusion */
 
-/* How the FP16 form samples source frames (the FP32 form always uses exact bilinear weights). */
-#define PM_SAMPLER_EXACT 0   /* FP16-rounded images, bilinear weights and interpolation in FP32 */
+/* How source frames are sampled.  The FP32 form takes PM_SAMPLER_EXACT or PM_SAMPLER_TEXTURE_F32,
+ * the FP16 form all three. */
+#define PM_SAMPLER_EXACT 0   /* bilinear weights and interpolation in FP32 (FP16 form: of the
+                                FP16-rounded images) */
 #define PM_SAMPLER_TEXTURE 1 /* FP16 texels filtered by the texture unit (8-bit weights, as the
                                 reference's own textures, calc_cost.cu:226-237; the unit filters
                                 FP16 texels at reduced precision) */
-#define PM_SAMPLER_TEXTURE_F32 2 /* FP16-rounded images in FP32 texels: the texture unit's 8-bit
-                                    weights with FP32 filtering, at the speed of PM_SAMPLER_TEXTURE */
+#define PM_SAMPLER_TEXTURE_F32 2 /* FP32 texels filtered by the texture unit: 8-bit weights with
+                                    FP32 filtering, at the speed of PM_SAMPLER_TEXTURE.  FP32 form:
+                                    the images themselves, the reference's own sampler; FP16 form:
+                                    the FP16-rounded images */
 
 #define PM_FUSION_GPU 0      /* StereoMapper::outputFusion + depth_fusion.cu kernels */
 #define PM_FUSION_CPU_PATH 1 /* the constants and masks of outputFusionCPU, run on the GPU */
@@ -80,7 +84,7 @@ typedef struct pm_config {
                             (drops planes when D is not a power of two); 0: exact minimum */
     int max_sources;     /* source frames kept per reference frame (lazy cost evaluation) */
     int device;          /* CUDA device ordinal */
-    int sampler;         /* PM_SAMPLER_*, FP16 form only */
+    int sampler;         /* PM_SAMPLER_* */
 } pm_config;
 
 typedef struct pm_mapper pm_mapper;
@@ -199,7 +203,7 @@ PM_API const char* pm_status_string(pm_status s);
  * calls, issued as ONE CUDA-graph launch in which the sequences are independent branches.
  * Sequences of the same shape share `lanes` sets of cost and path volumes (0: one set each).
  * Two buffer sets alternate by step, so frames for step t+1 can be written while step t runs.
- * The texture sampler and the CPU fusion variant are not available in a batch.
+ * The CPU fusion variant is not available in a batch.
  * --------------------------------------------------------------------------------------- */
 typedef struct pm_batch pm_batch;
 #define PM_BATCH_HOST_IO 1  /* frames in and fused depth/variance out through batch-owned pinned
@@ -286,7 +290,10 @@ PM_API pm_status pm_stage_to_float(int W, int H, const uint8_t* src, size_t src_
  * consecutive W*H float images; homs: 12*nsrc floats in HOST memory.  cost: W*H*D float.
  * When cnt is NULL the volume starts from cost=-1, cnt=0 (initReference); otherwise cost and
  * cnt hold the running state and are updated in place, exactly as repeated ad_calc_cost
- * calls would.  invalid (optional, W*H bytes) receives 1 where some plane was never measured. */
+ * calls would.  invalid (optional, W*H bytes) receives 1 where some plane was never measured.
+ * cfg->sampler PM_SAMPLER_TEXTURE_F32 samples the sources through textures, as the reference:
+ * the call then allocates pitched copies of the sources and their texture objects, and returns
+ * after the kernels have finished. */
 PM_API pm_status pm_stage_calc_cost(const pm_config* cfg, const float* ref, const float* srcs, int nsrc,
                              const float* homs, float* cost, float* cnt, uint8_t* invalid,
                              void* stream);

@@ -188,7 +188,7 @@ void usage() {
                  "  [--case N (0 raw-cost argmin, 1 SGM argmin, 2 filtered depth, >=3 fused; default 0)]\n"
                  "  [--planes 64] [--paths 4|8] [--fx F --fy F --cx F --cy F] [--downsample 0]\n"
                  "  [--agg 3] [--interval 6] [--min-depth 0.2] [--max-depth 20] [--format pfm|npy]\n"
-                 "  [--color] [--precision fp32|fp16] [--sampler exact|texture|texture_f32 (fp16)]\n"
+                 "  [--color] [--precision fp32|fp16] [--sampler exact|texture (fp16)|texture_f32]\n"
                  "  [--cost reference|corrected] [--associate SECONDS]\n"
                  "  [--limit N] [--device 0] [--dry-run]\n");
 }
@@ -413,7 +413,7 @@ int main(int argc, char** argv) {
             pm_config_default(&c, W, H, a.planes);
             c.num_paths = a.paths;
             c.precision = a.precision;
-            c.sampler = a.precision == PM_PREC_FP16 ? a.sampler : PM_SAMPLER_EXACT;
+            c.sampler = a.sampler;   // the library rejects FP16 texels in the FP32 form
             c.cost_mode = a.cost_mode;
             c.fusion_variant = PM_FUSION_CPU_PATH;   // outputFusionCPU (evaluate.cc:260)
             c.device = a.device;

@@ -30,9 +30,9 @@ struct pm_mapper {
     uint8_t* d_u8 = nullptr;    // upload staging, W*H bytes
     float* d_ref = nullptr;     // scaled reference image
     float4* d_srcq = nullptr;   // max_sources source frames in the quad layout (FP16 form: FP16-rounded values)
-    void* d_srch[kMaxSources] = {};               // FP16 form, texture samplers: pitched FP16 or FP32 texels
+    void* d_srch[kMaxSources] = {};               // texture samplers: pitched FP16 or FP32 texels
     size_t srch_pitch = 0;
-    cudaTextureObject_t tex[kMaxSources] = {};    // FP16 form: one texture object per slot
+    cudaTextureObject_t tex[kMaxSources] = {};    // texture samplers: one texture object per slot
     int nsrc = 0;               // queued (not yet folded) sources
     std::vector<float> homs;    // 12 floats per queued source
     std::vector<float> all_homs;  // every source since initReference (inspection)
@@ -194,8 +194,8 @@ pm_status check_config(const pm_config* c, pm_mapper* h) {
         return fail(h, PM_ERR_INVALID_ARGUMENT, "FP16 volumes need num_planes to be a multiple of 64");
     if (c->sampler != PM_SAMPLER_EXACT && c->sampler != PM_SAMPLER_TEXTURE && c->sampler != PM_SAMPLER_TEXTURE_F32)
         return fail(h, PM_ERR_INVALID_ARGUMENT, "unknown sampler %d", c->sampler);
-    if (c->sampler != PM_SAMPLER_EXACT && c->precision != PM_PREC_FP16)
-        return fail(h, PM_ERR_INVALID_ARGUMENT, "the texture sampler belongs to the FP16 form");
+    if (c->sampler == PM_SAMPLER_TEXTURE && c->precision != PM_PREC_FP16)
+        return fail(h, PM_ERR_INVALID_ARGUMENT, "FP16 texels belong to the FP16 form");
     if (c->fusion_variant != PM_FUSION_GPU && c->fusion_variant != PM_FUSION_CPU_PATH)
         return fail(h, PM_ERR_INVALID_ARGUMENT, "unknown fusion_variant %d", c->fusion_variant);
     if (c->max_sources < 1 || c->max_sources > kMaxSources)
@@ -248,7 +248,9 @@ pm_status upload_image(pm_mapper* h, const uint8_t* img, size_t pitch, float* ds
     }
     const float sc = h->cfg.intensity_scale;
     const bool half = h->cfg.precision == PM_PREC_FP16;
-    if (slot >= 0 && half && h->cfg.sampler == PM_SAMPLER_TEXTURE)
+    if (slot >= 0 && !half && h->cfg.sampler == PM_SAMPLER_TEXTURE_F32)
+        PM_CK(h, launch_to_float_pitched(W, H, dev, pitch, (float*)h->d_srch[slot], h->srch_pitch, sc, h->stream));
+    else if (slot >= 0 && half && h->cfg.sampler == PM_SAMPLER_TEXTURE)
         PM_CK(h, launch_to_half(W, H, dev, pitch, h->d_srch[slot], h->srch_pitch, sc, h->stream));
     else if (slot >= 0 && half && h->cfg.sampler == PM_SAMPLER_TEXTURE_F32)
         PM_CK(h, launch_to_float_h_pitched(W, H, dev, pitch, (float*)h->d_srch[slot], h->srch_pitch, sc, h->stream));
@@ -272,7 +274,7 @@ pm_status evaluate_cost(pm_mapper* h, bool into_state) {
     a.ref = h->d_ref;
     a.srcq = h->d_srcq;
     a.nsrc = h->nsrc;
-    if (c.precision == PM_PREC_FP16 && c.sampler != PM_SAMPLER_EXACT) {
+    if (c.sampler != PM_SAMPLER_EXACT) {
         a.use_tex = 1;
         for (int s = 0; s < h->nsrc; ++s) a.tex[s] = h->tex[s];
     }
@@ -428,16 +430,17 @@ pm_status pm_create(const pm_config* cfg, pm_mapper** out) {
     h->own_stream = ok;
     const bool half = cfg->precision == PM_PREC_FP16;
     ok = ok && alloc((void**)&h->d_u8, N) && alloc((void**)&h->d_ref, 4 * N) &&
-         ((half && cfg->sampler != PM_SAMPLER_EXACT) || alloc((void**)&h->d_srcq, 16 * N * cfg->max_sources)) &&
+         (cfg->sampler != PM_SAMPLER_EXACT || alloc((void**)&h->d_srcq, 16 * N * cfg->max_sources)) &&
          alloc(&h->d_cost, esz * V) && (!half || (alloc((void**)&h->d_off, 4 * N) && alloc((void**)&h->d_boff, 4 * N * (cfg->num_planes / 16)))) &&
          alloc((void**)&h->d_depth, 4 * N) &&
          alloc((void**)&h->d_idx, 4 * N) && alloc((void**)&h->d_ztable, 8 * N) &&
          alloc((void**)&h->d_table, 4 * N) && alloc((void**)&h->d_fused, 4 * N) &&
          alloc((void**)&h->d_var, 4 * N);
-    // FP16 form: per-slot pitched images (FP16 texels, or FP16-rounded values in FP32 texels)
-    // sampled through texture objects (linear filter, zero border, unnormalised coordinates: the
-    // reference's texture setup, calc_cost.cu:226-237)
-    for (int s = 0; half && cfg->sampler != PM_SAMPLER_EXACT && s < cfg->max_sources && ok; ++s)
+    // texture samplers: per-slot pitched images (FP16 form: FP16 texels, or FP16-rounded values in
+    // FP32 texels; FP32 form: the images in FP32 texels) sampled through texture objects (linear
+    // filter, zero border, unnormalised coordinates: the reference's texture setup,
+    // calc_cost.cu:226-237)
+    for (int s = 0; cfg->sampler != PM_SAMPLER_EXACT && s < cfg->max_sources && ok; ++s)
         ok = note(make_source_texture(cfg->width, cfg->height, cfg->sampler == PM_SAMPLER_TEXTURE_F32, &h->d_srch[s],
                                       &h->srch_pitch, &h->tex[s]));
     for (int r = 0; r < cfg->num_paths / 2 && ok; ++r) ok = alloc((void**)&h->d_part[r], 4 * V);
@@ -796,12 +799,20 @@ pm_status pm_stage_calc_cost(const pm_config* cfg, const float* ref, const float
     if (cfg->precision != PM_PREC_FP32) return PM_ERR_UNSUPPORTED;
     if (nsrc > kMaxSources && !cnt) return PM_ERR_INVALID_ARGUMENT;   // needs a running count
     const size_t N = (size_t)cfg->width * cfg->height;
+    const int W = cfg->width, H = cfg->height;
+    const bool tex = cfg->sampler == PM_SAMPLER_TEXTURE_F32;
+    const cudaStream_t st = (cudaStream_t)stream;
     CostLaunch a;
     fill_cost_launch(*cfg, a);
     a.ref = ref;
     a.cost = cost;
     a.cnt = cnt;
     a.invalid = invalid;
+    // texture sampler: pitched copies of one pass's sources behind texture objects, released
+    // once the pass has finished
+    void* buf[kMaxSources] = {};
+    size_t pitch = 0;
+    bool ok = true;
     int done = 0;
     do {
         const int n = std::min(nsrc - done, kMaxSources);
@@ -809,9 +820,25 @@ pm_status pm_stage_calc_cost(const pm_config* cfg, const float* ref, const float
         a.nsrc = n;
         for (int s = 0; s < n; ++s)
             for (int i = 0; i < 12; ++i) a.hom[s][i] = homs[12 * (done + s) + i];
+        for (int s = 0; tex && s < n && ok; ++s) {
+            ok = make_source_texture(W, H, true, &buf[s], &pitch, &a.tex[s]) == cudaSuccess &&
+                 cudaMemcpy2DAsync(buf[s], pitch, srcs + N * (done + s), 4 * (size_t)W, 4 * (size_t)W, (size_t)H,
+                                   cudaMemcpyDeviceToDevice, st) == cudaSuccess;
+        }
+        a.use_tex = tex ? 1 : 0;
         // with a count buffer the call continues the running state, like repeated ad_calc_cost
         a.incremental = cnt ? 1 : 0;
-        if (launch_cost(a, (cudaStream_t)stream) != cudaSuccess) return PM_ERR_CUDA;
+        ok = ok && launch_cost(a, st) == cudaSuccess;
+        if (tex) {
+            ok = cudaStreamSynchronize(st) == cudaSuccess && ok;
+            for (int s = 0; s < n; ++s) {
+                if (a.tex[s]) cudaDestroyTextureObject(a.tex[s]);
+                cudaFree(buf[s]);
+                a.tex[s] = 0;
+                buf[s] = nullptr;
+            }
+        }
+        if (!ok) return PM_ERR_CUDA;
         done += n;
     } while (done < nsrc);
     return PM_OK;

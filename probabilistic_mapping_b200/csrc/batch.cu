@@ -64,7 +64,7 @@ struct Seq {
     // persistent device state
     float* d_ref = nullptr;
     float4* d_srcq = nullptr;
-    // FP16 form with a texture sampler: pitched source images and their texture objects
+    // texture samplers: pitched source images and their texture objects
     void* d_srch[kMaxSources] = {};
     size_t srch_pitch = 0;
     cudaTextureObject_t tex[kMaxSources] = {};
@@ -247,7 +247,8 @@ cudaError_t enqueue_seq(pm_batch* b, int i, int k) {
         if (c.sampler == PM_SAMPLER_TEXTURE)
             e = launch_to_half(W, H, f, W, q.d_srch[s], q.srch_pitch, sc, m);
         else if (c.sampler == PM_SAMPLER_TEXTURE_F32)
-            e = launch_to_float_h_pitched(W, H, f, W, (float*)q.d_srch[s], q.srch_pitch, sc, m);
+            e = half ? launch_to_float_h_pitched(W, H, f, W, (float*)q.d_srch[s], q.srch_pitch, sc, m)
+                     : launch_to_float_pitched(W, H, f, W, (float*)q.d_srch[s], q.srch_pitch, sc, m);
         else
             e = half ? launch_to_quad_half(W, H, f, W, q.d_srcq + (size_t)s * N, sc, m)
                      : launch_to_quad(W, H, f, W, q.d_srcq + (size_t)s * N, sc, m);

@@ -1,6 +1,7 @@
 // convert.cu -- image conversions.
 //   to_float_kernel: uint8 -> scaled float, the convertTo(CV_32F) + upload of
-//                    StereoMapper::initReference / update (stereo_mapper.cpp:65-67,75-77).
+//                    StereoMapper::initReference / update (stereo_mapper.cpp:65-67,75-77);
+//                    pitched, it fills the FP32 texels of the FP32 form's texture sampler.
 //   to_half_kernel:  uint8 -> scaled FP16 (pitched texture storage of the FP16 form), or the
 //                    same values widened to float (its reference image).
 //   convert_kernel:  pitched <-> linear float copy (reference: convert.cu:4-45).  The pitch is
@@ -15,10 +16,11 @@ namespace pm {
 namespace {
 
 __global__ void __launch_bounds__(256) to_float_kernel(int W, int H, const uint8_t* __restrict__ src,
-                                                       size_t pitch, float* __restrict__ dst, float scale) {
+                                                       size_t pitch, float* __restrict__ dst, size_t dst_pitch,
+                                                       float scale) {
     const int y = blockIdx.y;
     const uint8_t* row = src + (size_t)y * pitch;
-    float* out = dst + (size_t)y * W;
+    float* out = reinterpret_cast<float*>(reinterpret_cast<char*>(dst) + (size_t)y * dst_pitch);
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < W; x += gridDim.x * blockDim.x)
         out[x] = __fmul_rn((float)row[x], scale);
 }
@@ -94,7 +96,14 @@ __global__ void __launch_bounds__(256) convert_kernel(int W, int H, const float*
 cudaError_t launch_to_float(int W, int H, const uint8_t* src, size_t src_pitch, float* dst, float scale,
                             cudaStream_t s) {
     const dim3 grid((W + 255) / 256, H);
-    to_float_kernel<<<grid, 256, 0, s>>>(W, H, src, src_pitch, dst, scale);
+    to_float_kernel<<<grid, 256, 0, s>>>(W, H, src, src_pitch, dst, 4 * (size_t)W, scale);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_to_float_pitched(int W, int H, const uint8_t* src, size_t src_pitch, float* dst,
+                                    size_t dst_pitch, float scale, cudaStream_t s) {
+    const dim3 grid((W + 255) / 256, H);
+    to_float_kernel<<<grid, 256, 0, s>>>(W, H, src, src_pitch, dst, dst_pitch, scale);
     return cudaGetLastError();
 }
 

@@ -70,9 +70,11 @@ __device__ __forceinline__ float2 shfl_down2(float2 v) {
 
 // Source access: plain float rows, the quad layout (one 16-byte load per bilinear sample; in the
 // FP16 form its values are rounded to FP16 but kept in FP32 lanes, since a per-sample conversion
-// costs more issue slots than the wider loads cost bandwidth in this issue-bound kernel), or (FP16
-// form) a texture object over an FP16 image, filtered by the texture unit.
-enum { kPlain = 0, kQuad = 1, kTex = 2, kQuadH = 3 };
+// costs more issue slots than the wider loads cost bandwidth in this issue-bound kernel), or a
+// texture object filtered by the texture unit: FP16 form (kTex, FP16 or FP16-rounded FP32 texels,
+// hardware reciprocal estimate in the warp) or FP32 form (kTexF, FP32 texels of the images, the
+// warp's Newton reciprocal: the reference's own sampler, calc_cost.cu:226-237).
+enum { kPlain = 0, kQuad = 1, kTex = 2, kQuadH = 3, kTexF = 4 };
 template <int SAMP> struct Src;
 template <> struct Src<kPlain> {
     const float* __restrict__ p;
@@ -84,6 +86,10 @@ template <> struct Src<kQuad> {
     unsigned off;   // (1.5 * 2^23 bit pattern) * (W + 1), folded out of the quad index
 };
 template <> struct Src<kTex> {
+    cudaTextureObject_t t;
+    int W, H;
+};
+template <> struct Src<kTexF> {
     cudaTextureObject_t t;
     int W, H;
 };
@@ -119,7 +125,7 @@ __device__ __forceinline__ float2 sample2(const Src<SAMP>& src, const WarpConst&
     const float2 u = __fmul2_rn(nx, r), v = __fmul2_rn(ny, r);
     const bool ok0 = (w.x >= 0.0f) && (u.x >= 0.0f) && (u.x <= c.W1) && (v.x >= 0.0f) && (v.x <= c.H1);
     const bool ok1 = (w.y >= 0.0f) && (u.y >= 0.0f) && (u.y <= c.W1) && (v.y >= 0.0f) && (v.y <= c.H1);
-    if constexpr (SAMP == kTex) {
+    if constexpr (SAMP == kTex || SAMP == kTexF) {
         // texel centres at +0.5, as the reference's tex2D(t, u + 0.5f, v + 0.5f) (calc_cost.cu:93)
         const float s0 = tex2D<float>(src.t, u.x + 0.5f, v.x + 0.5f);
         const float s1 = tex2D<float>(src.t, u.y + 0.5f, v.y + 0.5f);
@@ -274,7 +280,7 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
         if constexpr (SAMP == kQuad || SAMP == kQuadH) {
             src.q = a.srcq + (size_t)s * W * H;
             src.off = 0x4B400000u * (unsigned)(W + 1);
-        } else if constexpr (SAMP == kTex) {
+        } else if constexpr (SAMP == kTex || SAMP == kTexF) {
             src.t = a.tex[s];
         } else {
             src.p = a.srcs + (size_t)s * W * H;
@@ -467,12 +473,12 @@ cudaError_t launch_t(const CostLaunch& a, dim3 grid, cudaStream_t s) {
 
 template <int MODE, bool HALF>
 cudaError_t launch_q(const CostLaunch& a, dim3 grid, cudaStream_t s) {
-    // FP16 volumes come from the FP16 form's samplers, FP32 volumes from the exact FP32 ones
+    // FP16 volumes come from the FP16 form's samplers, FP32 volumes from the FP32 ones
     if constexpr (HALF) {
         if (a.use_tex) return launch_t<MODE, true, kTex>(a, grid, s);
         return a.srcq ? launch_t<MODE, true, kQuadH>(a, grid, s) : cudaErrorInvalidValue;
     } else {
-        if (a.use_tex) return cudaErrorInvalidValue;
+        if (a.use_tex) return launch_t<MODE, false, kTexF>(a, grid, s);
         return a.srcq ? launch_t<MODE, false, kQuad>(a, grid, s) : launch_t<MODE, false, kPlain>(a, grid, s);
     }
 }

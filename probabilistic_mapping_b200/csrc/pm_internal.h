@@ -20,8 +20,8 @@ struct CostLaunch {
     // nsrc consecutive W*H quad images (2x2 bilinear footprints); in the FP16 form (cost_half)
     // their values are rounded to FP16
     const float4* srcq;
-    // FP16 form with use_tex: the sources through these texture objects (FP16 pitched images,
-    // linear filtering, zero border)
+    // use_tex: the sources through these texture objects (pitched images, linear filtering, zero
+    // border; FP16 form: FP16 or FP16-rounded FP32 texels, FP32 form: FP32 texels)
     unsigned long long tex[kMaxSources];
     int use_tex;
     int W, H, D, nsrc;
@@ -98,20 +98,23 @@ cudaError_t launch_filter(const float* sum, int W, int H, int D, const FilterPar
 // ---- image conversion (convert.cu + the uint8 -> float upload) ----------------------------
 cudaError_t launch_to_float(int W, int H, const uint8_t* src, size_t src_pitch, float* dst,
                             float scale, cudaStream_t s);
-// uint8 -> scaled quad image: dst[y*W + x] = (I(x,y), I(x,y+1), I(x+1,y), I(x+1,y+1)), zero
-// outside the image (the border addressing of the reference textures, calc_cost.cu:230-237).
+// uint8 -> scaled float rows with a byte pitch (the FP32 form's texture storage).
+cudaError_t launch_to_float_pitched(int W, int H, const uint8_t* src, size_t src_pitch, float* dst,
+                                    size_t dst_pitch, float scale, cudaStream_t s);
 // uint8 -> scaled FP16 image with a byte pitch (the FP16 form's texture storage).
 cudaError_t launch_to_half(int W, int H, const uint8_t* src, size_t src_pitch, void* dst, size_t dst_pitch,
                            float scale, cudaStream_t s);
-// uint8 -> quads of FP16-rounded values in FP32 lanes: the FP16 form's exact sampler.
 // uint8 -> FP16-rounded values in pitched float rows (the FP16 form's FP32-texel textures).
 cudaError_t launch_to_float_h_pitched(int W, int H, const uint8_t* src, size_t src_pitch, float* dst,
                                      size_t dst_pitch, float scale, cudaStream_t s);
+// uint8 -> quads of FP16-rounded values in FP32 lanes: the FP16 form's exact sampler.
 cudaError_t launch_to_quad_half(int W, int H, const uint8_t* src, size_t src_pitch, float4* dst, float scale,
                                 cudaStream_t s);
 // uint8 -> scaled float image whose values are rounded to FP16 (the FP16 form's reference image).
 cudaError_t launch_to_float_h(int W, int H, const uint8_t* src, size_t src_pitch, float* dst, float scale,
                               cudaStream_t s);
+// uint8 -> scaled quad image: dst[y*W + x] = (I(x,y), I(x,y+1), I(x+1,y), I(x+1,y+1)), zero
+// outside the image (the border addressing of the reference textures, calc_cost.cu:230-237).
 cudaError_t launch_to_quad(int W, int H, const uint8_t* src, size_t src_pitch, float4* dst,
                            float scale, cudaStream_t s);
 // A pitched W x H source image (FP16 texels, or FP32 texels when f32) and its texture object:

@@ -53,6 +53,19 @@ def test_create_rejects_bad_config(pm_lib, field, value):
     assert not h.value
 
 
+def test_fp16_texels_belong_to_the_fp16_form(pm_lib):
+    """The FP32 form takes the exact sampler or the texture unit on FP32 texels; FP16 texels (and
+    unknown samplers) are rejected before any device work."""
+    from probabilistic_mapping_b200 import _lib
+    for precision, sampler in ((_lib.PM_PREC_FP32, _lib.PM_SAMPLER_TEXTURE), (_lib.PM_PREC_FP32, 5),
+                               (_lib.PM_PREC_FP16, 3)):
+        c = _lib.default_config(64, 48, 64)
+        c.precision, c.sampler = precision, sampler
+        h = ctypes.c_void_p()
+        assert pm_lib.pm_create(ctypes.byref(c), ctypes.byref(h)) == _lib.PM_ERR_INVALID_ARGUMENT
+        assert not h.value
+
+
 def test_fp16_needs_even_planes_per_lane(pm_lib):
     from probabilistic_mapping_b200 import _lib
     c = _lib.default_config(64, 48, 96)

@@ -25,6 +25,7 @@ SEQS = [
     dict(width=96, height=64, num_planes=64, precision=0, cost_mode=0, num_paths=4),
     dict(width=96, height=64, num_planes=64, precision=0, cost_mode=0, num_paths=8),   # shares seq 0's lane
     dict(width=128, height=96, num_planes=64, precision=1, cost_mode=0, num_paths=8, sampler=2),  # FP32 texels
+    dict(width=112, height=80, num_planes=64, precision=0, cost_mode=0, num_paths=8, sampler=2),  # FP32 form, texture
 ]
 
 

@@ -5,7 +5,8 @@ uniqueness 0.95, scaled intensities.  FP16 form = FP16 source images and referen
 cost volume (shifted per pixel by its smallest measured cost), FP32 SGM accumulators; its sources
 are sampled either with exact bilinear weights in FP32 arithmetic (PM_SAMPLER_EXACT) or by the
 texture unit with 8-bit weights, as the reference's own textures, from FP32 texels
-(PM_SAMPLER_TEXTURE_F32) or FP16 texels (PM_SAMPLER_TEXTURE).  Reported per pixel where both maps hold a depth: median and
+(PM_SAMPLER_TEXTURE_F32) or FP16 texels (PM_SAMPLER_TEXTURE).  The FP32 form is run with the
+exact sampler and with the texture unit on FP32 texels of the unrounded images.  Reported per pixel where both maps hold a depth: median and
 p99 of |rho - rho64| / rho64 (inverse depth), plus the WTA plane-index match rate over all pixels.
 With PM_REPORT_DIR set the numbers are also written to $PM_REPORT_DIR/precision_752x480x128.json.
 """
@@ -76,12 +77,13 @@ def test_fp16_form_against_fp64(frames, mode):
     d16, x16 = run_gpu(frames, _lib.PM_PREC_FP16, mode, _lib.PM_SAMPLER_EXACT)
     dtx, xtx = run_gpu(frames, _lib.PM_PREC_FP16, mode, _lib.PM_SAMPLER_TEXTURE)
     dtf, xtf = run_gpu(frames, _lib.PM_PREC_FP16, mode, _lib.PM_SAMPLER_TEXTURE_F32)
+    d3t, x3t = run_gpu(frames, _lib.PM_PREC_FP32, mode, _lib.PM_SAMPLER_TEXTURE_F32)
     r32, r16, rtx = stats(d32, x32, d64, i64), stats(d16, x16, d64, i64), stats(dtx, xtx, d64, i64)
-    rtf = stats(dtf, xtf, d64, i64)
+    rtf, r3t = stats(dtf, xtf, d64, i64), stats(d3t, x3t, d64, i64)
     report = {"config": f"{W}x{H}, f={F}, {D} planes, {S} sources, 8 paths, "
                         f"{'reference' if mode == 0 else 'corrected'} cost samples",
               "fp32": r32, "fp16_exact_sampler": r16, "fp16_texture_sampler": rtx,
-              "fp16_texture_f32_sampler": rtf}
+              "fp16_texture_f32_sampler": rtf, "fp32_texture_f32_sampler": r3t}
     print(json.dumps(report))
     out = os.environ.get("PM_REPORT_DIR")
     if out:
@@ -90,6 +92,9 @@ def test_fp16_form_against_fp64(frames, mode):
             json.dump(report, f, indent=1)
     assert r32["wta_index_match"] >= 0.995
     assert r32["rel_inv_depth_median"] < 1e-4
+    # the FP32 form with the reference's own sampler (texture unit, FP32 texels, 8-bit weights)
+    assert r3t["wta_index_match"] >= 0.995
+    assert r3t["rel_inv_depth_median"] <= 0.01
     # the FP16 form's accuracy bound: <= 1 % inverse-depth error, >= 99.5 % identical WTA indices
     assert r16["rel_inv_depth_median"] <= 0.01
     assert r16["wta_index_match"] >= 0.995
