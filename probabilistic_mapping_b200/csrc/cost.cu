@@ -126,9 +126,11 @@ __device__ __forceinline__ float2 sample2(const Src<SAMP>& src, const WarpConst&
     const bool ok0 = (w.x >= 0.0f) && (u.x >= 0.0f) && (u.x <= c.W1) && (v.x >= 0.0f) && (v.x <= c.H1);
     const bool ok1 = (w.y >= 0.0f) && (u.y >= 0.0f) && (u.y <= c.W1) && (v.y >= 0.0f) && (v.y <= c.H1);
     if constexpr (SAMP == kTex || SAMP == kTexF) {
-        // texel centres at +0.5, as the reference's tex2D(t, u + 0.5f, v + 0.5f) (calc_cost.cu:93)
-        const float s0 = tex2D<float>(src.t, u.x + 0.5f, v.x + 0.5f);
-        const float s1 = tex2D<float>(src.t, u.y + 0.5f, v.y + 0.5f);
+        // texel centres at +0.5, as the reference's tex2D(t, u + 0.5f, v + 0.5f) (calc_cost.cu:93),
+        // both planes' coordinates in one packed add each
+        const float2 uh = __fadd2_rn(u, f2(0.5f, 0.5f)), vh = __fadd2_rn(v, f2(0.5f, 0.5f));
+        const float s0 = tex2D<float>(src.t, uh.x, vh.x);
+        const float s1 = tex2D<float>(src.t, uh.y, vh.y);
         return f2(ok0 ? s0 : nan_f(), ok1 ? s1 : nan_f());
     } else if constexpr (SAMP == kQuad || SAMP == kQuadH) {
         // 0 <= u, v < 2^22: u + 1.5*2^23 rounded down is 1.5*2^23 + floor(u), exactly, and the
