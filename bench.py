@@ -39,7 +39,7 @@ PATHS = 8
 # and FP64 rounding would disagree.
 P1, P2, TAU, UNIQ = 0.003, 0.01, 3.5 / 255.0, 0.95
 N_KEYFRAMES = 4
-SAMPLERS = {"exact": 0, "texture": 1, "texture_f32": 2}   # PM_SAMPLER_* of the FP16 form
+SAMPLERS = {"exact": 0, "texture": 1, "texture_f32": 2}   # PM_SAMPLER_* (FP32 form: exact or texture_f32)
 
 
 def peaks():
