@@ -1,0 +1,45 @@
+"""The bench's roofline denominators (no GPU): the path-grouped algorithmic bytes per depth map,
+B_alg = (S+1) N + 3 e V + 8 V + 60 N, reproduce the published table for every configuration
+(FP32 and FP16 volumes), the cost kernel's algorithmic work is 144 flop per voxel and source,
+and the SGM stage's byte model counts what the pair kernels and the combine must move."""
+import os
+import sys
+
+import pytest
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+import bench  # noqa: E402
+
+# (W, H, D, S) -> (B_alg FP32, B_alg FP16) in MB, as published for this metric
+TABLE = {(320, 240, 64, 4): (103.3, 73.8), (640, 480, 128, 5): (806.7, 570.8),
+         (752, 480, 128, 5): (947.9, 670.7), (1280, 720, 192, 4): (3599.0, 2537.0)}
+
+
+@pytest.fixture
+def shape(monkeypatch):
+    def set_shape(W, H, D, S):
+        for k, v in dict(W=W, H=H, D=D, S=S).items():
+            monkeypatch.setattr(bench, k, v)
+    return set_shape
+
+
+@pytest.mark.parametrize("cfg", list(TABLE))
+def test_b_alg_matches_the_published_table(shape, cfg):
+    shape(*cfg)
+    for e, want in ((4, TABLE[cfg][0]), (2, TABLE[cfg][1])):
+        b_alg, _ = bench.algorithmic_bytes(e)
+        assert abs(b_alg / 1e6 - want) <= 0.05 * (1 if want < 1000 else 10), (cfg, e, b_alg)
+
+
+def test_cost_and_sgm_work_at_the_headline_shape(shape):
+    shape(640, 480, 128, 5)
+    N, V = 640 * 480, 640 * 480 * 128
+    flop, nbytes = bench.cost_kernel_work(4)
+    assert flop == 144 * V * 5 == 28_311_552_000
+    assert nbytes == 4 * V + 4 * N + 16 * N * 5            # volume once, reference, 5 quad images
+    assert bench.cost_kernel_work(2, texels=True)[1] == 2 * V + 4 * N + 4 * N * 5
+    _, sgm = bench.algorithmic_bytes(4)
+    # 8 paths read C and the reference; 4 pair volumes stored, reduced into (read + write) and
+    # read once by the combine; depth and index written
+    assert sgm == 8 * (4 * V + 4 * N) + 4 * (4 * V + 8 * V) + 4 * 4 * V + 8 * N
+    assert abs(sgm / V - 96) < 0.5                        # ~96 bytes per voxel for FP32
