@@ -115,6 +115,27 @@ def test_sgm_is_bounded_below_by_paths_times_cost(oracle_lib):
     assert (vol[~valid] == 0).all()   # COST_INF = 0 at pixels with an unmeasured plane
 
 
+@pytest.mark.parametrize("paths", [4, 8])
+def test_sgm_shifts_with_a_per_pixel_cost_shift(oracle_lib, paths):
+    """The FP16 form stores C(p, .) - c_p and adds c_p back once per path: L_r(p, d) = C(p, d) +
+    min(...) - min_k L_r(p - r, k) (sgm.cu:85-98) moves every L_r(p, .) by c_p when C(p, .) does,
+    and the next pixel's min(...) and min_k terms move together, so the sum over P paths moves
+    by exactly P c_p.  Checked on the FP64 transcription with a random shift at every valid
+    pixel (invalid pixels, with a plane never measured, keep cost -1)."""
+    fs, p = small_case(W=48, H=32, D=32, S=2)
+    p.num_paths = paths
+    cost, _ = oracle.calc_cost(p, fs.ref, fs.srcs, homographies(fs), "f64")
+    valid = (cost >= 0).all(axis=2)
+    shift = np.random.default_rng(3).random(valid.shape) * valid
+    vol = oracle.sgm(p, fs.ref, cost, "f64")
+    moved = oracle.sgm(p, fs.ref, np.where(valid[..., None], cost + shift[..., None], cost), "f64")
+    np.testing.assert_allclose(moved, vol + paths * shift[..., None] * valid[..., None], rtol=0, atol=1e-9)
+    # and so the winner-take-all index is unchanged
+    _, i0 = oracle.filter_cost(p, vol, "f64")
+    _, i1 = oracle.filter_cost(p, moved - paths * shift[..., None], "f64")
+    assert (i0 == i1).mean() > 0.999
+
+
 def test_fp32_and_fp64_instantiations_agree(oracle_lib):
     fs, p = small_case(W=96, H=64, D=64, S=3)
     homs = homographies(fs)
