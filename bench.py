@@ -161,17 +161,32 @@ def algorithmic_bytes(e: int):
 
 
 # Cost construction: 9 projective warps + 9 bilinear samples + 9 absolute differences per voxel
-# and source, 144 FP32 flop counting a division as one.
+# and source, 144 FP32 flop counting a division as one: per sample 8 for the warp (three
+# multiply-adds and the division), 6 for the bilinear interpolation (three lerps), 2 for the
+# absolute difference and its sum.  With a texture sampler the texture unit does the
+# interpolations (54 of the 144), so the SIMT pipes are credited with the other 90 only.
 FLOP_PER_VOXEL_SOURCE = 144
+FLOP_BILINEAR_PER_VOXEL_SOURCE = 9 * 6
 
 
 def cost_kernel_work(e: int, texels: bool = False):
     """Algorithmic flop and bytes of one cost-kernel launch (all S sources folded at once): the
     volume written once (e V), the reference image and the S source images read once (16-byte
-    quads for the exact sampler, 4-byte texels for the texture sampler)."""
+    quads for the exact sampler, 4-byte texels for the texture sampler).  Returns (flop on the
+    SIMT pipes, flop done by the texture unit, bytes)."""
     N = W * H
     V = N * D
-    return FLOP_PER_VOXEL_SOURCE * V * S, e * V + 4 * N + (4 if texels else 16) * N * S
+    tex_flop = FLOP_BILINEAR_PER_VOXEL_SOURCE * V * S if texels else 0
+    return FLOP_PER_VOXEL_SOURCE * V * S - tex_flop, tex_flop, e * V + 4 * N + (4 if texels else 16) * N * S
+
+
+def sgm_alg_bytes(e: int):
+    """The SGM + winner-take-all + fusion share of B_alg per map: two sweeps over the cost volume
+    (2 e V), the forward sweep's path sum written and read back once (8 V), the reference image
+    (4 N) and the fusion state and outputs (56 N)."""
+    N = W * H
+    V = N * D
+    return 2 * e * V + 8 * V + 4 * N + 56 * N
 
 
 def run_ours(args, rank, world, precision: str = "fp32", passes=("dev", "e2e", "stage")):
@@ -219,7 +234,7 @@ def run_ours(args, rank, world, precision: str = "fp32", passes=("dev", "e2e", "
         for i in range(args.warmup):
             step(i, ref, src, dep, var)
         m.enable_stage_timing(stage_timing)
-        stage = np.zeros(4)
+        stage = np.zeros(5)
         barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -235,7 +250,7 @@ def run_ours(args, rank, world, precision: str = "fp32", passes=("dev", "e2e", "
         return e0.elapsed_time(e1), stage / args.steps
 
     t_dev = t_e2e = 0.0
-    stage_ms = np.zeros(4)
+    stage_ms = np.zeros(5)
     clk = ClockSampler(dev)
     if "dev" in passes:
         with clk:
@@ -413,6 +428,91 @@ def mixed_main(args, rank, world):
         print(json.dumps(line))
 
 
+# The configuration the reference's own CUDA is compiled for (parameters.h: 640x480, 64 planes;
+# sgm2's 4 paths; parameters.cpp's penalties on 0..255 intensities; DEP_SAMPLE with plane 0 at
+# infinity), 5 sources, cost + SGM + winner-take-all (stereo_mapper.cpp:63-109), no fusion.
+REF_CFG = dict(W=640, H=480, D=64, S=5, f=520.0, seed=99)
+REF_CFG_NAME = ("640x480, 64 planes, 5 sources, 4-path SGM, reference parameters (pi1 8, pi2 24, tau_so 4, "
+                "q1 2, q2 3) on 0..255 intensities, plane 0 at inverse depth 0; initReference + 5 updates + "
+                "output (cost, SGM, winner-take-all), device-resident inputs")
+
+
+def ref_cfg_frames():
+    from probabilistic_mapping_b200 import scene
+    c = REF_CFG
+    return scene.make_frameset(c["W"], c["H"], c["f"], c["S"], seed=c["seed"]), 2.0 / (c["D"] - 1)
+
+
+def run_matched_reference_config(args, sampler: str):
+    """This library's plain FP32 form at the reference CUDA's own configuration (REF_CFG): ms per
+    depth map by CUDA events over args.steps maps after args.warmup, inputs resident on the device."""
+    import torch
+    from probabilistic_mapping_b200.mapper import StereoMapper
+    c = REF_CFG
+    fs, dep_sample = ref_cfg_frames()
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    m = StereoMapper(c["W"], c["H"], c["D"], rho0=0.0, intensity_scale=1.0, num_paths=4, p1=8.0, p2=24.0,
+                     tau_so=4.0, q1=2.0, q2=3.0, uniqueness_ratio=0.0, cost_mode=0, precision=0, device=dev,
+                     sampler=SAMPLERS[sampler])
+    m.initIntrinsic(fs.K, 0.0, dep_sample)
+    stream = torch.cuda.Stream(device=dev)
+    m.set_stream(stream.cuda_stream)
+    d_ref = torch.from_numpy(fs.ref).cuda()
+    d_src = [torch.from_numpy(np.ascontiguousarray(fs.srcs[s])).cuda() for s in range(c["S"])]
+    out = torch.empty((c["H"], c["W"]), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+
+    def one():
+        m.initReference(d_ref)
+        for s in range(c["S"]):
+            m.update(d_src[s], fs.R_ref, fs.T_ref, fs.R_srcs[s], fs.T_srcs[s])
+        m.output(out)
+
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        one()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    m.close()
+    return e0.elapsed_time(e1) / args.steps
+
+
+def reference_cuda_sample(reps: int):
+    """The reference's own CUDA (calc_cost.cu, sgm.cu, filter_cost.cu built unmodified for sm_100a
+    through a texture-object shim into oracle/_ref/libref_640x480x64.so) on REF_CFG: ms per depth
+    map (CUDA events inside the library), or None with the reason."""
+    import ctypes
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None, "no CUDA device"
+    except Exception as ex:   # noqa: BLE001
+        return None, f"torch unavailable: {ex}"
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_640x480x64.so")
+    if not os.path.exists(path):
+        return None, "oracle/_ref/libref_640x480x64.so was not built (the reference sources were absent at build time)"
+    import oracle
+    lib = ctypes.CDLL(path)
+    lib.ref_set_params(ctypes.c_float(8.0), ctypes.c_float(24.0), ctypes.c_float(4.0), ctypes.c_float(2.0),
+                       ctypes.c_float(3.0), ctypes.c_float(1.02))
+    fs, dep_sample = ref_cfg_frames()
+    ref = np.ascontiguousarray(fs.ref.astype(np.float32))
+    srcs = np.ascontiguousarray(fs.srcs.astype(np.float32))
+    homs = np.ascontiguousarray(np.stack([oracle.compose_homography(fs.K, fs.R_ref, fs.T_ref, fs.R_srcs[s],
+                                                                     fs.T_srcs[s]) for s in range(REF_CFG["S"])]
+                                         ).astype(np.float32))
+    ms = np.zeros(1, np.float32)
+    P = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))   # noqa: E731
+    st = lib.ref_bench(P(ref), P(srcs), REF_CFG["S"], P(homs), ctypes.c_float(dep_sample), int(reps), P(ms))
+    if st != 0:
+        return None, f"ref_bench returned CUDA error {st}"
+    return float(ms[0]), None
+
+
 def cpu_baseline_sample(threads: int | None = None, maps: int = 1):
     """FP64 oracle (all host threads) on full-size depth maps of the same workload."""
     import oracle
@@ -464,6 +564,8 @@ def main():
     ap.add_argument("--batch", type=int, default=16, help="sequences per batch (batched form)")
     ap.add_argument("--cost-mode", choices=["reference", "corrected"], default="reference")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-matched", action="store_true",
+                    help="skip the plain FP32 form at the reference CUDA's own configuration")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -487,6 +589,15 @@ def main():
                 "cpu_baseline": {"value": rate, "unit": "depth maps/s", "cores": cores, "kind": "port",
                                  "sample": f"{args.steps} full {W}x{H}x{D} depth maps (FP64 oracle, OpenMP)"},
                 "e2e": {"value": rate, "unit": "depth maps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        # the reference's own CUDA on this GPU, at the configuration it is compiled for; this
+        # library's plain FP32 form at the same configuration is in the other arm's line
+        # ("matched_reference_config")
+        ms, why = reference_cuda_sample(max(args.steps, 1))
+        line["reference_cuda"] = ({"ms_per_map": ms, "maps_per_s": 1000.0 / ms, "config": REF_CFG_NAME,
+                                   "source": "oracle/_ref/libref_640x480x64.so: the reference's calc_cost.cu, "
+                                             "sgm.cu and filter_cost.cu compiled unmodified for sm_100a through "
+                                             "a texture-object shim (texture references were removed in CUDA 12)"}
+                                  if ms else {"unavailable": why})
         print(json.dumps(line))
         return
 
@@ -531,17 +642,29 @@ def main():
         ms_per_step = t_dev / args.steps
     e = 2 if args.precision == "fp16" else 4
     b_alg, sgm_bytes = algorithmic_bytes(e)
+    b_sgm_alg = sgm_alg_bytes(e)
     peak_hbm, sm_mhz, peak_kind = peaks()
     peak_fp32 = fp32_peak_tflops(sm_mhz)
-    cost_ms, sgm_ms = float(stage_ms[0]), float(stage_ms[1])
-    cost_flop, cost_bytes = cost_kernel_work(e, sampler_name(args, args.precision) != "exact")
-    cost_tflops = cost_flop / (cost_ms / 1000.0) / 1e12 if cost_ms > 0 else None
+    cost_stage_ms, sgm_ms, fuse_ms = float(stage_ms[0]), float(stage_ms[1]), float(stage_ms[2])
+    cost_ms = float(stage_ms[4]) if stage_ms[4] > 0 else cost_stage_ms   # the cost kernel alone
+    texels = sampler_name(args, args.precision) != "exact"
+    simt_flop, tex_flop, cost_bytes = cost_kernel_work(e, texels)
+    cost_tflops = simt_flop / (cost_ms / 1000.0) / 1e12 if cost_ms > 0 else None
+    cost_tflops_all = (simt_flop + tex_flop) / (cost_ms / 1000.0) / 1e12 if cost_ms > 0 else None
     cost_gbs = cost_bytes / (cost_ms / 1000.0) / 1e9 if cost_ms > 0 else None
     sgm_gbs = sgm_bytes / (sgm_ms / 1000.0) / 1e9 if sgm_ms > 0 else None
+    sgm_alg_gbs = b_sgm_alg / ((sgm_ms + fuse_ms) / 1000.0) / 1e9 if sgm_ms > 0 else None
     map_s = 1.0 / (value / world)   # seconds per map per GPU
     # to_float (reference) + one conversion per source, cost (+ the FP16 volume's rebase), one
     # kernel per opposite-path pair, combine + winner-take-all, fusion transform + update
     launches_per_map = 1 + S + 1 + (1 if e == 2 else 0) + PATHS // 2 + 1 + 2
+    matched = None
+    if rank == 0 and not args.no_matched:
+        matched = {"config": REF_CFG_NAME,
+                   "ms_per_map_fp32_exact": run_matched_reference_config(args, "exact"),
+                   "ms_per_map_fp32_texture_f32": run_matched_reference_config(args, "texture_f32"),
+                   "note": "the reference's own CUDA at this configuration is timed by the reference arm "
+                           "(bench.py --impl reference, key reference_cuda)"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "depth maps/s", "n_gpus": world, "steps": args.steps,
@@ -557,32 +680,47 @@ def main():
             "plain_fp32": {"value": plain_value, "e2e": plain_e2e, "ms_per_map": t_plain / args.steps,
                            "unit": "depth maps/s"},
             "speedup_vs_plain_fp32": value / plain_value,
-            # the dominant kernel (cost_kernel, ~2/3 of a map) is FP32-ALU-bound, not HBM-bound
-            "roofline": {"bound": "fp32", "kernel": "cost_kernel" + (" (stage time includes the FP16 rebase pass)"
-                                                                    if e == 2 else ""),
+            # the dominant kernel (cost_kernel, more than half of a map) is FP32-ALU-bound, not
+            # HBM-bound; its time is the kernel alone (CUDA events on the mapper's stream, the FP16
+            # form's rebase pass excluded), its flop the algorithmic count on the SIMT pipes
+            "roofline": {"bound": "fp32", "kernel": "cost_kernel",
                          "achieved": cost_tflops, "peak": peak_fp32,
                          "unit": "TFLOP/s", "frac": (cost_tflops / peak_fp32) if cost_tflops else None,
                          "traffic": ncu_traffic("cost_kernel" if e == 4 and args.fp32_sampler == "exact"
                                                 else "cost_kernel_fp16" if e == 2 else None),
-                         "ms_per_launch": cost_ms,
-                         "algorithmic_flop_per_launch": cost_flop, "algorithmic_bytes_per_launch": cost_bytes,
+                         "ms_per_launch": cost_ms, "stage_ms_with_rebase": cost_stage_ms,
+                         "algorithmic_flop_per_launch": simt_flop,
+                         "texture_unit_flop_per_launch": tex_flop,
+                         "frac_counting_texture_interpolation": (cost_tflops_all / peak_fp32) if cost_tflops_all
+                         else None,
+                         "algorithmic_bytes_per_launch": cost_bytes,
                          "hbm_achieved_gbs": cost_gbs, "hbm_frac": (cost_gbs / peak_hbm) if cost_gbs else None,
                          "precision": args.precision,
-                         "peak_kind": f"derived: 148 SM x 128 lanes x 2 flop x {sm_mhz:.0f} MHz ({peak_kind} clock)"},
+                         "peak_kind": f"derived FP32 peak: 148 SM x 128 lanes x 2 flop x {sm_mhz:.0f} MHz "
+                                      f"({peak_kind} clock); no measured FP32 SIMT peak exists"},
+            # the SGM stage against the bytes this implementation moves, and the SGM + winner-take-
+            # all + fusion stages against their share of the path-grouped lower bound B_alg
             "roofline_sgm": {"bound": "hbm", "kernel": "sgm_pair_kernel x 4 + combine_kernel (winner-take-all)",
                              "achieved": sgm_gbs, "peak": peak_hbm, "unit": "GB/s",
                              "frac": (sgm_gbs / peak_hbm) if sgm_gbs else None,
-                             "algorithmic_bytes_per_map": sgm_bytes, "ms": sgm_ms, "peak_kind": peak_kind},
-            "map_roofline": {"b_alg_bytes": b_alg, "f_alg_flop": cost_flop, "ms_per_map_per_gpu": map_s * 1000,
+                             "implementation_bytes_per_map": sgm_bytes, "ms": sgm_ms, "peak_kind": peak_kind,
+                             "b_alg_share_bytes": b_sgm_alg, "b_alg_share_ms": sgm_ms + fuse_ms,
+                             "b_alg_share_achieved_gbs": sgm_alg_gbs,
+                             "b_alg_share_frac": (sgm_alg_gbs / peak_hbm) if sgm_alg_gbs else None,
+                             "implementation_over_algorithmic_bytes": sgm_bytes / (b_sgm_alg - 60 * W * H)},
+            "map_roofline": {"b_alg_bytes": b_alg, "f_alg_flop": simt_flop + tex_flop,
+                             "ms_per_map_per_gpu": map_s * 1000,
                              "frac_of_hbm": b_alg / map_s / 1e9 / peak_hbm,
-                             "frac_of_fp32": cost_flop / map_s / 1e12 / peak_fp32},
-            "stage_ms": {"cost": cost_ms, "sgm_wta": sgm_ms, "fusion": float(stage_ms[2]),
+                             "frac_of_fp32": (simt_flop + tex_flop) / map_s / 1e12 / peak_fp32},
+            "stage_ms": {"cost": cost_stage_ms, "cost_kernel": cost_ms, "sgm_wta": sgm_ms, "fusion": fuse_ms,
                          "copy_out": float(stage_ms[3]), "source": f"plain {args.precision} mapper, CUDA events"},
             "e2e": {"value": e2e, "unit": "depth maps/s", "h2d_bytes_per_step": B * (S + 1) * W * H,
                     "d2h_bytes_per_step": B * 2 * 4 * W * H},
             "gpu_launches": launches_per_map * B * args.steps,
             "clocks": clocks,
         }
+        if matched:
+            line["matched_reference_config"] = matched
         if tuning:
             line["sgm_schedule"] = {"pair_warps": tuning[0], "serial_pairs": tuning[1], "tuned_ms": tuning[2]}
         if not args.no_cpu_baseline:

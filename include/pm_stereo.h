@@ -177,7 +177,9 @@ PM_API pm_status pm_get_homography(pm_mapper* h, int i, float out[12]);
 /* Opt-in CUDA-event timers around the stages of pm_output / pm_output_fusion (recorded on the
  * handle's stream).  pm_get_stage_times synchronises and returns, in milliseconds, the
  * time of the last call's stages: [0] cost volume, [1] SGM + winner-take-all, [2] fusion,
- * [3] copy-out.  n is the capacity of ms; returns PM_ERR_BAD_STATE when timing is off. */
+ * [3] copy-out.  n is the capacity of ms; returns PM_ERR_BAD_STATE when timing is off.
+ * With n > PM_NUM_STAGES, ms[PM_NUM_STAGES] is the cost kernel alone: stage [0] without the
+ * FP16 form's rebase pass (equal to [0] for the FP32 form). */
 #define PM_NUM_STAGES 4
 PM_API pm_status pm_enable_stage_timing(pm_mapper* h, int enable);
 PM_API pm_status pm_get_stage_times(pm_mapper* h, float* ms, int n);
@@ -235,6 +237,9 @@ PM_API pm_status pm_batch_copy_output(pm_batch* b, int seq, float* depth, size_t
                                       size_t var_pitch);
 /* Winner-take-all depth (device, W*H float) of the last step of sequence seq. */
 PM_API pm_status pm_batch_wta_depth(pm_batch* b, int seq, const float** depth);
+/* Copies it into a caller buffer (host or device, byte pitch, 0 = packed) after waiting for the
+ * batch's stream. */
+PM_API pm_status pm_batch_copy_wta_depth(pm_batch* b, int seq, float* depth, size_t pitch);
 /* SGM schedule of sequence seq: scanlines per block of the path-pair kernel, serial (1) or
  * concurrent (0) path pairs, and the stage time the autotuner measured (ms; 0 if untuned). */
 PM_API pm_status pm_batch_tuning(pm_batch* b, int seq, int* pair_warps, int* serial_pairs, float* ms);
@@ -329,11 +334,27 @@ PM_API pm_status pm_stage_depth_fuse(int W, int H, const float pose[12], const f
  * library-owned __device__ array of 2^19 pixels (4 MiB, held by every GPU that loads the
  * library until exit); W*H above that returns PM_ERR_INVALID_ARGUMENT.  The array is cleared
  * at the start of each call and shared by all calls, so calls that overlap on the GPU race.
- * The first call on a device looks up the array's device address (cudaGetSymbolAddress);
- * make that first call before any stream capture. */
+ * The call uses the array of the CURRENT device: `stream` must belong to the current device's
+ * context (0 or the per-thread default stream are fine), else PM_ERR_INVALID_ARGUMENT.  The
+ * first call in a context looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  After a cudaDeviceReset the device has a new
+ * context, and the next call looks the address up again (again before any capture). */
 PM_API pm_status pm_stage_depth_fuse_noalloc(int W, int H, const float pose[12], const float cam[4],
                                              float* depth, float* const pre[4], float* const cur[4],
                                              int32_t* table, void* stream);
+
+/* The CPU fusion variant's step for a non-first keyframe, as outputFusionCPU runs it
+ * (stereo_mapper.cpp:741-784): the masks of :743-760 on `result`, depthFuseCPU (:568-587:
+ * transformMapCPU, holeFillingCPU, depthPreditCPU, depthUpdateCPU), then the re-mask of
+ * :773-784.  pose: R_p2c row-major then t_p2c, doubles (the reference's Eigen types); cam: fx,
+ * fy, cx, cy.  result: W*H, in = WTA depth, out = fused depth.  pre/cur: alpha, beta, mu, sigma
+ * (4 device pointers each, W*H floats; pre is modified in place as transformMapCPU does).
+ * table (optional): W*H uint32, the filled propagation table packed (y << 16) | x.  scratch:
+ * pm_stage_depth_fuse_cpu_path_scratch(W, H) bytes of device memory.  W, H < 65536. */
+PM_API size_t pm_stage_depth_fuse_cpu_path_scratch(int W, int H);
+PM_API pm_status pm_stage_depth_fuse_cpu_path(int W, int H, const double pose[12], const float cam[4],
+                                              float* result, float* const pre[4], float* const cur[4],
+                                              uint32_t* table, void* scratch, void* stream);
 
 /* convert (convert.cu:26-45).  flag != 0: linear -> pitched, else pitched -> linear.  The
  * pitch is in BYTES (the reference passed a byte step but indexed with it in floats). */

@@ -16,35 +16,7 @@
 #include <texture_fetch_functions.h>
 #include <cstring>
 
-#ifndef PM_REF_W
-#define PM_REF_W 640
-#endif
-#ifndef PM_REF_H
-#define PM_REF_H 480
-#endif
-#ifndef PM_REF_D
-#define PM_REF_D 64
-#endif
-
-// ---- parameters.h at the test shape (same names the reference declares) ----------------
-#define _parameters_h
-#define FLOAT_EPS 1e-5
-const int WIDTH = PM_REF_W;
-const int HEIGHT = PM_REF_H;
-extern int CASE;
-const int DEP_CNT = PM_REF_D;
-const float SAD_WEIGHT = 1.0f;
-const int MARGIN = 2;
-const int PATCH_SIZE = (2 * MARGIN + 1) * (2 * MARGIN + 1);
-extern float pi1;
-extern float pi2;
-extern float tau_so;
-extern float sgm_q1;
-extern float sgm_q2;
-extern float var_scale;
-const float DEP_INF_1 = 2000.0f;
-const float DEP_INF = 1000.0f;
-const float COST_INF = 0.0f;
+#include "ref_params.h"
 
 // ---- texture references on top of texture objects ---------------------------------------
 template <class T, int Dim, enum cudaTextureReadMode Mode>

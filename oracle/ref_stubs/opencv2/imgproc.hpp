@@ -1,0 +1,3 @@
+// TEST INFRASTRUCTURE -- see opencv.hpp.
+#pragma once
+#include "opencv.hpp"

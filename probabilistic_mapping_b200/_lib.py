@@ -112,6 +112,10 @@ SIGNATURES = {
     "pm_batch_output": (_I, [_VP, _I, _P(_VP), _P(_VP)]),
     "pm_batch_copy_output": (_I, [_VP, _I, _VP, _SZ, _VP, _SZ]),
     "pm_batch_wta_depth": (_I, [_VP, _I, _P(_VP)]),
+    "pm_batch_copy_wta_depth": (_I, [_VP, _I, _VP, _SZ]),
+    "pm_stage_depth_fuse_cpu_path_scratch": (_SZ, [_I, _I]),
+    "pm_stage_depth_fuse_cpu_path": (_I, [_I, _I, _P(ctypes.c_double), _P(ctypes.c_float), _VP, _P(_VP), _P(_VP),
+                                          _VP, _VP, _VP]),
     "pm_batch_tuning": (_I, [_VP, _I, _P(_I), _P(_I), _P(_F)]),
     "pm_batch_stream": (_VP, [_VP]),
     "pm_batch_last_error": (ctypes.c_char_p, [_VP]),

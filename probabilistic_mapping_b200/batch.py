@@ -118,6 +118,15 @@ class StereoBatch:
                     "pm_batch_copy_output")
         return depth, variance
 
+    def wta_depth(self, seq: int, depth=None):
+        """Winner-take-all depth of the last step (before fusion), copied into a numpy array or a
+        torch tensor (host or CUDA); a new numpy array when not given."""
+        H, W = self.shapes[seq]
+        if depth is None:
+            depth = np.empty((H, W), np.float32)
+        self._check(self.lib.pm_batch_copy_wta_depth(self.b, seq, _addr(depth), 0), "pm_batch_copy_wta_depth")
+        return depth
+
     def tuning(self, seq: int):
         w, s, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
         self._check(self.lib.pm_batch_tuning(self.b, seq, ctypes.byref(w), ctypes.byref(s), ctypes.byref(ms)),

@@ -72,6 +72,8 @@ struct pm_mapper {
     bool timing = false;
     cudaEvent_t ev[PM_NUM_STAGES + 1] = {};
     bool ev_valid[PM_NUM_STAGES] = {};
+    cudaEvent_t ev_cost_kernel = nullptr;   // end of the cost kernel alone (stage 0 minus the rebase)
+    bool ev_cost_valid = false;
 };
 
 namespace pm {
@@ -283,6 +285,10 @@ pm_status evaluate_cost(pm_mapper* h, bool into_state) {
     a.cost = h->d_cost;
     a.offset = h->d_off;
     a.block_offset = h->d_boff;
+    if (h->timing && !into_state) {
+        a.kernel_done = h->ev_cost_kernel;
+        h->ev_cost_valid = true;
+    }
     if (into_state || h->has_state) {
         if (!h->d_cnt) PM_CK(h, cudaMalloc(&h->d_cnt, sizeof(float) * (size_t)c.width * c.height * c.num_planes));
         a.cnt = h->d_cnt;
@@ -368,6 +374,7 @@ void release(pm_mapper* h) {
     cudaFree(h->d_ctab);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
+    if (h->ev_cost_kernel) cudaEventDestroy(h->ev_cost_kernel);
     for (int g = 0; g < 3; ++g) {
         if (h->side.stream[g]) cudaStreamDestroy(h->side.stream[g]);
         if (h->side.join[g]) cudaEventDestroy(h->side.join[g]);
@@ -548,6 +555,7 @@ pm_status pm_output(pm_mapper* h, float* depth, size_t pitch) {
     if (!depth) return fail(h, PM_ERR_INVALID_ARGUMENT, "depth pointer is NULL");
     DeviceGuard g(h->cfg.device);
     for (bool& v : h->ev_valid) v = false;
+    h->ev_cost_valid = false;
     mark(h, 0);
     pm_status st = evaluate_cost(h, false);
     mark_done(h, 0);
@@ -569,6 +577,7 @@ pm_status pm_output_case(pm_mapper* h, int output_case, float* result, size_t pi
     DeviceGuard g(h->cfg.device);
     const pm_config& c = h->cfg;
     for (bool& v : h->ev_valid) v = false;
+    h->ev_cost_valid = false;
     mark(h, 0);
     pm_status st = evaluate_cost(h, false);
     mark_done(h, 0);
@@ -605,6 +614,7 @@ pm_status pm_output_fusion(pm_mapper* h, float* depth, size_t depth_pitch, float
     const int W = h->cfg.width, H = h->cfg.height;
     const size_t N = (size_t)W * H;
     for (bool& v : h->ev_valid) v = false;
+    h->ev_cost_valid = false;
     mark(h, 0);
     pm_status st = evaluate_cost(h, false);
     mark_done(h, 0);
@@ -743,10 +753,13 @@ pm_status pm_get_homography(pm_mapper* h, int i, float out[12]) {
 pm_status pm_enable_stage_timing(pm_mapper* h, int enable) {
     if (!h) return PM_ERR_INVALID_ARGUMENT;
     DeviceGuard g(h->cfg.device);
-    if (enable && !h->ev[0])
+    if (enable && !h->ev[0]) {
         for (auto& e : h->ev) PM_CK(h, cudaEventCreate(&e));
+        PM_CK(h, cudaEventCreate(&h->ev_cost_kernel));
+    }
     h->timing = enable != 0;
     for (bool& v : h->ev_valid) v = false;
+    h->ev_cost_valid = false;
     return PM_OK;
 }
 
@@ -758,6 +771,11 @@ pm_status pm_get_stage_times(pm_mapper* h, float* ms, int n) {
     for (int i = 0; i < n && i < PM_NUM_STAGES; ++i) {
         ms[i] = 0.0f;
         if (h->ev_valid[i]) PM_CK(h, cudaEventElapsedTime(&ms[i], h->ev[i], h->ev[i + 1]));
+    }
+    if (n > PM_NUM_STAGES) {
+        ms[PM_NUM_STAGES] = 0.0f;
+        if (h->ev_valid[0] && h->ev_cost_valid)
+            PM_CK(h, cudaEventElapsedTime(&ms[PM_NUM_STAGES], h->ev[0], h->ev_cost_kernel));
     }
     return PM_OK;
 }
@@ -915,6 +933,49 @@ pm_status pm_stage_depth_fuse(int W, int H, const float pose[12], const float ca
     f.ztable = reinterpret_cast<unsigned long long*>(ztable);
     f.table = table;
     return launch_fuse_gpu(f, (cudaStream_t)stream) == cudaSuccess ? PM_OK : PM_ERR_CUDA;
+}
+
+// Scratch of pm_stage_depth_fuse_cpu_path, W*H each: mask (u8), original mean (f32), list head
+// and link (i32), initial table (u32); sections 256-byte aligned.
+static size_t cpu_path_section(size_t n, size_t elem) { return (n * elem + 255) & ~(size_t)255; }
+
+size_t pm_stage_depth_fuse_cpu_path_scratch(int W, int H) {
+    if (W <= 0 || H <= 0) return 0;
+    const size_t n = (size_t)W * H;
+    return cpu_path_section(n, 1) + 4 * cpu_path_section(n, 4);
+}
+
+pm_status pm_stage_depth_fuse_cpu_path(int W, int H, const double pose[12], const float cam[4], float* result,
+                                       float* const pre[4], float* const cur[4], uint32_t* table, void* scratch,
+                                       void* stream) {
+    if (W <= 0 || H <= 0 || W >= 65536 || H >= 65536 || !pose || !cam || !result || !pre || !cur || !scratch)
+        return PM_ERR_INVALID_ARGUMENT;
+    if (!finite_n(pose, 12)) return PM_ERR_INVALID_ARGUMENT;
+    FuseCpuLaunch f;
+    std::memset(&f, 0, sizeof f);
+    f.W = W;
+    f.H = H;
+    for (int i = 0; i < 12; ++i) f.pose[i] = pose[i];
+    for (int i = 0; i < 4; ++i) f.cam[i] = cam[i];
+    f.result = result;
+    for (int k = 0; k < 4; ++k) {
+        if (!pre[k] || !cur[k]) return PM_ERR_INVALID_ARGUMENT;
+        f.pre[k] = pre[k];
+        f.cur[k] = cur[k];
+    }
+    f.table = table;
+    const size_t n = (size_t)W * H;
+    unsigned char* p = static_cast<unsigned char*>(scratch);
+    f.mask = reinterpret_cast<uint8_t*>(p);
+    p += cpu_path_section(n, 1);
+    f.orig_mu = reinterpret_cast<float*>(p);
+    p += cpu_path_section(n, 4);
+    f.head = reinterpret_cast<int*>(p);
+    p += cpu_path_section(n, 4);
+    f.next = reinterpret_cast<int*>(p);
+    p += cpu_path_section(n, 4);
+    f.tab0 = reinterpret_cast<uint32_t*>(p);
+    return launch_fuse_cpu_variant(f, (cudaStream_t)stream) == cudaSuccess ? PM_OK : PM_ERR_CUDA;
 }
 
 pm_status pm_stage_convert(int W, int H, const float* in, float* out, int flag, size_t pitch, void* stream) {

@@ -671,6 +671,21 @@ pm_status pm_batch_wta_depth(pm_batch* b, int seq, const float** depth) {
     return PM_OK;
 }
 
+pm_status pm_batch_copy_wta_depth(pm_batch* b, int seq, float* depth, size_t pitch) {
+    const float* d = nullptr;
+    pm_status st = pm_batch_wta_depth(b, seq, &d);
+    if (st != PM_OK) return st;
+    if (!depth) return bfail(b, PM_ERR_INVALID_ARGUMENT, "null destination");
+    const Seq& q = b->seqs[seq];
+    const size_t row = sizeof(float) * (size_t)q.cfg.width;
+    if (pitch == 0) pitch = row;
+    if (pitch < row) return bfail(b, PM_ERR_INVALID_ARGUMENT, "output pitch too small");
+    DevGuard dg(b->device);
+    PB_CK(b, cudaStreamSynchronize(b->run));
+    PB_CK(b, cudaMemcpy2D(depth, pitch, d, row, row, (size_t)q.cfg.height, cudaMemcpyDefault));
+    return PM_OK;
+}
+
 pm_status pm_batch_tuning(pm_batch* b, int seq, int* pair_warps, int* serial_pairs, float* ms) {
     if (!b) return PM_ERR_INVALID_ARGUMENT;
     if (seq < 0 || seq >= (int)b->seqs.size()) return bfail(b, PM_ERR_INVALID_ARGUMENT, "no sequence %d", seq);

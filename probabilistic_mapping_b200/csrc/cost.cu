@@ -495,6 +495,7 @@ cudaError_t launch_cost(const CostLaunch& a, cudaStream_t s) {
     if (a.mode == 0) e = a.cost_half ? launch_q<0, true>(a, grid, s) : launch_q<0, false>(a, grid, s);
     else e = a.cost_half ? launch_q<1, true>(a, grid, s) : launch_q<1, false>(a, grid, s);
     if (e != cudaSuccess) return e;
+    if (a.kernel_done && (e = cudaEventRecord(a.kernel_done, s)) != cudaSuccess) return e;
     if (a.cost_half) {
         const long np = (long)a.W * a.H;
         const unsigned blocks = (unsigned)((np + 8 * RB - 1) / (8 * RB));

@@ -10,6 +10,8 @@
 // exits, and every call shares it: the kernels clear it at the start of each call, and calls
 // that run at the same time on the GPU (two streams, two host threads) overwrite each other's
 // z-buffer and give wrong results.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "pm_device.cuh"
@@ -21,25 +23,88 @@ namespace {
 constexpr size_t kNoAllocMaxPixels = size_t(1) << 19;
 static __device__ __align__(256) unsigned long long g_noalloc_ztable[kNoAllocMaxPixels];
 
-// Device address of the array per device ordinal, looked up once per device.  In host code the
-// symbol g_noalloc_ztable only names a host-side stand-in, so its address must come from
-// cudaGetSymbolAddress with the device current before a kernel may use it.
+// Device address of the array per device ordinal, with the id of the context it was looked up
+// in.  In host code the symbol g_noalloc_ztable only names a host-side stand-in, so its address
+// must come from cudaGetSymbolAddress with the device current before a kernel may use it.  The
+// address belongs to one context: after a cudaDeviceReset the device gets a new primary context
+// (a new id) and the library image is loaded again, so the address is looked up again.
 constexpr int kMaxDevices = 128;
 std::mutex g_setup_mu;
-unsigned long long* g_ztable_dev[kMaxDevices] = {};
+struct Slot {
+    unsigned long long ctx_id = 0;   // 0: not looked up yet (context ids start at 1)
+    unsigned long long* ptr = nullptr;
+};
+Slot g_slot[kMaxDevices];
 
-pm_status ztable_for_current_device(unsigned long long** out) {
+// The three driver calls used here, looked up through the runtime (cudaGetDriverEntryPoint-
+// ByVersion) so that the library needs no link-time dependency on libcuda.
+struct DriverCalls {
+    CUresult (*ctx_get_current)(CUcontext*) = nullptr;
+    CUresult (*ctx_get_id)(CUcontext, unsigned long long*) = nullptr;
+    CUresult (*stream_get_ctx)(CUstream, CUcontext*) = nullptr;
+    bool ok = false;
+};
+DriverCalls g_drv;   // filled under g_setup_mu
+
+bool driver_calls() {
+    if (g_drv.ok) return true;
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !p)
+        return false;
+    g_drv.ctx_get_current = reinterpret_cast<CUresult (*)(CUcontext*)>(p);
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !p)
+        return false;
+    g_drv.ctx_get_id = reinterpret_cast<CUresult (*)(CUcontext, unsigned long long*)>(p);
+    if (cudaGetDriverEntryPointByVersion("cuStreamGetCtx", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !p)
+        return false;
+    g_drv.stream_get_ctx = reinterpret_cast<CUresult (*)(CUstream, CUcontext*)>(p);
+    g_drv.ok = true;
+    return true;
+}
+
+// The current context and its id; null when the runtime has not made one current yet.
+CUresult current_context(CUcontext* ctx, unsigned long long* id) {
+    *ctx = nullptr;
+    *id = 0;
+    CUresult r = g_drv.ctx_get_current(ctx);
+    if (r != CUDA_SUCCESS || !*ctx) return r;
+    return g_drv.ctx_get_id(*ctx, id);
+}
+
+pm_status ztable_for_current_device(CUcontext* ctx_out, unsigned long long** out) {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess) return PM_ERR_CUDA;
     if (dev < 0 || dev >= kMaxDevices) return PM_ERR_UNSUPPORTED;
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_ztable_dev[dev]) {
+    if (!driver_calls()) return PM_ERR_CUDA;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (current_context(&ctx, &id) != CUDA_SUCCESS) return PM_ERR_CUDA;
+    if (!ctx || id != g_slot[dev].ctx_id) {
+        // cudaGetSymbolAddress makes the device's primary context current if it is not yet
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_ztable) != cudaSuccess || !p) return PM_ERR_CUDA;
-        g_ztable_dev[dev] = static_cast<unsigned long long*>(p);
+        if (current_context(&ctx, &id) != CUDA_SUCCESS || !ctx) return PM_ERR_CUDA;
+        g_slot[dev].ctx_id = id;
+        g_slot[dev].ptr = static_cast<unsigned long long*>(p);
     }
-    *out = g_ztable_dev[dev];
+    *ctx_out = ctx;
+    *out = g_slot[dev].ptr;
     return PM_OK;
+}
+
+// The stream must run in the current context: the array's address is that context's.
+bool stream_in_context(void* stream, CUcontext ctx) {
+    const uintptr_t s = reinterpret_cast<uintptr_t>(stream);
+    if (s == 0 || s == reinterpret_cast<uintptr_t>(cudaStreamLegacy) ||
+        s == reinterpret_cast<uintptr_t>(cudaStreamPerThread))
+        return true;   // the default streams belong to the current context
+    CUcontext sctx = nullptr;
+    return g_drv.stream_get_ctx(static_cast<CUstream>(stream), &sctx) == CUDA_SUCCESS && sctx == ctx;
 }
 
 }  // namespace
@@ -62,8 +127,10 @@ extern "C" pm_status pm_stage_depth_fuse_noalloc(int W, int H, const float pose[
     }
     f.table = table;
     f.variance = nullptr;
-    pm_status st = ztable_for_current_device(&f.ztable);
+    CUcontext ctx = nullptr;
+    pm_status st = ztable_for_current_device(&ctx, &f.ztable);
     if (st != PM_OK) return st;
+    if (!stream_in_context(stream, ctx)) return PM_ERR_INVALID_ARGUMENT;
     // launch_fuse_gpu clears the z-buffer on `stream` before the kernels use it
     return pm::launch_fuse_gpu(f, (cudaStream_t)stream) == cudaSuccess ? PM_OK : PM_ERR_CUDA;
 }

@@ -42,6 +42,7 @@ struct CostLaunch {
     float* cnt;            // running count (incremental mode) or nullptr
     uint8_t* invalid;      // W*H, 1 where a plane was never measured (optional)
     int incremental;       // start from (cost, cnt) in memory instead of (-1, 0)
+    cudaEvent_t kernel_done = nullptr;   // recorded right after the cost kernel (before the rebase)
 };
 cudaError_t launch_cost(const CostLaunch& a, cudaStream_t s);
 

@@ -150,9 +150,10 @@ class StereoMapper:
         self._check(self.lib.pm_enable_stage_timing(self.h, int(enable)), "pm_enable_stage_timing")
 
     def stage_times(self) -> np.ndarray:
-        """Milliseconds of [cost, sgm+wta, fusion, copy-out] of the last output call."""
-        out = np.zeros(4, np.float32)
-        self._check(self.lib.pm_get_stage_times(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), 4),
+        """Milliseconds of [cost, sgm+wta, fusion, copy-out, cost kernel alone] of the last output call
+        (the last entry is the cost stage without the FP16 form's rebase pass)."""
+        out = np.zeros(5, np.float32)
+        self._check(self.lib.pm_get_stage_times(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), 5),
                     "pm_get_stage_times")
         return out
 

@@ -34,10 +34,16 @@ def test_b_alg_matches_the_published_table(shape, cfg):
 def test_cost_and_sgm_work_at_the_headline_shape(shape):
     shape(640, 480, 128, 5)
     N, V = 640 * 480, 640 * 480 * 128
-    flop, nbytes = bench.cost_kernel_work(4)
-    assert flop == 144 * V * 5 == 28_311_552_000
+    flop, tex_flop, nbytes = bench.cost_kernel_work(4)
+    assert flop == 144 * V * 5 == 28_311_552_000 and tex_flop == 0
     assert nbytes == 4 * V + 4 * N + 16 * N * 5            # volume once, reference, 5 quad images
-    assert bench.cost_kernel_work(2, texels=True)[1] == 2 * V + 4 * N + 4 * N * 5
+    simt, tex, nb16 = bench.cost_kernel_work(2, texels=True)
+    assert nb16 == 2 * V + 4 * N + 4 * N * 5
+    # the texture unit takes the nine bilinear interpolations (6 flop each) off the SIMT pipes
+    assert tex == 54 * V * 5 and simt + tex == 144 * V * 5
+    # the SGM + winner-take-all + fusion share of B_alg: two sweeps over C, the forward sum
+    # written and read once, the reference image, fusion state and outputs
+    assert bench.sgm_alg_bytes(4) == 16 * V + 60 * N and bench.sgm_alg_bytes(2) == 12 * V + 60 * N
     _, sgm = bench.algorithmic_bytes(4)
     # 8 paths read C and the reference; 4 pair volumes stored, reduced into (read + write) and
     # read once by the combine; depth and index written

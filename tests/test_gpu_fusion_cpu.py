@@ -99,3 +99,51 @@ def test_fusion_step_times_640x480():
         with open(os.path.join(out, "fusion_640x480.json"), "w") as f:
             json.dump(report, f, indent=1)
     assert all(v > 0 for v in report.values())
+
+
+def test_cpu_variant_kernels_match_the_reference_itself():
+    """pm_stage_depth_fuse_cpu_path against the reference's own outputFusionCPU (compiled
+    unmodified on the host; tests/golden/ref_cpu_fusion_80x60x32.npz) over a 6-keyframe sequence:
+    every propagation table identical, every fused result and the final state within 1e-4
+    relative (CUDA's expf against the host's), and identical wherever the update's
+    transcendental does not enter (zero / non-fused pixels)."""
+    import ctypes
+    import os
+    import torch
+    from probabilistic_mapping_b200 import _lib as L
+    lib = L.load()
+    here = os.path.dirname(os.path.abspath(__file__))
+    z = dict(np.load(os.path.join(here, "golden", "ref_cpu_fusion_80x60x32.npz")))
+    F, H, W = z["in_wta"].shape
+    N = W * H
+    K = z["in_K"]
+    cam = np.array([K[0, 0], K[1, 1], K[0, 2], K[1, 2]], np.float32)
+    state = [[torch.zeros(N, dtype=torch.float32, device="cuda") for _ in range(4)] for _ in range(2)]
+    table = torch.zeros(N, dtype=torch.int32, device="cuda")
+    scratch = torch.empty(lib.pm_stage_depth_fuse_cpu_path_scratch(W, H), dtype=torch.uint8, device="cuda")
+    pre = 0
+    for k in range(F):
+        if k == 0:
+            continue   # the first keyframe only zeroes the state (done above)
+        rel = oracle.relative_pose(z["in_R"][k], z["in_t"][k], z["in_R"][k - 1], z["in_t"][k - 1])
+        res = torch.from_numpy(np.ascontiguousarray(z["in_wta"][k].reshape(-1))).cuda()
+        prep = (ctypes.c_void_p * 4)(*[t.data_ptr() for t in state[pre]])
+        curp = (ctypes.c_void_p * 4)(*[t.data_ptr() for t in state[pre ^ 1]])
+        st = lib.pm_stage_depth_fuse_cpu_path(W, H, rel.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                              cam.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                              ctypes.c_void_p(res.data_ptr()), prep, curp,
+                                              ctypes.c_void_p(table.data_ptr()), ctypes.c_void_p(scratch.data_ptr()),
+                                              None)
+        assert st == 0
+        torch.cuda.synchronize()
+        got = res.cpu().numpy().reshape(H, W)
+        want = z["ref_fused"][k]
+        assert (table.cpu().numpy().view(np.uint32) == z["ref_tables"][k]).all(), f"keyframe {k}: table"
+        assert ((got == 0) == (want == 0)).all(), f"keyframe {k}: fused / rejected pixels differ"
+        np.testing.assert_allclose(got, want, rtol=1e-4, atol=0, err_msg=f"keyframe {k}")
+        pre ^= 1
+    assert pre == int(z["ref_final_pre_index"])
+    for h in range(2):
+        for i, name in enumerate(("alpha", "beta", "mu", "sigma")):
+            np.testing.assert_allclose(state[h][i].cpu().numpy(), z["ref_state"][i][h], rtol=1e-4, atol=1e-6,
+                                       err_msg=f"{name}[{h}]")

@@ -64,14 +64,47 @@ def run(lib, case, noalloc):
 
 
 def test_noalloc_fusion_matches_allocating_entry_point_twice(pm_lib):
-    for seed in (5, 6):   # two calls in a row, different scenes and poses
-        case = inputs(seed)
+    # two calls in a row on different scenes and poses; the first image is the larger one, so
+    # the second call runs over an array that still holds the first call's z-buffer beyond its
+    # own pixels.  Both entry points run the same kernels on the same inputs: bit-identical.
+    for seed, (W, H) in ((5, (128, 96)), (6, (96, 64))):
+        case = inputs(seed, W, H)
         want = run(pm_lib, case, noalloc=False)
         got = run(pm_lib, case, noalloc=True)
         assert (got[1] == want[1]).all(), "propagation tables differ"
         assert (want[1] != 0).mean() > 0.5
         for g, w in zip(got[:1] + got[2:], want[:1] + want[2:]):
-            np.testing.assert_allclose(g, w, rtol=1e-4, atol=1e-5)
+            assert (g.view(np.uint32) == w.view(np.uint32)).all(), "fusion outputs differ"
+
+
+def test_noalloc_rejects_a_stream_of_another_context(pm_lib):
+    # a stream created in a context other than the current one: the array address would be the
+    # wrong context's, so the call refuses it before any GPU work
+    import ctypes.util
+    cu = ctypes.CDLL(ctypes.util.find_library("cuda") or "libcuda.so.1")
+    torch.cuda.init()
+    dev = ctypes.c_int(0)
+    assert cu.cuDeviceGet(ctypes.byref(dev), torch.cuda.current_device()) == 0
+    ctx = ctypes.c_void_p()
+    assert cu.cuCtxCreate_v2(ctypes.byref(ctx), 0, dev) == 0   # made current by the call
+    try:
+        stream = ctypes.c_void_p()
+        assert cu.cuStreamCreate(ctypes.byref(stream), 0) == 0
+        popped = ctypes.c_void_p()
+        assert cu.cuCtxPopCurrent_v2(ctypes.byref(popped)) == 0   # back to the primary context
+        W, H, pose, cam, depth, state = inputs(5, 64, 48)
+        N = W * H
+        bufs = [torch.zeros(N, dtype=torch.float32, device="cuda") for _ in range(10)]
+        ptrs = (ctypes.c_void_p * 4)(*[t.data_ptr() for t in bufs[2:6]])
+        ptrs2 = (ctypes.c_void_p * 4)(*[t.data_ptr() for t in bufs[6:10]])
+        st = pm_lib.pm_stage_depth_fuse_noalloc(W, H, fptr(pose), fptr(cam), vp(bufs[0]), ptrs, ptrs2,
+                                                ctypes.c_void_p(0), stream)
+        assert st == 1   # PM_ERR_INVALID_ARGUMENT
+        assert cu.cuCtxPushCurrent_v2(ctx) == 0
+        assert cu.cuStreamDestroy_v2(stream) == 0
+        assert cu.cuCtxPopCurrent_v2(ctypes.byref(popped)) == 0
+    finally:
+        assert cu.cuCtxDestroy_v2(ctx) == 0
 
 
 def test_noalloc_rejects_images_beyond_its_array(pm_lib):
