@@ -152,11 +152,11 @@ def algorithmic_bytes(e: int):
     N = W * H
     V = N * D
     b_alg = (S + 1) * N + 3 * e * V + 8 * V + 60 * N
-    # every path reads C and the reference image; each opposite-path pair stores one FP32 volume
-    # and adds into it once (a read and a write); the combine reads the pair volumes and writes
-    # depth and index
+    # every path reads C and the reference image; each opposite-path pair stores one volume (FP32,
+    # or FP16 in the FP16 form, the element size of its cost volume) and adds into it once (a read
+    # and a write); the combine reads the pair volumes and writes depth and index
     pairs = PATHS // 2
-    sgm_pass = PATHS * (e * V + 4 * N) + pairs * (4 * V + 8 * V) + pairs * 4 * V + 8 * N
+    sgm_pass = PATHS * (e * V + 4 * N) + pairs * (e * V + 2 * e * V) + pairs * e * V + 8 * N
     return b_alg, sgm_pass
 
 

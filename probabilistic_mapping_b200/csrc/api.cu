@@ -313,6 +313,8 @@ pm_status run_sgm_filter(pm_mapper* h) {
     a.ref = h->d_ref;
     for (int r = 0; r < c.num_paths / 2; ++r) a.part[r] = h->d_part[r];
     a.total = h->store_sgm ? h->d_part[0] : nullptr;   // combine reads part[0] of a pixel before writing it
+    // the FP16 form keeps its pair volumes in FP16, unless the FP32 sum is to be stored over them
+    a.part_half = a.cost_half && !h->store_sgm;
     a.depth = h->d_depth;
     a.depth_pitch = sizeof(float) * (size_t)c.width;
     a.index = h->d_idx;
@@ -592,6 +594,7 @@ pm_status pm_output_case(pm_mapper* h, int output_case, float* result, size_t pi
         a.offset = h->d_off;
         a.ref = h->d_ref;
         for (int r = 0; r < c.num_paths / 2; ++r) a.part[r] = h->d_part[r];
+        a.part_half = a.cost_half;
         a.depth = h->d_fused;
         a.depth_pitch = sizeof(float) * (size_t)c.width;
         a.index = h->d_idx;

@@ -204,6 +204,7 @@ SgmLaunch sgm_launch(const Seq& q, const LaneBufs& l, int priority) {
     a.cost_half = c.precision == PM_PREC_FP16;
     a.ref = q.d_ref;
     for (int r = 0; r < c.num_paths / 2; ++r) a.part[r] = l.part[r];
+    a.part_half = a.cost_half;   // the FP16 form keeps its pair volumes in FP16
     a.W = c.width;
     a.H = c.height;
     a.D = c.num_planes;

@@ -123,8 +123,12 @@ __device__ __forceinline__ float2 sample2(const Src<SAMP>& src, const WarpConst&
         r = rcp_warp2(w);
     }
     const float2 u = __fmul2_rn(nx, r), v = __fmul2_rn(ny, r);
-    const bool ok0 = (w.x >= 0.0f) && (u.x >= 0.0f) && (u.x <= c.W1) && (v.x >= 0.0f) && (v.x <= c.H1);
-    const bool ok1 = (w.y >= 0.0f) && (u.y >= 0.0f) && (u.y <= c.W1) && (v.y >= 0.0f) && (v.y <= c.H1);
+    // u + 0 turns -0 into +0 (which the reference's u < 0 accepts); then 0 <= u <= W-1 is one
+    // unsigned compare of the bit patterns: negative values and NaN have patterns above W-1's
+    const float2 uz = __fadd2_rn(u, f2(0.0f, 0.0f)), vz = __fadd2_rn(v, f2(0.0f, 0.0f));
+    const unsigned Wb = __float_as_uint(c.W1), Hb = __float_as_uint(c.H1);
+    const bool ok0 = (w.x >= 0.0f) && (__float_as_uint(uz.x) <= Wb) && (__float_as_uint(vz.x) <= Hb);
+    const bool ok1 = (w.y >= 0.0f) && (__float_as_uint(uz.y) <= Wb) && (__float_as_uint(vz.y) <= Hb);
     if constexpr (SAMP == kTex || SAMP == kTexF) {
         // texel centres at +0.5, as the reference's tex2D(t, u + 0.5f, v + 0.5f) (calc_cost.cu:93),
         // both planes' coordinates in one packed add each
@@ -340,12 +344,11 @@ __global__ void __launch_bounds__(NT, 3) cost_kernel(const CostLaunch a) {
                     d[7] = sub2(Rld, Ld);
                     d[8] = sub2(Rru, Ru);
                 }
-                float tx = fabsf(d[0].x), ty = fabsf(d[0].y);
+                // the nine terms in the reference's order, both planes in one packed add each
+                float2 t2 = f2(fabsf(d[0].x), fabsf(d[0].y));
 #pragma unroll
-                for (int k = 1; k < 9; ++k) {
-                    tx = __fadd_rn(tx, fabsf(d[k].x));
-                    ty = __fadd_rn(ty, fabsf(d[k].y));
-                }
+                for (int k = 1; k < 9; ++k) t2 = __fadd2_rn(t2, f2(fabsf(d[k].x), fabsf(d[k].y)));
+                const float tx = t2.x, ty = t2.y;
                 float2* const ap = accp + o * (TXU * SP / 2);
                 float2* const cp = cntp + o * (TXU * SP / 2);
                 float2 av = *ap, nv = *cp;

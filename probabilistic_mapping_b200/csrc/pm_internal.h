@@ -62,7 +62,9 @@ struct SgmLaunch {
     const void* cost;      // W*H*D float or __half
     int cost_half;
     const float* ref;      // W*H scaled reference image (path gradient D1, sgm.cu:75)
-    float* part[4];        // W*H*D volume of each opposite-path pair (num_paths / 2 of them): P_2p + P_2p+1
+    void* part[4];         // W*H*D volume of each opposite-path pair (num_paths / 2 of them): P_2p + P_2p+1,
+                           // float, or __half when part_half
+    int part_half;         // FP16 form: the pair volumes hold FP16 values (sums rounded to FP16)
     float* total;          // W*H*D complete sum (may alias part[0]); nullptr: not stored
     const float* offset;   // W*H per-pixel shift of an FP16 cost volume (see CostLaunch), or nullptr
     int W, H, D, num_paths;

@@ -8,7 +8,12 @@
 //     d-1 / d+1 come from one shuffle each, and the minimum over planes is a single
 //     redux.sync.min.f32;
 //   * the per-pixel plane vector (contiguous in the plane-innermost layout) is streamed with
-//     cp.async into a per-lane shared-memory ring PF steps ahead of the recurrence;
+//     cp.async into a per-lane shared-memory ring PF steps ahead of the recurrence; the reference
+//     pixels of a scanline are read 32 steps at a time, one per lane, and become one ballot of
+//     adaptive-penalty flags, so a step costs a bit test instead of a load and a comparison;
+//   * a step's arithmetic is the reference's, element for element, with the adds of two planes
+//     on the packed FP32x2 pipe and no per-plane inclusion masks when every plane takes part in
+//     the minima (D a power of two, or the exact minimum);
 //   * opposite paths run as pairs: one warp walks a scanline from both ends at once, so it keeps
 //     two independent recurrences in flight; the pairs (L/R, T/B and the two diagonals) run
 //     concurrently on separate streams.  Each pair owns one volume: the path that reaches a pixel
@@ -21,6 +26,10 @@
 //     therefore differs from the reference's sequential path order only by rounding; the CPU
 //     oracle replays this exact order.  (The reduction unit flushes subnormal sums to zero; path
 //     values are costs plus penalties, never below 2^-126 unless exactly 0.)
+//   * the FP16 form (FP16 cost volume) keeps its pair volumes in FP16 as well: each path's values
+//     are rounded to FP16, the second end adds with packed FP16 reductions, and the combine adds
+//     the pairs in FP32.  That halves the bytes of the pair volumes, which with FP32 pairs were
+//     60 % of the stage's traffic; the FP16 form is held to its FP64 accuracy bound, not to bits.
 #include <climits>
 #include <vector>
 
@@ -195,11 +204,10 @@ template <bool HALF> struct CostElem;
 template <> struct CostElem<false> { using T = float; };
 template <> struct CostElem<true> { using T = __half; };
 
-// Per-lane cost slice of one chain step, and the ring stage of a warp: for each of its two
-// chains the 32 lanes' cost slices followed by 32 copies of the reference pixel.
+// Ring stage of a warp: for each of its two chains the 32 lanes' cost slices of one step.
 template <int PPL, bool HALF> struct Ring {
     static constexpr int CB = PPL * (int)sizeof(typename CostElem<HALF>::T);
-    static constexpr int CHAIN_B = 32 * CB + 32 * 4;
+    static constexpr int CHAIN_B = 32 * CB;
     static constexpr int STAGE_B = 2 * CHAIN_B;
 };
 
@@ -236,56 +244,162 @@ template <int PPL> __device__ __forceinline__ void red_planes(float* p, const fl
     }
 }
 
-// Recurrence state of one path along one scanline.
+// The FP16 form's pair volumes: the lane's planes rounded to FP16 (round to nearest) and stored,
+// or added to what is stored with packed FP16 reductions (the sum rounded to FP16, no flush).
+template <int PPL> __device__ __forceinline__ void pack_h(uint32_t (&w)[PPL / 2], const float (&v)[PPL]) {
+    static_assert(PPL % 2 == 0, "FP16 pair volumes need an even number of planes per lane");
+#pragma unroll
+    for (int j = 0; j < PPL / 2; ++j) {
+        const __half2 h = __floats2half2_rn(v[2 * j], v[2 * j + 1]);
+        w[j] = *reinterpret_cast<const uint32_t*>(&h);
+    }
+}
+template <int PPL> __device__ __forceinline__ void store_planes_h(__half* p, const float (&v)[PPL]) {
+    uint32_t w[PPL / 2];
+    pack_h<PPL>(w, v);
+    if constexpr (PPL == 8) {
+        *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+    } else if constexpr (PPL == 4) {
+        *reinterpret_cast<uint2*>(p) = make_uint2(w[0], w[1]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < PPL / 2; ++j) reinterpret_cast<uint32_t*>(p)[j] = w[j];
+    }
+}
+template <int PPL> __device__ __forceinline__ void red_planes_h(__half* p, const float (&v)[PPL]) {
+    uint32_t w[PPL / 2];
+    pack_h<PPL>(w, v);
+    if constexpr (PPL == 8) {
+        asm volatile("red.global.add.noftz.v4.f16x2 [%0], {%1, %2, %3, %4};" ::"l"(p), "r"(w[0]), "r"(w[1]),
+                     "r"(w[2]), "r"(w[3])
+                     : "memory");
+    } else if constexpr (PPL == 4) {
+        asm volatile("red.global.add.noftz.v2.f16x2 [%0], {%1, %2};" ::"l"(p), "r"(w[0]), "r"(w[1]) : "memory");
+    } else {
+#pragma unroll
+        for (int j = 0; j < PPL / 2; ++j)
+            asm volatile("red.global.add.noftz.f16x2 [%0], %1;" ::"l"(p + 2 * j), "r"(w[j]) : "memory");
+    }
+}
+// The meeting pixel of an odd chain in an FP16 pair volume: both paths' values rounded to FP16
+// and added in FP16, as the reduction does for the other pixels.
+template <int PPL> __device__ __forceinline__ void add_h(float (&o)[PPL], const float (&a)[PPL], const float (&b)[PPL]) {
+#pragma unroll
+    for (int j = 0; j < PPL; ++j) o[j] = __half2float(__hadd(__float2half_rn(a[j]), __float2half_rn(b[j])));
+}
+
+// Recurrence state of one path along one scanline, and the adaptive-penalty flags of the 32
+// steps of the current batch (bit i: step k0 + i has a reference-image gradient below tau).
 template <int PPL> struct PathState {
     float L[PPL];
-    float mprev, Iprev;
+    float mprev;
+    unsigned qmask;
 };
 
-// One pixel step of a path (sgm.cu:57-108): L(p, d) = C(p, d) + min(L(p-r, d), L(p-r, d+-1) + P1,
-// min_k L(p-r, k) + P2) - min_k L(p-r, k), P1/P2 scaled by q1/q2 where the reference image's
-// path gradient is below tau; a plane never measured (cost -1) makes the pixel invalid: its
-// cost counts as 0 and the path's output there is COST_INF = 0.  o receives the output.
+// a + b for the planes of a lane, two at a time on the packed FP32x2 pipe (each element rounds
+// as the scalar add does).
 template <int PPL>
-__device__ __forceinline__ void path_step(const SgmLaunch& a, PathState<PPL>& s, const float (&cv)[PPL], float I,
-                                          bool first, uint32_t incl, int lane, float (&o)[PPL]) {
-    bool neg = false;
+__device__ __forceinline__ void add_planes(float (&o)[PPL], const float (&a)[PPL], const float (&b)[PPL]) {
 #pragma unroll
-    for (int j = 0; j < PPL; ++j) neg |= (((incl >> j) & 1u) && cv[j] < 0.0f);
-    const bool inv = __any_sync(kFull, neg);
-    float Ln[PPL];
-    if (first) {
-#pragma unroll
-        for (int j = 0; j < PPL; ++j) Ln[j] = inv ? 0.0f : cv[j];
-    } else {
-        // adaptive penalties from the path gradient of the reference image (sgm.cu:75-82)
-        const float D1 = fabsf(__fsub_rn(I, s.Iprev));
-        float P1 = a.p1, P2 = a.p2;
-        if (D1 < a.tau) { P1 = __fmul_rn(P1, a.q1); P2 = __fmul_rn(P2, a.q2); }
-        const float mP2 = __fadd_rn(s.mprev, P2);
-        float lm = __shfl_up_sync(kFull, s.L[PPL - 1], 1);
-        float lp = __shfl_down_sync(kFull, s.L[0], 1);
-        if (lane == 0) lm = inf_f();
-        if (lane == 31) lp = inf_f();
-        // min(L[d], minL + P2, L[d-1] + P1, L[d+1] + P1) (sgm.cu:85-92); min(a+P1, b+P1) is
-        // min(a, b) + P1 exactly because rounding is monotonic
-#pragma unroll
-        for (int j = 0; j < PPL; ++j) {
-            const float left = (j == 0) ? lm : s.L[j - 1];
-            const float right = (j == PPL - 1) ? lp : s.L[j + 1];
-            const float vv = min3f(s.L[j], mP2, __fadd_rn(fminf(left, right), P1));
-            Ln[j] = __fsub_rn(__fadd_rn(inv ? 0.0f : cv[j], vv), s.mprev);   // (:98)
-        }
+    for (int j = 0; j + 1 < PPL; j += 2) {
+        const float2 r = __fadd2_rn(make_float2(a[j], a[j + 1]), make_float2(b[j], b[j + 1]));
+        o[j] = r.x;
+        o[j + 1] = r.y;
     }
-    s.Iprev = I;
-    float lmin = inf_f();
+    if constexpr (PPL % 2) o[PPL - 1] = __fadd_rn(a[PPL - 1], b[PPL - 1]);
+}
+template <int PPL> __device__ __forceinline__ void add_planes(float (&o)[PPL], const float (&a)[PPL], float b) {
+#pragma unroll
+    for (int j = 0; j + 1 < PPL; j += 2) {
+        const float2 r = __fadd2_rn(make_float2(a[j], a[j + 1]), make_float2(b, b));
+        o[j] = r.x;
+        o[j + 1] = r.y;
+    }
+    if constexpr (PPL % 2) o[PPL - 1] = __fadd_rn(a[PPL - 1], b);
+}
+
+// Smallest of the lane's planes that take part in the minimum (all of them when FULL).
+template <int PPL, bool FULL> __device__ __forceinline__ float lane_min(const float (&v)[PPL], uint32_t incl) {
+    if constexpr (FULL) {
+        float m = v[0];
+        int j = 1;
+#pragma unroll
+        for (; j + 1 < PPL; j += 2) m = min3f(m, v[j], v[j + 1]);
+        if (j < PPL) m = fminf(m, v[j]);
+        return m;
+    } else {
+        float m = inf_f();
+#pragma unroll
+        for (int j = 0; j < PPL; ++j)
+            if ((incl >> j) & 1u) m = fminf(m, v[j]);
+        return m;
+    }
+}
+
+// Whether the pixel has a plane that was never measured (cost < 0): the path treats its cost as 0
+// and outputs COST_INF = 0 there (sgm.cu:33-38, 67-71, 101-104).
+template <int PPL, bool FULL> __device__ __forceinline__ bool pixel_invalid(const float (&cv)[PPL], uint32_t incl) {
+    return __any_sync(kFull, lane_min<PPL, FULL>(cv, incl) < 0.0f);
+}
+
+// First pixel of a path: L = C, or 0 on an invalid pixel (sgm.cu:21-43).
+template <int PPL, bool FULL>
+__device__ __forceinline__ void path_first(PathState<PPL>& s, const float (&cv)[PPL], uint32_t incl, float (&o)[PPL]) {
+    const bool inv = pixel_invalid<PPL, FULL>(cv, incl);
+#pragma unroll
+    for (int j = 0; j < PPL; ++j) s.L[j] = o[j] = inv ? 0.0f : cv[j];
+    s.mprev = warp_min_f32(lane_min<PPL, FULL>(s.L, incl));
+}
+
+// One pixel step of a path (sgm.cu:57-108): L(p, d) = C(p, d) + min(L(p-r, d), L(p-r, d+-1) + P1,
+// min_k L(p-r, k) + P2) - min_k L(p-r, k), P1/P2 scaled by q1/q2 when the flag q says the
+// reference image's path gradient is below tau; a plane never measured makes the pixel invalid:
+// its cost counts as 0 and the path's output there is COST_INF = 0.  o receives the output.
+template <int PPL, bool FULL>
+__device__ __forceinline__ void path_step(const SgmLaunch& a, PathState<PPL>& s, const float (&cv)[PPL], bool q,
+                                          float p1q, float p2q, uint32_t incl, int lane, float (&o)[PPL]) {
+    const bool inv = pixel_invalid<PPL, FULL>(cv, incl);
+    const float P1 = q ? p1q : a.p1, P2 = q ? p2q : a.p2;
+    const float mP2 = __fadd_rn(s.mprev, P2);
+    float lm = __shfl_up_sync(kFull, s.L[PPL - 1], 1);
+    float lp = __shfl_down_sync(kFull, s.L[0], 1);
+    if (lane == 0) lm = inf_f();
+    if (lane == 31) lp = inf_f();
+    // min(L[d], minL + P2, L[d-1] + P1, L[d+1] + P1) (sgm.cu:85-92); min(a+P1, b+P1) is
+    // min(a, b) + P1 exactly because rounding is monotonic
+    float nb[PPL], cz[PPL], vv[PPL];
 #pragma unroll
     for (int j = 0; j < PPL; ++j) {
-        s.L[j] = Ln[j];
-        if ((incl >> j) & 1u) lmin = fminf(lmin, Ln[j]);
-        o[j] = inv ? 0.0f : Ln[j];
+        nb[j] = fminf(j == 0 ? lm : s.L[j - 1], j == PPL - 1 ? lp : s.L[j + 1]);
+        cz[j] = inv ? 0.0f : cv[j];
     }
-    s.mprev = warp_min_f32(lmin);
+    add_planes<PPL>(nb, nb, P1);
+#pragma unroll
+    for (int j = 0; j < PPL; ++j) vv[j] = min3f(s.L[j], mP2, nb[j]);
+    add_planes<PPL>(vv, cz, vv);               // C + val
+    add_planes<PPL>(s.L, vv, -s.mprev);        // - minL (:98); the negation is exact
+#pragma unroll
+    for (int j = 0; j < PPL; ++j) o[j] = inv ? 0.0f : s.L[j];
+    s.mprev = warp_min_f32(lane_min<PPL, FULL>(s.L, incl));
+}
+
+// Reference intensity of step k of a chain starting at pixel p0 (0 past its end).
+__device__ __forceinline__ float chain_ref(const float* __restrict__ ref, long p0, long step, int k, int n) {
+    return k < n ? __ldg(ref + p0 + (long)k * step) : 0.0f;
+}
+
+// The flags |I(k) - I(k-1)| < tau of the 32 steps k0 .. k0+31 of one chain as a ballot (bit i:
+// step k0 + i).  Lane i holds I(k0 + i) in `cur` (read one batch ahead into `nxt`, which is
+// then refilled with I(k0 + 64 + i)); `last` carries I(k0 - 1).
+__device__ __forceinline__ unsigned penalty_flags(float& cur, float& nxt, const float* __restrict__ ref, long p0,
+                                                  long step, int k0, int n, int lane, float tau, float& last) {
+    const float I = cur;
+    cur = nxt;
+    nxt = chain_ref(ref, p0, step, k0 + 64 + lane, n);
+    float prev = __shfl_up_sync(kFull, I, 1);
+    if (lane == 0) prev = last;
+    last = __shfl_sync(kFull, I, 31);
+    return __ballot_sync(kFull, fabsf(__fsub_rn(I, prev)) < tau);
 }
 
 // A pair of opposite paths along the same scanlines: warp c takes scanline c of direction
@@ -293,11 +407,14 @@ __device__ __forceinline__ void path_step(const SgmLaunch& a, PathState<PPL>& s,
 // two ends have not met, each stores its pixel's path values; after they have, each adds its
 // values to what the other end stored there; at the meeting pixel of an odd chain the two are
 // added in registers.  The two recurrences are independent, so each warp keeps two dependency
-// chains in flight.  The cost slices and reference pixels of both ends are streamed
-// PF steps ahead with cp.async into a per-warp shared ring.
-template <int PPL, bool HALF, int NW>
+// chains in flight.  The cost slices of both ends are streamed PF steps ahead with cp.async into
+// a per-warp shared ring; the reference pixels are read 32 steps at a time (one per lane, a batch
+// ahead) and turned into one ballot of penalty flags.  The loop is split at the meeting point,
+// so the store and the reduction phases run without a per-step branch.  HOUT: FP16 pair volume.
+template <int PPL, bool HALF, int NW, bool FULL, bool HOUT>
 __global__ void __launch_bounds__(NW * 32) sgm_pair_kernel(const SgmLaunch a, int dx, int dy, int slot) {
     using CT = typename CostElem<HALF>::T;
+    using OT = typename CostElem<HOUT>::T;
     using RG = Ring<PPL, HALF>;
     constexpr int CB = RG::CB, CHAIN_B = RG::CHAIN_B, STAGE_B = RG::STAGE_B;
     extern __shared__ __align__(16) unsigned char ring[];
@@ -307,64 +424,120 @@ __global__ void __launch_bounds__(NW * 32) sgm_pair_kernel(const SgmLaunch a, in
     const int c = blockIdx.x * NW + warp;
     if (c >= num_chains(dx, dy, W, H)) return;        // warp-uniform; no block barriers below
     const Chain ch = chain_start(c, dx, dy, W, H);
+    const int n = ch.n;
     const long step = (long)dy * W + dx;
     const long pf0 = (long)ch.y * W + ch.x;             // forward start
-    const long pb0 = pf0 + (long)(ch.n - 1) * step;     // backward start (the forward end)
+    const long pb0 = pf0 + (long)(n - 1) * step;        // backward start (the forward end)
+    const long gstep = step * D;                         // elements per step in the volumes
 
     unsigned char* const wbase = ring + (size_t)warp * PF * STAGE_B;
-    const CT* __restrict__ cost = reinterpret_cast<const CT*>(a.cost);
-    float* const out = a.part[slot >> 1];
+    const CT* const cf0 = reinterpret_cast<const CT*>(a.cost) + (size_t)pf0 * D + lane * PPL;
+    const CT* const cb0 = reinterpret_cast<const CT*>(a.cost) + (size_t)pb0 * D + lane * PPL;
+    OT* const out = static_cast<OT*>(a.part[slot >> 1]);
+    OT* qf = out + (size_t)pf0 * D + lane * PPL;        // the current step's output slices
+    OT* qb = out + (size_t)pb0 * D + lane * PPL;
+    auto put = [](OT* q, const float (&v)[PPL]) {
+        if constexpr (HOUT) store_planes_h<PPL>(q, v);
+        else store_planes<PPL>(q, v);
+    };
+    auto add = [](OT* q, const float (&v)[PPL]) {
+        if constexpr (HOUT) red_planes_h<PPL>(q, v);
+        else red_planes<PPL>(q, v);
+    };
+    auto meet = [](float (&o)[PPL], const float (&b)[PPL]) {   // o = o + b at the meeting pixel
+        if constexpr (HOUT) {
+            add_h<PPL>(o, o, b);
+        } else {
+#pragma unroll
+            for (int j = 0; j < PPL; ++j) o[j] = __fadd_rn(o[j], b[j]);
+        }
+    };
 
     auto issue = [&](unsigned char* sb, int k) {
-        const long qf = pf0 + k * step, qb = pb0 - k * step;
-        cp_async_bytes<CB>(sb + lane * CB, cost + (size_t)qf * D + lane * PPL);
-        cp_async_4(sb + 32 * CB + lane * 4, a.ref + qf);
-        cp_async_bytes<CB>(sb + CHAIN_B + lane * CB, cost + (size_t)qb * D + lane * PPL);
-        cp_async_4(sb + CHAIN_B + 32 * CB + lane * 4, a.ref + qb);
+        cp_async_bytes<CB>(sb + lane * CB, cf0 + (long)k * gstep);
+        cp_async_bytes<CB>(sb + CHAIN_B + lane * CB, cb0 - (long)k * gstep);
     };
 #pragma unroll 1
     for (int k = 0; k < PF; ++k) {
-        if (k < ch.n) issue(wbase + k * STAGE_B, k);
+        if (k < n) issue(wbase + k * STAGE_B, k);
         cp_async_commit();
     }
 
-    const uint32_t incl = a.order.incl[lane];
+    uint32_t incl = kFull;
+    if constexpr (!FULL) incl = a.order.incl[lane];
+    const float p1q = __fmul_rn(a.p1, a.q1), p2q = __fmul_rn(a.p2, a.q2);
     PathState<PPL> fs, bs;
-#pragma unroll
-    for (int j = 0; j < PPL; ++j) fs.L[j] = bs.L[j] = 0.0f;
-    fs.mprev = bs.mprev = fs.Iprev = bs.Iprev = 0.0f;
-    int st = 0;
+    float lastf = 0.0f, lastb = 0.0f;
+    // intensities of steps lane and 32 + lane of both chains; then the flags of steps 0..31
+    float If = chain_ref(a.ref, pf0, step, lane, n), Ifn = chain_ref(a.ref, pf0, step, 32 + lane, n);
+    float Ib = chain_ref(a.ref, pb0, -step, lane, n), Ibn = chain_ref(a.ref, pb0, -step, 32 + lane, n);
+    fs.qmask = penalty_flags(If, Ifn, a.ref, pf0, step, 0, n, lane, a.tau, lastf);
+    bs.qmask = penalty_flags(Ib, Ibn, a.ref, pb0, -step, 0, n, lane, a.tau, lastb);
 
-#pragma unroll 1
-    for (int k = 0; k < ch.n; ++k) {
+    // step 0: the first pixel of both paths
+    cp_async_wait<PF - 1>();
+    {
+        float cf[PPL], cb[PPL], of[PPL], ob[PPL];
+        load_slice<PPL, HALF>(cf, wbase + lane * CB);
+        load_slice<PPL, HALF>(cb, wbase + CHAIN_B + lane * CB);
+        path_first<PPL, FULL>(fs, cf, incl, of);
+        path_first<PPL, FULL>(bs, cb, incl, ob);
+        if (n == 1) {
+            meet(of, ob);
+            put(qf, of);
+        } else {
+            put(qf, of);
+            put(qb, ob);
+        }
+        if (PF < n) issue(wbase, PF);
+        cp_async_commit();
+    }
+    int st = PF > 1 ? 1 : 0;
+
+    // steps 1 .. n-1: the first visits (stores), the meeting pixel of an odd chain, then the
+    // second visits (reductions)
+    auto body = [&](int k, float (&of)[PPL], float (&ob)[PPL]) {
+        qf += gstep;
+        qb -= gstep;
+        if ((k & 31) == 0) {
+            fs.qmask = penalty_flags(If, Ifn, a.ref, pf0, step, k, n, lane, a.tau, lastf);
+            bs.qmask = penalty_flags(Ib, Ibn, a.ref, pb0, -step, k, n, lane, a.tau, lastb);
+        }
         cp_async_wait<PF - 1>();
         unsigned char* sb = wbase + st * STAGE_B;
         float cf[PPL], cb[PPL];
         load_slice<PPL, HALF>(cf, sb + lane * CB);
         load_slice<PPL, HALF>(cb, sb + CHAIN_B + lane * CB);
-        const float If = *reinterpret_cast<const float*>(sb + 32 * CB + lane * 4);
-        const float Ib = *reinterpret_cast<const float*>(sb + CHAIN_B + 32 * CB + lane * 4);
-        float of[PPL], ob[PPL];
-        path_step<PPL>(a, fs, cf, If, k == 0, incl, lane, of);
-        path_step<PPL>(a, bs, cb, Ib, k == 0, incl, lane, ob);
-        float* const qf = out + (size_t)(pf0 + k * step) * D + lane * PPL;
-        float* const qb = out + (size_t)(pb0 - k * step) * D + lane * PPL;
-        const int other = ch.n - 1 - k;   // the step at which the other end visits this pixel
-        if (k < other) {                  // first visits (warp-uniform)
-            store_planes<PPL>(qf, of);
-            store_planes<PPL>(qb, ob);
-        } else if (k > other) {           // second visits: the first ones were this thread's stores
-            red_planes<PPL>(qf, of);
-            red_planes<PPL>(qb, ob);
-        } else {                          // both ends on the same pixel
-#pragma unroll
-            for (int j = 0; j < PPL; ++j) of[j] = __fadd_rn(of[j], ob[j]);
-            store_planes<PPL>(qf, of);
-        }
+        const int bit = k & 31;
+        path_step<PPL, FULL>(a, fs, cf, (fs.qmask >> bit) & 1u, p1q, p2q, incl, lane, of);
+        path_step<PPL, FULL>(a, bs, cb, (bs.qmask >> bit) & 1u, p1q, p2q, incl, lane, ob);
         // refill this stage (consumed above) with step k + PF
-        if (k + PF < ch.n) issue(sb, k + PF);
+        if (k + PF < n) issue(sb, k + PF);
         cp_async_commit();
         st = (st + 1 == PF) ? 0 : st + 1;
+    };
+    const int half = n >> 1;   // steps k < half are first visits of both ends
+#pragma unroll 1
+    for (int k = 1; k < half; ++k) {
+        float of[PPL], ob[PPL];
+        body(k, of, ob);
+        put(qf, of);
+        put(qb, ob);
+    }
+    int k = half > 1 ? half : 1;
+    if ((n & 1) && n > 1) {   // both ends on the middle pixel (k == half)
+        float of[PPL], ob[PPL];
+        body(k, of, ob);
+        meet(of, ob);
+        put(qf, of);
+        ++k;
+    }
+#pragma unroll 1
+    for (; k < n; ++k) {   // second visits: the first ones were this warp's own stores
+        float of[PPL], ob[PPL];
+        body(k, of, ob);
+        add(qf, of);
+        add(qb, ob);
     }
     cp_async_wait<0>();
 }
@@ -373,7 +546,7 @@ __global__ void __launch_bounds__(NW * 32) sgm_pair_kernel(const SgmLaunch a, in
 // [+ ((P4 + P5) + (P6 + P7))], then the winner-take-all filter (MODE kCombineFilter), the debug
 // argmin (kCombineArgmin) or only a store of the sum (kCombineStore).  One warp per pixel,
 // grid-stride; the next pixel's slices are loaded before the current one is reduced.
-template <int PPL, int MODE, int NP>
+template <int PPL, int MODE, int NP, bool HIN>
 __global__ void __launch_bounds__(256) combine_kernel(const SgmLaunch a) {
     const int lane = threadIdx.x & 31;
     const long nw = (long)gridDim.x * (blockDim.x >> 5);
@@ -385,7 +558,12 @@ __global__ void __launch_bounds__(256) combine_kernel(const SgmLaunch a) {
     auto loadp = [&](long pix, float (&s)[NP][PPL]) {
         const size_t e = (size_t)pix * D + lane * PPL;
 #pragma unroll
-        for (int g = 0; g < NP; ++g) load_planes<PPL>(s[g], a.part[g] + e);
+        for (int g = 0; g < NP; ++g) {
+            if constexpr (HIN)
+                load_slice<PPL, true>(s[g], reinterpret_cast<const unsigned char*>(static_cast<const __half*>(a.part[g]) + e));
+            else
+                load_planes<PPL>(s[g], static_cast<const float*>(a.part[g]) + e);
+        }
     };
     long pix = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     float cur[NP][PPL], nxt[NP][PPL];
@@ -504,7 +682,17 @@ cudaError_t launch_with_priority(void (*kern)(Args...), dim3 grid, dim3 block, s
 template <int PPL, bool HALF, int NW>
 cudaError_t launch_pair_nw(const SgmLaunch& a, int pair, cudaStream_t s) {
     const size_t smem = (size_t)NW * PF * Ring<PPL, HALF>::STAGE_B;
-    auto kern = sgm_pair_kernel<PPL, HALF, NW>;
+    // every plane takes part in the minima (D a power of two, or the exact minimum): no masks
+    bool full = true;
+    for (int l = 0; l < 32; ++l) full = full && a.order.incl[l] == (1u << PPL) - 1u;
+    void (*kern)(SgmLaunch, int, int, int);
+    if constexpr (HALF && PPL % 2 == 0) {
+        if (a.part_half) kern = full ? sgm_pair_kernel<PPL, HALF, NW, true, true> : sgm_pair_kernel<PPL, HALF, NW, false, true>;
+        else kern = full ? sgm_pair_kernel<PPL, HALF, NW, true, false> : sgm_pair_kernel<PPL, HALF, NW, false, false>;
+    } else {
+        if (a.part_half) return cudaErrorInvalidValue;   // FP16 pair volumes come with FP16 cost volumes
+        kern = full ? sgm_pair_kernel<PPL, HALF, NW, true, false> : sgm_pair_kernel<PPL, HALF, NW, false, false>;
+    }
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -536,10 +724,25 @@ cudaError_t launch_combine(const SgmLaunch& a, int mode, cudaStream_t s) {
     const long blocks_needed = (npix + 7) / 8;   // 8 warps per block
     const int blocks = (int)(blocks_needed < (long)sms * 8 ? blocks_needed : (long)sms * 8);
     const bool eight = a.num_paths == 8;
-    void (*kern)(SgmLaunch);
-    if (mode == kCombineFilter) kern = eight ? combine_kernel<PPL, kCombineFilter, 4> : combine_kernel<PPL, kCombineFilter, 2>;
-    else if (mode == kCombineArgmin) kern = eight ? combine_kernel<PPL, kCombineArgmin, 4> : combine_kernel<PPL, kCombineArgmin, 2>;
-    else kern = eight ? combine_kernel<PPL, kCombineStore, 4> : combine_kernel<PPL, kCombineStore, 2>;
+    void (*kern)(SgmLaunch) = nullptr;
+    if (a.part_half) {
+        if constexpr (PPL % 2 == 0) {
+            if (mode == kCombineFilter)
+                kern = eight ? combine_kernel<PPL, kCombineFilter, 4, true> : combine_kernel<PPL, kCombineFilter, 2, true>;
+            else if (mode == kCombineArgmin)
+                kern = eight ? combine_kernel<PPL, kCombineArgmin, 4, true> : combine_kernel<PPL, kCombineArgmin, 2, true>;
+            else
+                kern = eight ? combine_kernel<PPL, kCombineStore, 4, true> : combine_kernel<PPL, kCombineStore, 2, true>;
+        } else {
+            return cudaErrorInvalidValue;
+        }
+    } else if (mode == kCombineFilter) {
+        kern = eight ? combine_kernel<PPL, kCombineFilter, 4, false> : combine_kernel<PPL, kCombineFilter, 2, false>;
+    } else if (mode == kCombineArgmin) {
+        kern = eight ? combine_kernel<PPL, kCombineArgmin, 4, false> : combine_kernel<PPL, kCombineArgmin, 2, false>;
+    } else {
+        kern = eight ? combine_kernel<PPL, kCombineStore, 4, false> : combine_kernel<PPL, kCombineStore, 2, false>;
+    }
     return launch_with_priority(kern, dim3(blocks), dim3(256), 0, s, a.priority, a);
 }
 

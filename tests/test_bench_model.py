@@ -44,6 +44,8 @@ def test_cost_and_sgm_work_at_the_headline_shape(shape):
     # the SGM + winner-take-all + fusion share of B_alg: two sweeps over C, the forward sum
     # written and read once, the reference image, fusion state and outputs
     assert bench.sgm_alg_bytes(4) == 16 * V + 60 * N and bench.sgm_alg_bytes(2) == 12 * V + 60 * N
+    _, sgm16 = bench.algorithmic_bytes(2)   # the FP16 form's pair volumes are FP16 as well
+    assert abs(sgm16 / V - 48) < 0.5
     _, sgm = bench.algorithmic_bytes(4)
     # 8 paths read C and the reference; 4 pair volumes stored, reduced into (read + write) and
     # read once by the combine; depth and index written
