@@ -277,7 +277,7 @@ def max_over_ranks(vals, world):
     return t.tolist()
 
 
-def run_batched(args, rank, world, precision: str, B: int, host_io: bool, clocks: bool):
+def run_batched(args, rank, world, precision: str, B: int, host_io: bool, clocks: bool, persistent: bool = False):
     """B sequences of the bench workload in one pm_batch: each step is one CUDA-graph launch that
     maps every sequence.  The two frame sets of the batch hold keyframes 0 and 1 of each
     sequence (device memory, or pinned host memory copied inside the graph with host_io); the
@@ -293,7 +293,8 @@ def run_batched(args, rank, world, precision: str, B: int, host_io: bool, clocks
                tau_so=TAU, uniqueness_ratio=UNIQ, cost_mode=1 if args.cost_mode == "corrected" else 0,
                precision=prec, device=dev, sampler=SAMPLERS[sampler_name(args, prec)])
     seqs = [scene.make_sequence(W, H, F_PX, S, 2, seed=2000 + 97 * rank + i) for i in range(B)]
-    b = StereoBatch([cfg] * B, S, lanes=0, host_io=host_io, autotune=True, priority=args.priority)
+    b = StereoBatch([cfg] * B, S, lanes=0, host_io=host_io, autotune=not persistent, priority=args.priority,
+                    persistent=persistent)
     for i in range(B):
         b.init_intrinsic(i, seqs[i][0].K, drho)
 
@@ -325,7 +326,7 @@ def run_batched(args, rank, world, precision: str, B: int, host_io: bool, clocks
     if sampler:
         sampler.__exit__(None, None, None)
     t = e0.elapsed_time(e1)
-    tuning = b.tuning(0)
+    tuning = None if persistent else b.tuning(0)
     b.close()
     t = max_over_ranks([t], world)[0]
     return t, (sampler.summary() if sampler else None), tuning
@@ -336,7 +337,7 @@ MIXED = [(320, 240, 64, 260.0), (640, 480, 128, 520.0), (1280, 720, 192, 1040.0)
 MIXED_PER_SHAPE, MIXED_S = 16, 4
 
 
-def run_mixed(args, rank, world, precision: str, host_io: bool, clocks: bool):
+def run_mixed(args, rank, world, precision: str, host_io: bool, clocks: bool, persistent: bool = False):
     """This rank's shard (balanced by voxels x sources) of the 48-sequence mixed batch in one
     pm_batch; each step is one CUDA-graph launch that maps every sequence of the shard.  Two
     seeded scenes per size are shared by that size's sequences (the inputs only need the size)."""
@@ -359,8 +360,8 @@ def run_mixed(args, rank, world, precision: str, host_io: bool, clocks: bool):
     mine = shard_sequences(cfgs, world, MIXED_S)[rank]
     scenes = {k: [scene.make_sequence(w, h, f, MIXED_S, 2, seed=3000 + 10 * k + j) for j in range(2)]
               for k, (w, h, d, f) in enumerate(MIXED) if any(shapes[i] == k for i in mine)}
-    b = StereoBatch([cfgs[i] for i in mine], MIXED_S, lanes=args.lanes, host_io=host_io, autotune=True,
-                    priority=args.priority)
+    b = StereoBatch([cfgs[i] for i in mine], MIXED_S, lanes=0 if persistent else args.lanes, host_io=host_io,
+                    autotune=not persistent, priority=args.priority, persistent=persistent)
     seqs = []
     for j, i in enumerate(mine):
         seqs.append(scenes[shapes[i]][i % 2])
@@ -401,30 +402,106 @@ def run_mixed(args, rank, world, precision: str, host_io: bool, clocks: bool):
     return t, (sampler.summary() if sampler else None), len(mine), h2d, d2h
 
 
+def run_mixed_plain_fp32(args, rank, world):
+    """The plain FP32 form run per sequence over this rank's shard of the mixed batch: one
+    StereoMapper per size, each sequence's keyframe mapped after the other (initReference, the
+    updates, outputFusion), device-resident frames; ms per step of all the shard's sequences."""
+    import torch
+    from probabilistic_mapping_b200 import scene
+    from probabilistic_mapping_b200.mapper import StereoMapper
+    from probabilistic_mapping_b200.shard import shard_sequences
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    cfgs, shapes = [], []
+    for k, (w, h, d, f) in enumerate(MIXED):
+        for _ in range(MIXED_PER_SHAPE):
+            cfgs.append(dict(width=w, height=h, num_planes=d))
+            shapes.append(k)
+    mine = shard_sequences(cfgs, world, MIXED_S)[rank]
+    mappers, frames = {}, {}
+    for k, (w, h, d, f) in enumerate(MIXED):
+        if not any(shapes[i] == k for i in mine):
+            continue
+        rho0, drho = scene.plane_range(d)
+        m = StereoMapper(w, h, d, rho0=rho0, intensity_scale=1 / 255, num_paths=PATHS, p1=P1, p2=P2, tau_so=TAU,
+                         uniqueness_ratio=UNIQ, precision=0, device=dev)
+        seq = [scene.make_sequence(w, h, f, MIXED_S, 2, seed=3000 + 10 * k + j) for j in range(2)]
+        m.initIntrinsic(seq[0][0].K, 0.0, drho)
+        mappers[k] = m
+        frames[k] = [[(torch.from_numpy(fs.ref).cuda(), [torch.from_numpy(np.ascontiguousarray(x)).cuda()
+                                                         for x in fs.srcs], fs) for fs in sq] for sq in seq]
+    outs = {k: torch.empty((MIXED[k][1], MIXED[k][0]), dtype=torch.float32, device="cuda") for k in mappers}
+
+    def step(t):
+        for i in mine:
+            k = shapes[i]
+            ref, srcs, fs = frames[k][i % 2][t % 2]
+            m = mappers[k]
+            m.initReference(ref)
+            for s in range(MIXED_S):
+                m.update(srcs[s], fs.R_ref, fs.T_ref, fs.R_srcs[s], fs.T_srcs[s])
+            K = fs.K
+            m.outputFusion(fs.R_ref, fs.T_ref, K[0, 0], K[1, 1], K[0, 2], K[1, 2], out=outs[k], want_variance=False)
+
+    for t in range(args.warmup):
+        step(t)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for t in range(args.steps):
+        step(args.warmup + t)
+    e1.record()
+    torch.cuda.synchronize()
+    for m in mappers.values():
+        m.close()
+    return max_over_ranks([e0.elapsed_time(e1)], world)[0]
+
+
+def mixed_measure(args, rank, world):
+    """The mixed batch in both batched modes (graph and persistent) and the plain FP32 form per
+    sequence; returns (best mode name, per-mode results, plain FP32 ms, shard size, h2d, d2h)."""
+    precision = args.precision or "fp16"
+    total = len(MIXED) * MIXED_PER_SHAPE
+    res = {}
+    for mode in args.batch_modes:
+        persistent = mode == "persistent"
+        t, clocks, n_mine, _, _ = run_mixed(args, rank, world, precision, host_io=False, clocks=True,
+                                            persistent=persistent)
+        te, _, _, h2d, d2h = run_mixed(args, rank, world, precision, host_io=True, clocks=False,
+                                       persistent=persistent)
+        res[mode] = {"value": total * args.steps / (t / 1000.0), "e2e": total * args.steps / (te / 1000.0),
+                     "ms_per_step": t / args.steps, "clocks": clocks}
+    best = max(res, key=lambda k: res[k]["value"])
+    t_plain = run_mixed_plain_fp32(args, rank, world)
+    return best, res, t_plain, n_mine, h2d, d2h
+
+
 def mixed_main(args, rank, world):
     precision = args.precision or "fp16"
-    t, clocks, n_mine, _, _ = run_mixed(args, rank, world, precision, host_io=False, clocks=True)
-    te, _, _, h2d, d2h = run_mixed(args, rank, world, precision, host_io=True, clocks=False)
+    best, res, t_plain, n_mine, h2d, d2h = mixed_measure(args, rank, world)
     total = len(MIXED) * MIXED_PER_SHAPE
-    value = total * args.steps / (t / 1000.0)
-    e2e = total * args.steps / (te / 1000.0)
     if rank == 0:
         vox = sum(w * h * d for w, h, d, _ in MIXED) * MIXED_PER_SHAPE
+        r = res[best]
         line = {"metric": "depth maps/s, 48-sequence mixed batch (16 each at 320x240x64, 640x480x128, "
-                          "1280x720x192), 4 sources", "value": value, "unit": "depth maps/s", "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps, "higher_is_better": True,
-                "scaling": "strong", "vs_baseline": None, "dtype": "f16" if precision == "fp16" else "f32",
-                "data": "synthetic",
+                          "1280x720x192), 4 sources", "value": r["value"], "unit": "depth maps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "f16" if precision == "fp16" else "f32", "data": "synthetic",
                 "config": {"workload": f"48 sequences, {MIXED_S} sources, {PATHS}-path SGM, fusion step, "
-                                       f"{precision} {sampler_name(args, precision)} sampler"
-                                       + f", lanes={args.lanes}", "global_batch": total, "seq_len": 0,
+                                       f"{precision} {sampler_name(args, precision)} sampler, {best} batch",
+                           "global_batch": total, "seq_len": 0,
                            "parallelism": f"sequence shards x{world}, balanced by voxels x sources",
                            "l2": "per-map working sets exceed the 126 MB L2"},
-                "voxels_per_s": vox * args.steps / (t / 1000.0),
+                "voxels_per_s": vox * args.steps / (r["ms_per_step"] * args.steps / 1000.0),
+                "batch_modes": {k: {kk: vv for kk, vv in v.items() if kk != "clocks"} for k, v in res.items()},
+                "plain_fp32_per_sequence": {"value": total * args.steps / (t_plain / 1000.0),
+                                            "unit": "depth maps/s", "ms_per_step": t_plain / args.steps},
+                "speedup_vs_plain_fp32_per_sequence": r["value"] / (total * args.steps / (t_plain / 1000.0)),
                 "sequences_on_rank0": n_mine,
-                "e2e": {"value": e2e, "unit": "depth maps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "note": "rank 0's shard bytes"},
-                "clocks": clocks}
+                "e2e": {"value": r["e2e"], "unit": "depth maps/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "note": "rank 0's shard bytes"},
+                "clocks": r["clocks"]}
         print(json.dumps(line))
 
 
@@ -557,6 +634,11 @@ def main():
     ap.add_argument("--fp32-sampler", choices=["exact", "texture_f32"], default="exact",
                     help="FP32 form: exact FP32 bilinear (bit-exact against the FP32 oracle) or the texture "
                          "unit on FP32 texels (the reference's own sampler)")
+    ap.add_argument("--batch-mode", choices=["graph", "persistent", "best"], default="best",
+                    help="batched forms: per-sequence kernels in one CUDA graph, the persistent kernel "
+                         "(PM_BATCH_PERSISTENT), or both with the faster as the headline")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="batched form: skip the 48-sequence mixed batch reported beside the headline")
     ap.add_argument("--priority", type=int, default=1, choices=[0, 1],
                     help="batched forms: SGM kernels at the greatest launch priority (1) or not (0)")
     ap.add_argument("--precision", choices=["fp32", "fp16"], default=None,
@@ -570,6 +652,7 @@ def main():
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    args.batch_modes = ["graph", "persistent"] if args.batch_mode == "best" else [args.batch_mode]
 
     if args.impl == "reference":
         # The reference implements this path only in CUDA (its host code adds the CPU fusion
@@ -621,13 +704,23 @@ def main():
     t_plain, t_plain_e2e, stage_ms, clocks_plain = run_ours(args, rank, world, "fp32")
     plain_value = world * args.steps / (t_plain / 1000.0)
     plain_e2e = world * args.steps / (t_plain_e2e / 1000.0)
+    batch_modes = None
     if args.form == "batched":
         B = args.batch
-        t_b, clocks, tuning = run_batched(args, rank, world, args.precision, B, host_io=False, clocks=True)
-        t_be, _, _ = run_batched(args, rank, world, args.precision, B, host_io=True, clocks=False)
-        value = world * B * args.steps / (t_b / 1000.0)
-        e2e = world * B * args.steps / (t_be / 1000.0)
-        ms_per_step = t_b / args.steps
+        batch_modes = {}
+        for mode in args.batch_modes:
+            persistent = mode == "persistent"
+            t_b, clocks_b, tuning_b = run_batched(args, rank, world, args.precision, B, host_io=False, clocks=True,
+                                                  persistent=persistent)
+            t_be, _, _ = run_batched(args, rank, world, args.precision, B, host_io=True, clocks=False,
+                                     persistent=persistent)
+            batch_modes[mode] = {"value": world * B * args.steps / (t_b / 1000.0),
+                                 "e2e": world * B * args.steps / (t_be / 1000.0), "ms_per_step": t_b / args.steps,
+                                 "clocks": clocks_b, "tuning": tuning_b}
+        best = max(batch_modes, key=lambda k: batch_modes[k]["value"])
+        value, e2e = batch_modes[best]["value"], batch_modes[best]["e2e"]
+        ms_per_step, clocks, tuning = (batch_modes[best]["ms_per_step"], batch_modes[best]["clocks"],
+                                       batch_modes["graph"]["tuning"] if "graph" in batch_modes else None)
         if args.precision == "fp16":   # stage times of the FP16 form's kernels (plain mapper)
             _, _, stage_ms, _ = run_ours(args, rank, world, "fp16", passes=("stage",))
     else:
@@ -658,6 +751,17 @@ def main():
     # to_float (reference) + one conversion per source, cost (+ the FP16 volume's rebase), one
     # kernel per opposite-path pair, combine + winner-take-all, fusion transform + update
     launches_per_map = 1 + S + 1 + (1 if e == 2 else 0) + PATHS // 2 + 1 + 2
+    mixed = None
+    if args.form == "batched" and not args.no_mixed:
+        best_m, res_m, t_plain_m, _, _, _ = mixed_measure(args, rank, world)
+        total_m = len(MIXED) * MIXED_PER_SHAPE
+        plain_m = total_m * args.steps / (t_plain_m / 1000.0)
+        mixed = {"workload": "48 sequences (16 each at 320x240x64, 640x480x128, 1280x720x192), 4 sources, "
+                             f"{PATHS}-path SGM, fusion step, {args.precision} {sampler_name(args, args.precision)} "
+                             "sampler", "unit": "depth maps/s", "best_mode": best_m,
+                 "batch_modes": {k: {kk: vv for kk, vv in v.items() if kk != "clocks"} for k, v in res_m.items()},
+                 "plain_fp32_per_sequence": plain_m,
+                 "speedup_vs_plain_fp32_per_sequence": res_m[best_m]["value"] / plain_m}
     matched = None
     if rank == 0 and not args.no_matched:
         matched = {"config": REF_CFG_NAME,
@@ -672,7 +776,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if e == 4 else "f16", "data": "synthetic",
             "config": {"workload": f"{W}x{H}, {D} planes, {S} sources, {PATHS}-path SGM, uniqueness {UNIQ}, "
                                    f"fusion step; {args.precision} {args.form} form"
-                                   + (f", {B} sequences per CUDA-graph launch" if args.form == "batched" else "")
+                                   + (f", {B} sequences per CUDA-graph launch ({best} batch)"
+                                      if args.form == "batched" else "")
                                    + f", {sampler_name(args, args.precision)} sampler"
                                    + f", {args.cost_mode} cost samples",
                        "global_batch": world * B, "seq_len": 0, "parallelism": f"replicas x{world}",
@@ -716,13 +821,21 @@ def main():
                          "copy_out": float(stage_ms[3]), "source": f"plain {args.precision} mapper, CUDA events"},
             "e2e": {"value": e2e, "unit": "depth maps/s", "h2d_bytes_per_step": B * (S + 1) * W * H,
                     "d2h_bytes_per_step": B * 2 * 4 * W * H},
-            "gpu_launches": launches_per_map * B * args.steps,
+            # the persistent batch: per sequence the conversions and the two fusion kernels, plus one
+            # persistent kernel per step for all sequences
+            "gpu_launches": ((1 + S + 2) * B + 1) * args.steps if batch_modes and best == "persistent"
+            else launches_per_map * B * args.steps,
             "clocks": clocks,
         }
         if matched:
             line["matched_reference_config"] = matched
         if tuning:
             line["sgm_schedule"] = {"pair_warps": tuning[0], "serial_pairs": tuning[1], "tuned_ms": tuning[2]}
+        if batch_modes:
+            line["batch_modes"] = {k: {kk: vv for kk, vv in v.items() if kk not in ("clocks", "tuning")}
+                                   for k, v in batch_modes.items()}
+        if mixed:
+            line["mixed_batch"] = mixed
         if not args.no_cpu_baseline:
             rate, cores = cpu_baseline_sample(maps=3)
             line["cpu_baseline"] = {"value": rate, "unit": "depth maps/s", "cores": cores, "kind": "port",

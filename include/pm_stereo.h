@@ -213,6 +213,15 @@ typedef struct pm_batch pm_batch;
 #define PM_BATCH_AUTOTUNE 2 /* time the SGM schedules for each distinct shape at creation */
 #define PM_BATCH_PRIORITY 4 /* SGM kernels at the device's greatest launch priority, so they
                                overlap the other sequences' cost kernels */
+#define PM_BATCH_PERSISTENT 8 /* the cost volumes, FP16 rebases, SGM path pairs and winner-take-all
+                                 of all sequences in ONE persistent kernel launch (inside the
+                                 graph), which takes the work items of every sequence from one
+                                 list, interleaving one sequence's cost tiles with the previous
+                                 one's SGM scanlines.  Needs lanes = 0 and one precision, sampler
+                                 and cost mode for all sequences (else PM_ERR_UNSUPPORTED);
+                                 PM_BATCH_AUTOTUNE and PM_BATCH_PRIORITY do not apply to it.
+                                 pm_batch_synchronize reports PM_ERR_CUDA if a dependency wait
+                                 of the last step ran out (its outputs are then invalid). */
 PM_API pm_status pm_batch_create(const pm_config* cfgs, int num_sequences, int num_sources, int lanes, int flags,
                                  pm_batch** out);
 PM_API void pm_batch_destroy(pm_batch* b);

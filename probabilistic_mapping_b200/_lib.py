@@ -28,6 +28,7 @@ PM_SAMPLER_TEXTURE_F32 = 2
 PM_BATCH_HOST_IO = 1
 PM_BATCH_AUTOTUNE = 2
 PM_BATCH_PRIORITY = 4
+PM_BATCH_PERSISTENT = 8
 PM_FUSION_GPU = 0
 PM_FUSION_CPU_PATH = 1
 PM_CASE_RAW_ARGMIN = 0

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "pm_internal.h"
+#include "pm_persist.h"
 #include "pm_stereo.h"
 
 namespace pm {
@@ -110,6 +111,14 @@ struct pm_batch {
     bool built = false;
     long step = 0;
     std::string err;
+    // PM_BATCH_PERSISTENT: the work list and per-sequence descriptors of the persistent kernel
+    bool persistent = false;
+    PersistSeq* d_pseq[2] = {};   // per buffer set (the homographies' device block differs)
+    PersistItem* d_items = nullptr;
+    unsigned* d_counters = nullptr;
+    size_t counter_bytes = 0;
+    PersistLaunch plaunch{};
+    cudaEvent_t persist_done = nullptr;
 };
 
 namespace {
@@ -192,6 +201,10 @@ void free_batch(pm_batch* b) {
         if (q.lane_free) cudaEventDestroy(q.lane_free);
     }
     if (b->root) cudaEventDestroy(b->root);
+    if (b->persist_done) cudaEventDestroy(b->persist_done);
+    for (auto* p : b->d_pseq) cudaFree(p);
+    cudaFree(b->d_items);
+    cudaFree(b->d_counters);
     if (b->run) cudaStreamDestroy(b->run);
 }
 
@@ -224,16 +237,14 @@ SgmLaunch sgm_launch(const Seq& q, const LaneBufs& l, int priority) {
     return a;
 }
 
-// The work of one sequence for buffer set k, on its own streams (captured into the graph).
-cudaError_t enqueue_seq(pm_batch* b, int i, int k) {
+// The parameter block, the frames and their conversions of one sequence for buffer set k.
+cudaError_t enqueue_inputs(pm_batch* b, int i, int k, cudaStream_t m) {
     Seq& q = b->seqs[i];
-    LaneBufs& l = b->lanes[q.lane];
     const pm_config& c = q.cfg;
     const int W = c.width, H = c.height, S = q.S;
     const size_t N = q.N;
     const bool host = b->flags & PM_BATCH_HOST_IO;
     const bool half = c.precision == PM_PREC_FP16;
-    cudaStream_t m = q.st[0];
     cudaError_t e;
     if ((e = cudaMemcpyAsync(q.d_par[k], q.h_par[k], sizeof(float) * q.par_floats, cudaMemcpyHostToDevice, m)))
         return e;
@@ -255,61 +266,228 @@ cudaError_t enqueue_seq(pm_batch* b, int i, int k) {
                      : launch_to_quad(W, H, f, W, q.d_srcq + (size_t)s * N, sc, m);
         if (e) return e;
     }
-    // the lane's volumes are free once the previous sequence in this lane has finished its SGM
-    if (l.last_user >= 0 && (e = cudaStreamWaitEvent(m, b->seqs[l.last_user].lane_free, 0))) return e;
-    l.last_user = i;
+    return cudaSuccess;
+}
+
+// The cost pass of one sequence (calc_cost.cu:212-253 for all its sources at once).
+CostLaunch cost_launch(const Seq& q, const LaneBufs& l, int k) {
+    const pm_config& c = q.cfg;
     CostLaunch a;
     std::memset(&a, 0, sizeof a);
     a.ref = q.d_ref;
     a.srcq = q.d_srcq;
     if (c.sampler != PM_SAMPLER_EXACT) {
         a.use_tex = 1;
-        for (int s = 0; s < S; ++s) a.tex[s] = q.tex[s];
+        for (int s = 0; s < q.S; ++s) a.tex[s] = q.tex[s];
     }
     a.offset = l.off;
     a.block_offset = l.boff;
-    a.W = W;
-    a.H = H;
+    a.W = c.width;
+    a.H = c.height;
     a.D = c.num_planes;
-    a.nsrc = S;
+    a.nsrc = q.S;
     a.rho0 = c.rho0;
     a.drho = c.rho_step;
     a.mode = c.cost_mode;
     a.hom_dev = q.d_par[k];
     a.cost = l.cost;
-    a.cost_half = half;
-    if ((e = launch_cost(a, m))) return e;
-    const SgmLaunch g = sgm_launch(q, l, b->sgm_priority);
-    if ((e = launch_sgm(g, kCombineFilter, m, &q.side))) return e;
-    if ((e = cudaEventRecord(q.lane_free, m))) return e;
-    // fusion (stereo_mapper.cpp:111-244) with the step's pose, flags and state index from d_par
+    a.cost_half = c.precision == PM_PREC_FP16;
+    return a;
+}
+
+// The fusion step of one sequence (stereo_mapper.cpp:111-244) with the step's pose, flags and
+// state index from its parameter block, and the host copies of its outputs.
+cudaError_t enqueue_fusion(pm_batch* b, int i, int k, cudaStream_t m) {
+    Seq& q = b->seqs[i];
+    const size_t N = q.N;
+    cudaError_t e;
     if ((e = cudaMemcpyAsync(q.d_fused, q.d_depth, 4 * N, cudaMemcpyDeviceToDevice, m))) return e;
     FuseLaunch f;
     std::memset(&f, 0, sizeof f);
-    f.W = W;
-    f.H = H;
+    f.W = q.cfg.width;
+    f.H = q.cfg.height;
     f.depth = q.d_fused;
     f.ztable = q.d_ztable;
     f.table = q.d_table;
     f.variance = q.d_var;
-    f.params_dev = q.d_par[k] + 12 * S;
-    f.flags_dev = reinterpret_cast<const int*>(q.d_par[k] + 12 * S + 16);
+    f.params_dev = q.d_par[k] + 12 * q.S;
+    f.flags_dev = reinterpret_cast<const int*>(q.d_par[k] + 12 * q.S + 16);
     for (int s = 0; s < 2; ++s)
         for (int j = 0; j < 4; ++j) f.state[s][j] = q.d_state[s][j];
     if ((e = launch_fuse_gpu(f, m))) return e;
-    if (host) {
+    if (b->flags & PM_BATCH_HOST_IO) {
         if ((e = cudaMemcpyAsync(q.h_out[k], q.d_fused, 4 * N, cudaMemcpyDeviceToHost, m))) return e;
         if ((e = cudaMemcpyAsync(q.h_out[k] + N, q.d_var, 4 * N, cudaMemcpyDeviceToHost, m))) return e;
     }
     return cudaSuccess;
 }
 
+// The work of one sequence for buffer set k, on its own streams (captured into the graph).
+cudaError_t enqueue_seq(pm_batch* b, int i, int k) {
+    Seq& q = b->seqs[i];
+    LaneBufs& l = b->lanes[q.lane];
+    cudaStream_t m = q.st[0];
+    cudaError_t e;
+    if ((e = enqueue_inputs(b, i, k, m))) return e;
+    // the lane's volumes are free once the previous sequence in this lane has finished its SGM
+    if (l.last_user >= 0 && (e = cudaStreamWaitEvent(m, b->seqs[l.last_user].lane_free, 0))) return e;
+    l.last_user = i;
+    if ((e = launch_cost(cost_launch(q, l, k), m))) return e;
+    const SgmLaunch g = sgm_launch(q, l, b->sgm_priority);
+    if ((e = launch_sgm(g, kCombineFilter, m, &q.side))) return e;
+    if ((e = cudaEventRecord(q.lane_free, m))) return e;
+    return enqueue_fusion(b, i, k, m);
+}
+
+// ---- the persistent form -------------------------------------------------------------------
+constexpr int kRebaseRange = 1024;    // pixels per rebase item (a multiple of 8 warps x RB)
+constexpr int kCombineRange = 2048;   // pixels per combine item
+
+// Blocks of eight scanlines of path pair p: rows (L/R), columns (T/B), diagonals.
+int sgm_blocks(const pm_config& c, int pair) {
+    const int n = pair == 0 ? c.height : (pair == 1 ? c.width : c.width + c.height - 1);
+    return (n + 7) / 8;
+}
+
+// The work list: the cost tiles of sequence s interleaved with the rebase, SGM and combine items
+// of sequence s - 1 (spread evenly among them), so every item comes after what it waits for.
+std::vector<PersistItem> persist_items(const pm_batch* b) {
+    const int n = (int)b->seqs.size();
+    std::vector<std::vector<PersistItem>> C(n), P(n);
+    auto item = [](int type, int seq, int wait_kind, unsigned target, int idx, int end, int sub) {
+        PersistItem it{};
+        it.type = (uint16_t)type;
+        it.seq = (uint16_t)seq;
+        it.wait_kind = (int8_t)wait_kind;
+        it.wait_target = target;
+        it.idx = idx;
+        it.end = end;
+        it.sub = (uint8_t)sub;
+        return it;
+    };
+    for (int s = 0; s < n; ++s) {
+        const pm_config& c = b->seqs[s].cfg;
+        const int npix = c.width * c.height;
+        const int ncost = ((c.width + 29) / 30) * ((c.height + 7) / 8) * (c.num_planes / 16);
+        for (int t = 0; t < ncost; ++t) C[s].push_back(item(kItemCost, s, -1, 0, t, 0, 0));
+        int wait_kind = kItemCost;
+        unsigned target = (unsigned)ncost;
+        if (c.precision == PM_PREC_FP16) {
+            unsigned nr = 0;
+            for (int p0 = 0; p0 < npix; p0 += kRebaseRange, ++nr)
+                P[s].push_back(item(kItemRebase, s, kItemCost, ncost, p0, std::min(npix, p0 + kRebaseRange), 0));
+            wait_kind = kItemRebase;
+            target = nr;
+        }
+        unsigned ng = 0;
+        for (int pair = 0; pair < c.num_paths / 2; ++pair)
+            for (int bx = 0; bx < sgm_blocks(c, pair); ++bx, ++ng)
+                P[s].push_back(item(kItemSgm, s, wait_kind, target, bx, 0, pair));
+        for (int p0 = 0; p0 < npix; p0 += kCombineRange)
+            P[s].push_back(item(kItemCombine, s, kItemSgm, ng, p0, std::min(npix, p0 + kCombineRange), 0));
+    }
+    std::vector<PersistItem> out(C[0]);
+    for (int s = 1; s <= n; ++s) {
+        const std::vector<PersistItem>& c = s < n ? C[s] : std::vector<PersistItem>();
+        const std::vector<PersistItem>& p = P[s - 1];
+        size_t j = 0;
+        for (size_t i = 0; i < c.size(); ++i) {
+            out.push_back(c[i]);
+            const size_t upto = (i + 1) * p.size() / c.size();
+            while (j < upto) out.push_back(p[j++]);
+        }
+        while (j < p.size()) out.push_back(p[j++]);
+    }
+    return out;
+}
+
+int persist_form(const pm_config& c) {
+    if (c.precision == PM_PREC_FP16) return c.sampler == PM_SAMPLER_EXACT ? kPersistFp16Quad : kPersistFp16Tex;
+    return c.sampler == PM_SAMPLER_EXACT ? kPersistFp32Quad : kPersistFp32Tex;
+}
+
+// Descriptors (both buffer sets), the work list and the counters; called once the plane
+// spacings are known (at the first run).
+pm_status setup_persist(pm_batch* b) {
+    const int n = (int)b->seqs.size();
+    std::vector<PersistSeq> h((size_t)n);
+    int max_ppl = 1;
+    size_t smem = 0;
+    for (int k = 0; k < 2; ++k) {
+        for (int i = 0; i < n; ++i) {
+            const Seq& q = b->seqs[i];
+            const LaneBufs& l = b->lanes[q.lane];
+            PersistSeq& d = h[i];
+            std::memset(&d, 0, sizeof d);
+            d.cost = cost_launch(q, l, k);
+            d.sgm = sgm_launch(q, l, 0);
+            d.gx = (q.cfg.width + 29) / 30;
+            d.gy = (q.cfg.height + 7) / 8;
+            d.ppl = q.cfg.num_planes / 32;
+            d.full = 1;
+            for (int ln = 0; ln < 32; ++ln) d.full &= q.order.incl[ln] == (1u << d.ppl) - 1u;
+            max_ppl = std::max(max_ppl, d.ppl);
+            smem = std::max(smem, persist_smem_bytes(d.ppl, q.cfg.precision == PM_PREC_FP16));
+        }
+        if (!b->d_pseq[k]) PB_CK(b, cudaMalloc((void**)&b->d_pseq[k], sizeof(PersistSeq) * n));
+        PB_CK(b, cudaMemcpy(b->d_pseq[k], h.data(), sizeof(PersistSeq) * n, cudaMemcpyHostToDevice));
+    }
+    const std::vector<PersistItem> items = persist_items(b);
+    if (!b->d_items) PB_CK(b, cudaMalloc((void**)&b->d_items, sizeof(PersistItem) * items.size()));
+    PB_CK(b, cudaMemcpy(b->d_items, items.data(), sizeof(PersistItem) * items.size(), cudaMemcpyHostToDevice));
+    b->counter_bytes = sizeof(unsigned) * (4 * (size_t)n + 2);
+    if (!b->d_counters) PB_CK(b, cudaMalloc((void**)&b->d_counters, b->counter_bytes));
+    PB_CK(b, cudaMemset(b->d_counters, 0, b->counter_bytes));
+    PersistLaunch& L = b->plaunch;
+    L.items = b->d_items;
+    L.n_seqs = n;
+    L.n_items = (int)items.size();
+    L.counters = b->d_counters;
+    L.mode = b->seqs[0].cfg.cost_mode;
+    L.form = persist_form(b->seqs[0].cfg);
+    L.max_ppl = max_ppl;
+    L.smem_bytes = smem;
+    L.max_blocks = 0;
+    return PM_OK;
+}
+
+// One step of the persistent form for buffer set k: the inputs of every sequence on its own
+// stream, then the persistent kernel on the run stream, then every sequence's fusion step.
+cudaError_t enqueue_persist(pm_batch* b, int k) {
+    cudaError_t e;
+    for (int i = 0; i < (int)b->seqs.size(); ++i) {
+        Seq& q = b->seqs[i];
+        if ((e = cudaStreamWaitEvent(q.st[0], b->root, 0))) return e;
+        if ((e = enqueue_inputs(b, i, k, q.st[0]))) return e;
+        if ((e = cudaEventRecord(q.side.fork, q.st[0]))) return e;
+        if ((e = cudaStreamWaitEvent(b->run, q.side.fork, 0))) return e;
+    }
+    if ((e = cudaMemsetAsync(b->d_counters, 0, b->counter_bytes, b->run))) return e;
+    PersistLaunch L = b->plaunch;
+    L.seqs = b->d_pseq[k];
+    if ((e = launch_persist(L, b->run))) return e;
+    if ((e = cudaEventRecord(b->persist_done, b->run))) return e;
+    for (int i = 0; i < (int)b->seqs.size(); ++i) {
+        Seq& q = b->seqs[i];
+        if ((e = cudaStreamWaitEvent(q.st[0], b->persist_done, 0))) return e;
+        if ((e = enqueue_fusion(b, i, k, q.st[0]))) return e;
+        if ((e = cudaEventRecord(q.done, q.st[0]))) return e;
+        if ((e = cudaStreamWaitEvent(b->run, q.done, 0))) return e;
+    }
+    return cudaSuccess;
+}
+
 pm_status build_graphs(pm_batch* b) {
+    if (b->persistent) {
+        pm_status st = setup_persist(b);
+        if (st != PM_OK) return st;
+    }
     for (int k = 0; k < 2; ++k) {
         for (auto& l : b->lanes) l.last_user = -1;
         PB_CK(b, cudaStreamBeginCapture(b->run, cudaStreamCaptureModeThreadLocal));
         cudaError_t e = cudaEventRecord(b->root, b->run);
-        for (int i = 0; i < (int)b->seqs.size() && e == cudaSuccess; ++i) {
+        if (b->persistent && e == cudaSuccess) e = enqueue_persist(b, k);
+        for (int i = 0; !b->persistent && i < (int)b->seqs.size() && e == cudaSuccess; ++i) {
             Seq& q = b->seqs[i];
             e = cudaStreamWaitEvent(q.st[0], b->root, 0);
             if (e == cudaSuccess) e = enqueue_seq(b, i, k);
@@ -401,10 +579,19 @@ pm_status pm_batch_create(const pm_config* cfgs, int n, int num_sources, int lan
         if (cfgs[i].fusion_variant != PM_FUSION_GPU || cfgs[i].device != cfgs[0].device)
             return PM_ERR_UNSUPPORTED;
     }
+    if (flags & PM_BATCH_PERSISTENT) {   // one form for all sequences, each with its own volumes
+        if (lanes != 0) return PM_ERR_UNSUPPORTED;
+        for (int i = 1; i < n; ++i)
+            if (cfgs[i].precision != cfgs[0].precision || cfgs[i].sampler != cfgs[0].sampler ||
+                cfgs[i].cost_mode != cfgs[0].cost_mode)
+                return PM_ERR_UNSUPPORTED;
+        if (n > 65535) return PM_ERR_UNSUPPORTED;
+    }
     pm_batch* b = new pm_batch();
     b->S = num_sources;
     b->flags = flags;
     b->device = cfgs[0].device;
+    b->persistent = (flags & PM_BATCH_PERSISTENT) != 0;
     DevGuard dg(b->device);
     if (flags & PM_BATCH_PRIORITY) {
         int least = 0, greatest = 0;
@@ -419,6 +606,7 @@ pm_status pm_batch_create(const pm_config* cfgs, int n, int num_sources, int lan
     bool ok = note(cudaStreamCreateWithFlags(&b->run, cudaStreamNonBlocking)) &&
               note(cudaEventCreateWithFlags(&b->root, cudaEventDisableTiming)) &&
               note(cudaEventCreateWithFlags(&b->launched[0], cudaEventDisableTiming)) &&
+              note(cudaEventCreateWithFlags(&b->persist_done, cudaEventDisableTiming)) &&
               note(cudaEventCreateWithFlags(&b->launched[1], cudaEventDisableTiming));
     b->seqs.resize(n);
     // lanes: per distinct shape, `lanes` sets of cost + path volumes (0: one per sequence)
@@ -481,7 +669,7 @@ pm_status pm_batch_create(const pm_config* cfgs, int n, int num_sources, int lan
         }
     }
     pm_status tune = PM_OK;
-    if (ok && (flags & PM_BATCH_AUTOTUNE)) {
+    if (ok && (flags & PM_BATCH_AUTOTUNE) && !b->persistent) {
         tune = autotune(b);
         ok = tune == PM_OK;
     }
@@ -628,6 +816,11 @@ pm_status pm_batch_synchronize(pm_batch* b) {
     if (!b) return PM_ERR_INVALID_ARGUMENT;
     DevGuard dg(b->device);
     PB_CK(b, cudaStreamSynchronize(b->run));
+    if (b->persistent && b->d_counters && b->step > 0) {   // the last step's error word
+        unsigned err = 0;
+        PB_CK(b, cudaMemcpy(&err, b->d_counters + 4 * b->seqs.size() + 1, sizeof err, cudaMemcpyDeviceToHost));
+        if (err) return bfail(b, PM_ERR_CUDA, "persistent kernel: a dependency wait ran out; the step's outputs are invalid");
+    }
     return PM_OK;
 }
 

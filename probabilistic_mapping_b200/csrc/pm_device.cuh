@@ -148,22 +148,23 @@ template <int BYTES> __device__ __forceinline__ void cp_async_bytes(void* smem, 
 }
 
 // ---- plane vectors: a lane owns PPL consecutive planes -----------------------------------
-template <int PPL> __device__ __forceinline__ void load_planes(float (&v)[PPL], const float* p) {
+// CG: through L2 only (ld.global.cg), for data written earlier in the same launch by other blocks.
+template <int PPL, bool CG = false> __device__ __forceinline__ void load_planes(float (&v)[PPL], const float* p) {
     if constexpr (PPL % 4 == 0) {
 #pragma unroll
         for (int j = 0; j < PPL; j += 4) {
-            const float4 t = *reinterpret_cast<const float4*>(p + j);
+            const float4 t = CG ? __ldcg(reinterpret_cast<const float4*>(p + j)) : *reinterpret_cast<const float4*>(p + j);
             v[j] = t.x; v[j + 1] = t.y; v[j + 2] = t.z; v[j + 3] = t.w;
         }
     } else if constexpr (PPL % 2 == 0) {
 #pragma unroll
         for (int j = 0; j < PPL; j += 2) {
-            const float2 t = *reinterpret_cast<const float2*>(p + j);
+            const float2 t = CG ? __ldcg(reinterpret_cast<const float2*>(p + j)) : *reinterpret_cast<const float2*>(p + j);
             v[j] = t.x; v[j + 1] = t.y;
         }
     } else {
 #pragma unroll
-        for (int j = 0; j < PPL; ++j) v[j] = p[j];
+        for (int j = 0; j < PPL; ++j) v[j] = CG ? __ldcg(p + j) : p[j];
     }
 }
 template <int PPL> __device__ __forceinline__ void store_planes(float* p, const float (&v)[PPL]) {
