@@ -418,6 +418,7 @@ def run_mixed_plain_fp32(args, rank, world):
             cfgs.append(dict(width=w, height=h, num_planes=d))
             shapes.append(k)
     mine = shard_sequences(cfgs, world, MIXED_S)[rank]
+    stream = torch.cuda.Stream(device=dev)   # every mapper on it, so that its events bracket the work
     mappers, frames = {}, {}
     for k, (w, h, d, f) in enumerate(MIXED):
         if not any(shapes[i] == k for i in mine):
@@ -427,6 +428,7 @@ def run_mixed_plain_fp32(args, rank, world):
                          uniqueness_ratio=UNIQ, precision=0, device=dev)
         seq = [scene.make_sequence(w, h, f, MIXED_S, 2, seed=3000 + 10 * k + j) for j in range(2)]
         m.initIntrinsic(seq[0][0].K, 0.0, drho)
+        m.set_stream(stream.cuda_stream)
         mappers[k] = m
         frames[k] = [[(torch.from_numpy(fs.ref).cuda(), [torch.from_numpy(np.ascontiguousarray(x)).cuda()
                                                          for x in fs.srcs], fs) for fs in sq] for sq in seq]
@@ -447,10 +449,10 @@ def run_mixed_plain_fp32(args, rank, world):
         step(t)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
+    e0.record(stream)
     for t in range(args.steps):
         step(args.warmup + t)
-    e1.record()
+    e1.record(stream)
     torch.cuda.synchronize()
     for m in mappers.values():
         m.close()

@@ -74,8 +74,11 @@ __device__ __forceinline__ void run_ppl(int type, const PersistSeq& q, const Per
 #undef PM_PERSIST_CASE
 }
 
+// Three blocks per SM where every sequence has at most 128 planes (the cost tiles then run at the
+// stand-alone kernel's occupancy; 618 against 554 maps/s with two blocks at 640x480x128), two
+// where the 8-plane-per-lane bodies need the registers.
 template <int MODE, bool HALF, int SAMP, int MAXPPL>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, MAXPPL <= 4 ? 3 : 2)
 persist_kernel(const PersistSeq* __restrict__ seqs, const PersistItem* __restrict__ items, int n_items,
                unsigned* cnt, unsigned* head, unsigned* err) {
     extern __shared__ __align__(16) unsigned char smem[];
