@@ -213,6 +213,22 @@ __device__ __forceinline__ void fold2(float2& acc, float2& cn, float2 tmp, float
     cn = f2(v0 ? n1.x : cn.x, v1 ? n1.y : cn.y);
 }
 
+// The FP16 form's first pass (from initReference): the state holds the SUM of the sources'
+// tmp/9 terms and their count, and the mean is formed once when the tile is stored (sum_to_mean);
+// a rejected sum (NaN) adds nothing.  The reference's running mean (calc_cost.cu:200-207) and this
+// mean differ only by FP32 rounding, far below the FP16 volume's step.
+__device__ __forceinline__ void fold2_sum(float2& acc, float2& cn, float2 tmp, float r9) {
+    const bool v0 = tmp.x == tmp.x, v1 = tmp.y == tmp.y;
+    acc = __ffma2_rn(make_float2(v0 ? tmp.x : 0.0f, v1 ? tmp.y : 0.0f), make_float2(r9, r9), acc);
+    cn = __fadd2_rn(cn, make_float2(v0 ? 1.0f : 0.0f, v1 ? 1.0f : 0.0f));
+}
+__device__ __forceinline__ float sum_to_mean(float sum, float cnt) {
+    if (cnt == 0.0f) return -1.0f;   // never measured (initReference's -1, stereo_mapper.cpp:69)
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(cnt));
+    return __fmul_rn(sum, r);
+}
+
 // MODE 0: reference sample set (calc_cost.cu:83-199); MODE 1: corrected 3x3 patch.
 // One CTA's tile (bx, by) and 16-plane block bz of the volume; smem_raw holds Smem::BYTES.
 template <int MODE, bool HALF, int SAMP, bool INC>
@@ -239,7 +255,7 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
     // state of earlier calls), or the initReference state cost = -1, count = 0
     for (int e = tid; e < NPIX * PCB; e += NT) {
         const int p = e / PCB, k = e - p * PCB;
-        float c0 = -1.0f, n0 = 0.0f;
+        float c0 = (HALF && !INC) ? 0.0f : -1.0f, n0 = 0.0f;   // sum or running mean, count
         if (INC) {
             const int o = p / TXU, i = p - o * TXU;
             const int gx = x0 + i, gy = y0 + o;
@@ -334,7 +350,8 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
                 float2* const ap = accp + o * (TXU * SP / 2);
                 float2* const cp = cntp + o * (TXU * SP / 2);
                 float2 av = *ap, nv = *cp;
-                fold2<INC, HALF>(av, nv, f2(tx, ty), r9);
+                if constexpr (HALF && !INC) fold2_sum(av, nv, f2(tx, ty), r9);
+                else fold2<INC, HALF>(av, nv, f2(tx, ty), r9);
                 *ap = av;
                 *cp = nv;
             }
@@ -348,6 +365,13 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
     // store contiguous plane runs of the volume (plane-innermost layout)
     __syncthreads();
     if constexpr (HALF) {
+        if constexpr (!INC) {   // sums and counts to means
+            for (int e = tid; e < NPIX * PCB; e += NT) {
+                const int p = e / PCB, k = e - p * PCB;
+                accs[p * SP + k] = sum_to_mean(accs[p * SP + k], cnts[p * SP + k]);
+            }
+            __syncthreads();
+        }
         // per pixel and 16-plane block: the smallest measured cost of the block (0 when none is
         // measured) is stored beside the block, and the half volume holds the differences
         float* const s_off = reinterpret_cast<float*>(smem_raw + Smem::OFF);

@@ -507,21 +507,57 @@ __device__ __forceinline__ void combine_pixels(const SgmLaunch& a, long first, l
     uint32_t incl;
     uint16_t rk[PPL];
     lane_order<PPL>(a.order, lane, incl, rk);
-    auto loadp = [&](long pix, float (&s)[NP][PPL]) {
+    // raw 32-bit words of the lane's slice of each pair volume (FP16 pairs: two planes per word);
+    // the FP16 volumes are half the bytes per pixel, so PD pixels are kept in flight instead of one
+    constexpr int WPP = HIN ? PPL / 2 : PPL;
+    constexpr int PD = HIN ? 3 : 1;
+    auto loadw = [&](long pix, uint32_t (&w)[NP][WPP], float& off) {
         const size_t e = (size_t)pix * D + lane * PPL;
 #pragma unroll
         for (int g = 0; g < NP; ++g) {
-            if constexpr (HIN)
-                load_slice<PPL, true, CG>(s[g], reinterpret_cast<const unsigned char*>(static_cast<const __half*>(a.part[g]) + e));
-            else
-                load_planes<PPL, CG>(s[g], static_cast<const float*>(a.part[g]) + e);
+            const uint32_t* src = HIN ? reinterpret_cast<const uint32_t*>(static_cast<const __half*>(a.part[g]) + e)
+                                      : reinterpret_cast<const uint32_t*>(static_cast<const float*>(a.part[g]) + e);
+            if constexpr (WPP % 4 == 0) {
+#pragma unroll
+                for (int j = 0; j < WPP; j += 4) {
+                    const uint4 t = CG ? __ldcg(reinterpret_cast<const uint4*>(src + j)) : *reinterpret_cast<const uint4*>(src + j);
+                    w[g][j] = t.x; w[g][j + 1] = t.y; w[g][j + 2] = t.z; w[g][j + 3] = t.w;
+                }
+            } else if constexpr (WPP % 2 == 0) {
+#pragma unroll
+                for (int j = 0; j < WPP; j += 2) {
+                    const uint2 t = CG ? __ldcg(reinterpret_cast<const uint2*>(src + j)) : *reinterpret_cast<const uint2*>(src + j);
+                    w[g][j] = t.x; w[g][j + 1] = t.y;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < WPP; ++j) w[g][j] = CG ? __ldcg(src + j) : src[j];
+            }
+        }
+        off = a.offset ? (CG ? __ldcg(a.offset + pix) : __ldg(a.offset + pix)) : 0.0f;
+    };
+    auto unpack = [](const uint32_t (&w)[WPP], float (&v)[PPL]) {
+#pragma unroll
+        for (int j = 0; j < WPP; ++j) {
+            if constexpr (HIN) {
+                const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[j]));
+                v[2 * j] = f.x;
+                v[2 * j + 1] = f.y;
+            } else {
+                v[j] = __uint_as_float(w[j]);
+            }
         }
     };
-    long pix = first;
-    float cur[NP][PPL], nxt[NP][PPL];
-    if (pix < npix) loadp(pix, cur);
-    for (; pix < npix; pix += nw) {
-        if (pix + nw < npix) loadp(pix + nw, nxt);
+    uint32_t ring[PD + 1][NP][WPP];
+    float offr[PD + 1];
+#pragma unroll
+    for (int i = 0; i < PD; ++i)
+        if (first + i * nw < npix) loadw(first + i * nw, ring[i], offr[i]);
+    for (long pix = first; pix < npix; pix += nw) {
+        if (pix + PD * nw < npix) loadw(pix + PD * nw, ring[PD], offr[PD]);
+        float cur[NP][PPL];
+#pragma unroll
+        for (int g = 0; g < NP; ++g) unpack(ring[0][g], cur[g]);
         float o[PPL];
 #pragma unroll
         for (int j = 0; j < PPL; ++j) {
@@ -531,7 +567,7 @@ __device__ __forceinline__ void combine_pixels(const SgmLaunch& a, long first, l
                 o[j] = __fadd_rn(cur[0][j], cur[1][j]);
         }
         if (a.offset) {   // every path carries the FP16 volume's per-pixel shift once
-            const float sh = __fmul_rn((float)(2 * NP), CG ? __ldcg(a.offset + pix) : __ldg(a.offset + pix));
+            const float sh = __fmul_rn((float)(2 * NP), offr[0]);
 #pragma unroll
             for (int j = 0; j < PPL; ++j) o[j] = __fadd_rn(o[j], sh);
         }
@@ -550,9 +586,13 @@ __device__ __forceinline__ void combine_pixels(const SgmLaunch& a, long first, l
             }
         }
 #pragma unroll
-        for (int g = 0; g < NP; ++g)
+        for (int i = 0; i < PD; ++i) {
+            offr[i] = offr[i + 1];
 #pragma unroll
-            for (int j = 0; j < PPL; ++j) cur[g][j] = nxt[g][j];
+            for (int g = 0; g < NP; ++g)
+#pragma unroll
+                for (int j = 0; j < WPP; ++j) ring[i][g][j] = ring[i + 1][g][j];
+        }
     }
 }
 
