@@ -184,6 +184,42 @@ PM_API pm_status pm_get_homography(pm_mapper* h, int i, float out[12]);
 PM_API pm_status pm_enable_stage_timing(pm_mapper* h, int enable);
 PM_API pm_status pm_get_stage_times(pm_mapper* h, float* ms, int n);
 
+/* Per-map pixel counters (opt-in).  They replace the reference's debug prints and its
+ * commented-out counters (stereo_mapper.cpp:56-60, 329, 431, 565).  Each pm_output,
+ * pm_output_fusion and pm_output_case call clears them on the handle's stream.  Then:
+ *   - The winner-take-all filter (filter_cost.cu:37-51; not pm_output_case's debug argmin)
+ *     puts every pixel in one of five wta_* classes.
+ *   - A non-first pm_output_fusion step adds the fusion classes.  tf_* follow transformMap
+ *     (depth_fusion.cu:26-48, transformMapCPU stereo_mapper.cpp:274-326, cnt0..cnt4).
+ *     pred_* follow depth_predict (:107-137, depthPreditCPU :405-421, cnt0/cnt1).
+ *     upd_* follow depthUpdate (:161-219, depthUpdateCPU :466-556, cnt0..cnt4).
+ * pm_get_stats waits for the handle's stream.  It returns PM_ERR_BAD_STATE while counting is off.
+ * Counting adds a one-byte class store per pixel and a counting kernel (W*H bytes) to the
+ * winner-take-all, and shared-memory tallies to the fusion kernels.  Outputs do not change. */
+typedef struct pm_stats {
+    uint32_t wta_depth;       /* sub-pixel depth written */
+    uint32_t wta_no_overlap;  /* |min| < FLOAT_EPS: DEP_INF written */
+    uint32_t wta_border;      /* minimum at the first or last plane: 0 */
+    uint32_t wta_flat;        /* flat minimum (var_scale test): 0 */
+    uint32_t wta_ambiguous;   /* uniqueness test failed: 0 */
+    uint32_t tf_empty;        /* previous alpha < FLOAT_EPS */
+    uint32_t tf_outlier;      /* previous inlier ratio below 0.4 (CPU variant: 0.5) */
+    uint32_t tf_behind;       /* moved depth < FLOAT_EPS */
+    uint32_t tf_outside;      /* projects outside the image */
+    uint32_t tf_moved;        /* moved into the current keyframe */
+    uint32_t pred_none;       /* cell without a predecessor after hole filling */
+    uint32_t pred_copied;     /* cell that received a predicted state */
+    uint32_t pred_filled;     /* of pred_copied: the predecessor came from hole filling */
+    uint32_t upd_empty;       /* no prior state and no measurement */
+    uint32_t upd_init;        /* no prior state; the measurement starts one */
+    uint32_t upd_no_measurement; /* prior state, no measurement */
+    uint32_t upd_output;      /* Bayesian update; inlier ratio above the output threshold */
+    uint32_t upd_hidden;      /* Bayesian update; inlier ratio at or below it */
+} pm_stats;
+#define PM_STATS_WORDS 18
+PM_API pm_status pm_enable_stats(pm_mapper* h, int enable);
+PM_API pm_status pm_get_stats(pm_mapper* h, pm_stats* out);
+
 PM_API pm_status pm_synchronize(pm_mapper* h);
 
 /* Exhaustive self-check of the exact FP32 shortcuts in the kernels (no counterpart in the

@@ -63,6 +63,14 @@ public:
             check(pm_output_case(h_, output_case, depth, depth_pitch), "outputFusionCPU");
     }
     void wtaDepth(float* depth, size_t pitch_bytes) { check(pm_get_wta_depth(h_, depth, pitch_bytes), "wtaDepth"); }
+    // Pixel counters of the last output call (the reference's commented-out cnt0..cnt4 counters,
+    // stereo_mapper.cpp:329, 431, 565, and the winner-take-all outcomes).
+    void enableStats(bool on) { check(pm_enable_stats(h_, on ? 1 : 0), "enableStats"); }
+    pm_stats stats() {
+        pm_stats s;
+        check(pm_get_stats(h_, &s), "stats");
+        return s;
+    }
     void setStream(void* cuda_stream) { check(pm_set_stream(h_, cuda_stream), "setStream"); }
     void synchronize() { check(pm_synchronize(h_), "synchronize"); }
     pm_mapper* handle() const { return h_; }

@@ -95,11 +95,15 @@ def lib():
         L.orc_sgm_f32.argtypes = [pp, u8, f, f]
         L.orc_filter_f64.argtypes = [pp, d, d, i32]
         L.orc_filter_f32.argtypes = [pp, f, f, i32]
+        L.orc_filter_classes_f32.argtypes = [pp, f, f, i32, u8]
         L.orc_tree_order.argtypes = [ctypes.c_int, ctypes.c_int, i32, i32]
         L.orc_fuse_gpu_f64.argtypes = [ctypes.c_int, ctypes.c_int, f, f] + [d] * 9 + [i32]
         L.orc_fuse_gpu_f32.argtypes = [ctypes.c_int, ctypes.c_int, f, f] + [f] * 9 + [i32]
+        L.orc_fuse_gpu_counts_f32.argtypes = [ctypes.c_int, ctypes.c_int, f, f] + [f] * 9 + [i32, u32]
         L.orc_fuse_cpu.argtypes = [ctypes.c_int, ctypes.c_int, d, f, ctypes.c_int,
                                    f, f, f, f, f, u32]
+        L.orc_fuse_cpu_counts.argtypes = [ctypes.c_int, ctypes.c_int, d, f, ctypes.c_int,
+                                          f, f, f, f, f, u32, u32]
         L.orc_convert.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                   ctypes.c_int, ctypes.c_uint64]
         dp = P(OrcDiffParams)
@@ -186,6 +190,24 @@ def filter_cost(p: Params, vol: np.ndarray, prec="f64"):
     return depth, idx
 
 
+# pm_stats word order of the fusion counters (orc_fuse_gpu_counts_f32 / orc_fuse_cpu_counts)
+FUSION_COUNTS = ("tf_empty", "tf_outlier", "tf_behind", "tf_outside", "tf_moved",
+                 "pred_none", "pred_copied", "pred_filled",
+                 "upd_empty", "upd_init", "upd_no_measurement", "upd_output", "upd_hidden")
+WTA_CLASSES = ("wta_depth", "wta_no_overlap", "wta_border", "wta_flat", "wta_ambiguous")
+
+
+def filter_classes(p: Params, vol: np.ndarray):
+    """a5 in FP32 with each pixel's outcome: (depth, index, class (H, W) uint8 in WTA_CLASSES order)."""
+    vol = np.ascontiguousarray(vol, np.float32)
+    depth = np.empty((p.H, p.W), np.float32)
+    idx = np.empty((p.H, p.W), np.int32)
+    cls = np.empty((p.H, p.W), np.uint8)
+    lib().orc_filter_classes_f32(ctypes.byref(p.c()), _ptr(vol, ctypes.c_float), _ptr(depth, ctypes.c_float),
+                                 _ptr(idx, ctypes.c_int32), _ptr(cls, ctypes.c_uint8))
+    return depth, idx, cls
+
+
 def tree_order(D: int, compat: int = 1):
     rank = np.empty(D, np.int32)
     incl = np.empty(D, np.int32)
@@ -208,33 +230,47 @@ class FusionState:
         return FusionState(self.alpha.copy(), self.beta.copy(), self.mu.copy(), self.sigma.copy())
 
 
-def fuse_gpu(W, H, pose12, cam4, depth, pre: FusionState, cur: FusionState, prec="f32"):
+def fuse_gpu(W, H, pose12, cam4, depth, pre: FusionState, cur: FusionState, prec="f32", counts=None):
     """a6-a10: one depth_fuse call.  depth is updated in place and returned with the
-    filled propagation table; pre is modified in place like transformMap does."""
+    filled propagation table; pre is modified in place like transformMap does.  counts: an
+    optional dict that receives the step's FUSION_COUNTS (FP32 only)."""
     dt, ct = _dt(prec)
     pose = np.ascontiguousarray(pose12, np.float32)
     cam = np.ascontiguousarray(cam4, np.float32)
     table = np.zeros(W * H, np.int32)
     for a in (depth, pre.alpha, pre.beta, pre.mu, pre.sigma, cur.alpha, cur.beta, cur.mu, cur.sigma):
         assert a.dtype == dt and a.flags["C_CONTIGUOUS"]
-    fn = lib().orc_fuse_gpu_f64 if prec == "f64" else lib().orc_fuse_gpu_f32
-    fn(W, H, _ptr(pose, ctypes.c_float), _ptr(cam, ctypes.c_float), _ptr(depth, ct),
-       _ptr(pre.alpha, ct), _ptr(pre.beta, ct), _ptr(pre.mu, ct), _ptr(pre.sigma, ct),
-       _ptr(cur.alpha, ct), _ptr(cur.beta, ct), _ptr(cur.mu, ct), _ptr(cur.sigma, ct),
-       _ptr(table, ctypes.c_int32))
+    args = [W, H, _ptr(pose, ctypes.c_float), _ptr(cam, ctypes.c_float), _ptr(depth, ct),
+            _ptr(pre.alpha, ct), _ptr(pre.beta, ct), _ptr(pre.mu, ct), _ptr(pre.sigma, ct),
+            _ptr(cur.alpha, ct), _ptr(cur.beta, ct), _ptr(cur.mu, ct), _ptr(cur.sigma, ct),
+            _ptr(table, ctypes.c_int32)]
+    if counts is not None:
+        assert prec == "f32"
+        c = np.zeros(len(FUSION_COUNTS), np.uint32)
+        lib().orc_fuse_gpu_counts_f32(*args, _ptr(c, ctypes.c_uint32))
+        counts.update(zip(FUSION_COUNTS, (int(v) for v in c)))
+    else:
+        (lib().orc_fuse_gpu_f64 if prec == "f64" else lib().orc_fuse_gpu_f32)(*args)
     return depth, table
 
 
-def fuse_cpu(W, H, pose12, cam4, pre_index, result, state: dict):
+def fuse_cpu(W, H, pose12, cam4, pre_index, result, state: dict, counts=None):
     """a13: outputFusionCPU for a non-first frame; state holds 'alpha','beta','mu','sigma'
-    arrays of shape (2, H*W) float32 and 'table' (2, H*W) uint32."""
+    arrays of shape (2, H*W) float32 and 'table' (2, H*W) uint32.  counts: an optional dict that
+    receives the step's FUSION_COUNTS."""
     pose = _f64(pose12)
     cam = np.ascontiguousarray(cam4, np.float32)
     result = np.ascontiguousarray(result, np.float32).reshape(-1)
-    lib().orc_fuse_cpu(W, H, _ptr(pose, ctypes.c_double), _ptr(cam, ctypes.c_float), int(pre_index),
-                       _ptr(result, ctypes.c_float), _ptr(state["alpha"], ctypes.c_float),
-                       _ptr(state["beta"], ctypes.c_float), _ptr(state["mu"], ctypes.c_float),
-                       _ptr(state["sigma"], ctypes.c_float), _ptr(state["table"], ctypes.c_uint32))
+    args = [W, H, _ptr(pose, ctypes.c_double), _ptr(cam, ctypes.c_float), int(pre_index),
+            _ptr(result, ctypes.c_float), _ptr(state["alpha"], ctypes.c_float),
+            _ptr(state["beta"], ctypes.c_float), _ptr(state["mu"], ctypes.c_float),
+            _ptr(state["sigma"], ctypes.c_float), _ptr(state["table"], ctypes.c_uint32)]
+    if counts is not None:
+        c = np.zeros(len(FUSION_COUNTS), np.uint32)
+        lib().orc_fuse_cpu_counts(*args, _ptr(c, ctypes.c_uint32))
+        counts.update(zip(FUSION_COUNTS, (int(v) for v in c)))
+    else:
+        lib().orc_fuse_cpu(*args)
     return result
 
 
@@ -279,8 +315,15 @@ class Mapper:
         p = self.p
         cost, cnt = calc_cost(p, self.ref, np.stack(self.srcs), np.stack(self.homs), self.prec)
         vol = sgm(p, self.ref, cost, self.prec)
-        depth, idx = filter_cost(p, vol, self.prec)
-        return dict(cost=cost, cnt=cnt, sgm=vol, depth=depth, idx=idx)
+        st = dict(cost=cost, cnt=cnt, sgm=vol)
+        if self.prec == "f32":   # with the pm_stats counters of the step
+            depth, idx, cls = filter_classes(p, vol)
+            st["stats"] = {n: int(np.count_nonzero(cls == k)) for k, n in enumerate(WTA_CLASSES)}
+            st["stats"].update((n, 0) for n in FUSION_COUNTS)
+        else:
+            depth, idx = filter_cost(p, vol, self.prec)
+        st.update(depth=depth, idx=idx)
+        return st
 
     def output(self):
         return self.stages()["depth"]
@@ -307,12 +350,13 @@ class Mapper:
             pre = self.gstate[self.pre_index]
             cur = self.gstate[self.pre_index ^ 1]
             depth = np.ascontiguousarray(st["depth"], dt).reshape(-1).copy()
-            fuse_gpu(W, H, rel.astype(np.float32), cam, depth, pre, cur, "f64" if dt == np.float64 else "f32")
+            fuse_gpu(W, H, rel.astype(np.float32), cam, depth, pre, cur, "f64" if dt == np.float64 else "f32",
+                     counts=st.get("stats"))
             st["fused"] = depth.reshape(H, W)
             st["variance"] = cur.sigma.reshape(H, W).copy()
         else:
             res = np.ascontiguousarray(st["depth"], np.float32).reshape(-1).copy()
-            fuse_cpu(W, H, rel, cam, self.pre_index, res, self.cstate)
+            fuse_cpu(W, H, rel, cam, self.pre_index, res, self.cstate, counts=st.get("stats"))
             st["fused"] = res.reshape(H, W)
             st["variance"] = self.cstate["sigma"][self.pre_index ^ 1].reshape(H, W).copy()
         self.R_prev, self.t_prev = np.array(R, np.float64), np.array(t, np.float64)

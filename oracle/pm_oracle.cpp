@@ -329,8 +329,10 @@ void sgm_paths(const orc_params* p, const uint8_t* ref8, const S* C, const int* 
 }
 
 // a5 -- filter_cost.cu:3-55 (+ the uniqueness extension after the flatness test).
+// cls (optional): the pixel's outcome, 0 depth, 1 non-overlap, 2 border plane, 3 flat, 4 ambiguous
+// (the pm_stats winner-take-all classes).
 template <typename S>
-void filter(const orc_params* p, const S* sgmv, S* depth, int32_t* idx) {
+void filter(const orc_params* p, const S* sgmv, S* depth, int32_t* idx, uint8_t* cls = nullptr) {
     const int W = p->W, H = p->H, D = p->D;
     std::vector<int> rank, incl;
     tree_order(D, p->tree_compat, rank, incl);
@@ -347,12 +349,16 @@ void filter(const orc_params* p, const S* sgmv, S* depth, int32_t* idx) {
         }
         idx[i] = best;
         S out;
+        uint8_t k = 0;
         if ((double)mn < kFloatEps && (double)mn > -kFloatEps) {
             out = (S)kDepInf;                                   // situation 1 (:37-38)
+            k = 1;
         } else if (best == 0 || best == D - 1) {
             out = (S)0;                                         // situation 2 (:39-40)
+            k = 2;
         } else if (c[best - 1] + c[best + 1] < (S)2 * mn * vs) {
             out = (S)0;                                         // situation 3 (:41-42)
+            k = 3;
         } else {
             bool reject = false;
             if (uniq) {
@@ -363,6 +369,7 @@ void filter(const orc_params* p, const S* sgmv, S* depth, int32_t* idx) {
             }
             if (reject) {
                 out = (S)0;
+                k = 4;
             } else {
                 const S pre = c[best - 1], post = c[best + 1];
                 const S a = pre - (S)2 * mn + post;            // (:48)
@@ -372,6 +379,7 @@ void filter(const orc_params* p, const S* sgmv, S* depth, int32_t* idx) {
             }
         }
         depth[i] = out;
+        if (cls) cls[i] = k;
     }
 }
 
@@ -383,10 +391,14 @@ template <typename S> inline S normpdf(S x, S mu, S sig) {
 }
 
 // a6-a10 -- depth_fusion.cu:8-225 with the deterministic z-buffer / fill rule.
+// counts (optional, 13 words, the pm_stats fusion classes): transform empty, outlier, behind,
+// outside, moved; prediction none, copied, filled; update empty, init, no measurement, output,
+// hidden.
 template <typename S>
 void fuse_gpu(int W, int H, const float pose[12], const float cam[4], S* depth, S* pa, S* pb,
-              S* pm, S* ps, S* ca, S* cb, S* cm, S* cs, int32_t* table_out) {
+              S* pm, S* ps, S* ca, S* cb, S* cm, S* cs, int32_t* table_out, uint32_t* counts = nullptr) {
     const size_t N = (size_t)W * H;
+    uint32_t cnt[13] = {};
     const S r11 = pose[0], r12 = pose[1], r13 = pose[2], r21 = pose[3], r22 = pose[4],
             r23 = pose[5], r31 = pose[6], r32 = pose[7], r33 = pose[8], t1 = pose[9],
             t2 = pose[10], t3 = pose[11];
@@ -398,9 +410,9 @@ void fuse_gpu(int W, int H, const float pose[12], const float cam[4], S* depth, 
         for (int x = 0; x < W; ++x) {
             const int index = y * W + x;
             const S a = pa[index];
-            if ((double)a < kFloatEps) continue;                    // (:26)
+            if ((double)a < kFloatEps) { ++cnt[0]; continue; }     // (:26)
             const S b = pb[index];
-            if ((double)(a / (a + b)) < 0.4) continue;              // (:30)
+            if ((double)(a / (a + b)) < 0.4) { ++cnt[1]; continue; }   // (:30)
             const S dep = pm[index];
             const S px = ((S)x - cx) / fx * dep;                     // (:34)
             const S py = ((S)y - cy) / fy * dep;
@@ -410,10 +422,11 @@ void fuse_gpu(int W, int H, const float pose[12], const float cam[4], S* depth, 
             const S px2 = fmaT(r13, pz, fmaT(r12, py, r11 * px)) + t1;
             const S py2 = fmaT(r23, pz, fmaT(r22, py, r21 * px)) + t2;
             const S pz2 = fmaT(r33, pz, fmaT(r32, py, r31 * px)) + t3;
-            if ((double)pz2 < kFloatEps) continue;                  // (:40)
+            if ((double)pz2 < kFloatEps) { ++cnt[2]; continue; }  // (:40)
             const int x2 = (int)((double)fmaT(px2 / pz2, fx, cx) + 0.5);   // (:43), truncation
             const int y2 = (int)((double)fmaT(py2 / pz2, fy, cy) + 0.5);
-            if (x2 < 0 || x2 >= W || y2 < 0 || y2 >= H) continue;
+            if (x2 < 0 || x2 >= W || y2 < 0 || y2 >= H) { ++cnt[3]; continue; }
+            ++cnt[4];
             pm[index] = pz2;                                         // (:48)
             ps[index] = (S)((double)ps[index] + (double)pz2 * 0.05); // (:49)
             if (index == 0) continue;   // table value 0 means empty: pixel 0 never propagates
@@ -443,6 +456,8 @@ void fuse_gpu(int W, int H, const float pose[12], const float cam[4], S* depth, 
     // depth_predict (:107-137)
     for (size_t e = 0; e < N; ++e) {
         const int t = filled[e];
+        ++cnt[t == 0 ? 5 : 6];
+        if (t != 0 && table[e] == 0) ++cnt[7];
         if (t == 0) {
             ca[e] = (S)-1.0;
         } else {
@@ -456,14 +471,17 @@ void fuse_gpu(int W, int H, const float pose[12], const float cam[4], S* depth, 
         if ((double)ca[e] < kFloatEps) {                            // (:161)
             if ((double)d < kFloatEps) {
                 depth[e] = (S)0;
+                ++cnt[8];
             } else {
                 ca[e] = (S)10; cb[e] = (S)10; cm[e] = d; cs[e] = (S)2500;
+                ++cnt[9];
             }
             continue;
         }
         if ((double)d < kFloatEps) {                                // (:176)
             const S a = ca[e], b = cb[e];
             depth[e] = ((double)(a / (a + b)) > 0.6) ? cm[e] : (S)0;
+            ++cnt[10];
             continue;
         }
         const S a = ca[e], b = cb[e], miu = cm[e], sq = cs[e];
@@ -484,8 +502,11 @@ void fuse_gpu(int W, int H, const float pose[12], const float cam[4], S* depth, 
         const S a_p = (ee - f) / (f - ee / f);
         const S b_p = a_p * ((S)1 - f) / f;
         ca[e] = a_p; cb[e] = b_p; cm[e] = mu_p; cs[e] = sig_p;
-        depth[e] = ((double)(a / (a + b)) > 0.6) ? mu_p : (S)0;              // (:219)
+        const bool shown = (double)(a / (a + b)) > 0.6;                       // (:219)
+        depth[e] = shown ? mu_p : (S)0;
+        ++cnt[shown ? 11 : 12];
     }
+    if (counts) std::memcpy(counts, cnt, sizeof cnt);
 }
 
 }  // namespace
@@ -563,6 +584,9 @@ void orc_filter_f64(const orc_params* p, const double* s, double* depth, int32_t
 void orc_filter_f32(const orc_params* p, const float* s, float* depth, int32_t* idx) {
     filter<float>(p, s, depth, idx);
 }
+void orc_filter_classes_f32(const orc_params* p, const float* s, float* depth, int32_t* idx, uint8_t* cls) {
+    filter<float>(p, s, depth, idx, cls);
+}
 void orc_tree_order(int D, int compat, int32_t* rank, int32_t* incl) {
     std::vector<int> r, in;
     tree_order(D, compat, r, in);
@@ -578,15 +602,23 @@ void orc_fuse_gpu_f32(int W, int H, const float pose[12], const float cam[4], fl
                       float* cm, float* cs, int32_t* table) {
     fuse_gpu<float>(W, H, pose, cam, depth, pa, pb, pm, ps, ca, cb, cm, cs, table);
 }
+void orc_fuse_gpu_counts_f32(int W, int H, const float pose[12], const float cam[4], float* depth,
+                             float* pa, float* pb, float* pm, float* ps, float* ca, float* cb,
+                             float* cm, float* cs, int32_t* table, uint32_t* counts) {
+    fuse_gpu<float>(W, H, pose, cam, depth, pa, pb, pm, ps, ca, cb, cm, cs, table, counts);
+}
 
 // a13 -- the CPU fusion variant that evaluate.cc:260 runs (outputFusionCPU, non-first frame):
 // masks of stereo_mapper.cpp:743-760, depthFuseCPU (:568-587) = transformMapCPU (:246-330),
 // holeFillingCPU (:332-389), depthPreditCPU (:391-432), depthUpdateCPU (:439-566), then the
 // re-mask of :773-784.  Sequential, raster order, as in the reference.
-void orc_fuse_cpu(int W, int H, const double pose[12], const float cam[4], int pre,
-                  float* result, float* alpha, float* beta, float* mu, float* sigma,
-                  uint32_t* table) {
+// counts (optional): the 13 pm_stats fusion words, as fuse_gpu's, with transformMapCPU's
+// inlier threshold 0.5 (:278) and depthUpdateCPU's output test (:552-556).
+void orc_fuse_cpu_counts(int W, int H, const double pose[12], const float cam[4], int pre,
+                         float* result, float* alpha, float* beta, float* mu, float* sigma,
+                         uint32_t* table, uint32_t* counts) {
     const size_t N = (size_t)W * H;
+    uint32_t cnt[13] = {};
     const int cur = pre ^ 1;
     float* aP = alpha + N * pre; float* bP = beta + N * pre; float* mP = mu + N * pre; float* sP = sigma + N * pre;
     float* aC = alpha + N * cur; float* bC = beta + N * cur; float* mC = mu + N * cur; float* sC = sigma + N * cur;
@@ -603,8 +635,8 @@ void orc_fuse_cpu(int W, int H, const double pose[12], const float cam[4], int p
     for (int y = 0; y < H; ++y)
         for (int x = 0; x < W; ++x) {
             const size_t i = (size_t)y * W + x;
-            if ((double)aP[i] < kFloatEps) continue;
-            if ((double)(aP[i] / (aP[i] + bP[i])) < 0.5) continue;
+            if ((double)aP[i] < kFloatEps) { ++cnt[0]; continue; }
+            if ((double)(aP[i] / (aP[i] + bP[i])) < 0.5) { ++cnt[1]; continue; }
             const float depth = mP[i];
             const double p0 = (double)(((float)x - cx) / fx * depth);
             const double p1 = (double)(((float)y - cy) / fy * depth);
@@ -612,10 +644,11 @@ void orc_fuse_cpu(int W, int H, const double pose[12], const float cam[4], int p
             double q[3];
             for (int r = 0; r < 3; ++r)
                 q[r] = pose[3 * r] * p0 + pose[3 * r + 1] * p1 + pose[3 * r + 2] * p2 + pose[9 + r];
-            if (q[2] < kFloatEps) continue;
+            if (q[2] < kFloatEps) { ++cnt[2]; continue; }
             const int x2 = (int)(q[0] / q[2] * fx + cx + 0.5);
             const int y2 = (int)(q[1] / q[2] * fy + cy + 0.5);
-            if (x2 < 0 || x2 >= W || y2 < 0 || y2 >= H) continue;
+            if (x2 < 0 || x2 >= W || y2 < 0 || y2 >= H) { ++cnt[3]; continue; }
+            ++cnt[4];
             mP[i] = (float)q[2];
             sP[i] = (float)((double)sP[i] + q[2] * 0.05);
             uint32_t& cell = tab[(size_t)y2 * W + x2];
@@ -632,6 +665,8 @@ void orc_fuse_cpu(int W, int H, const double pose[12], const float cam[4], int p
     // holeFillingCPU (:332-389), expand_sz = 3
     const int ex = 3;
     std::vector<uint8_t> vst(N, 0);
+    std::vector<uint8_t> occupied(N);
+    for (size_t i = 0; i < N; ++i) occupied[i] = tab[i] != 0;
     for (int y = ex; y < H - ex; ++y)
         for (int x = ex; x < W - ex; ++x) {
             const size_t i = (size_t)y * W + x;
@@ -645,6 +680,8 @@ void orc_fuse_cpu(int W, int H, const double pose[12], const float cam[4], int p
         }
     // depthPreditCPU (:391-432)
     for (size_t i = 0; i < N; ++i) {
+        ++cnt[tab[i] == 0 ? 5 : 6];
+        if (tab[i] != 0 && !occupied[i]) ++cnt[7];
         if (tab[i] == 0) {
             aC[i] = 0.0f;
         } else {
@@ -660,14 +697,17 @@ void orc_fuse_cpu(int W, int H, const double pose[12], const float cam[4], int p
         if ((double)aC[i] < kFloatEps) {
             if ((double)d < kFloatEps) {
                 result[i] = 0; mC[i] = d;
+                ++cnt[8];
             } else {
                 result[i] = 0; aC[i] = 10.0f; bC[i] = 10.0f; mC[i] = d; sC[i] = 256.0f;
+                ++cnt[9];
             }
             continue;
         }
         if ((double)d < kFloatEps) {
             bC[i] = (float)((double)bC[i] + 1.0);
             result[i] = ((double)(aC[i] / (aC[i] + bC[i])) > thr) ? mC[i] : 0.0f;
+            ++cnt[10];
             continue;
         }
         const float a = aC[i], b = bC[i], miu = mC[i], sq = sC[i];
@@ -690,13 +730,22 @@ void orc_fuse_cpu(int W, int H, const double pose[12], const float cam[4], int p
         const float a_p = (e - f) / (f - e / f);
         const float b_p = a_p * (1.0f - f) / f;
         aC[i] = a_p; bC[i] = b_p; mC[i] = mu_p; sC[i] = sig_p;
-        result[i] = ((double)(a_p / (a_p + b_p)) > thr) ? mu_p : 0.0f;
+        const bool shown = (double)(a_p / (a_p + b_p)) > thr;
+        result[i] = shown ? mu_p : 0.0f;
+        ++cnt[shown ? 11 : 12];
     }
     // re-mask (:773-784)
     for (size_t i = 0; i < N; ++i) {
         if (mask[i] > 100) result[i] = 0.0f;
         if ((double)result[i] < 0.1) result[i] = 0.0f;
     }
+    if (counts) std::memcpy(counts, cnt, sizeof cnt);
+}
+
+void orc_fuse_cpu(int W, int H, const double pose[12], const float cam[4], int pre,
+                  float* result, float* alpha, float* beta, float* mu, float* sigma,
+                  uint32_t* table) {
+    orc_fuse_cpu_counts(W, H, pose, cam, pre, result, alpha, beta, mu, sigma, table, nullptr);
 }
 
 void orc_convert(int W, int H, const void* in, void* out, int flag, uint64_t pitch_bytes) {

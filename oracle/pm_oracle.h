@@ -71,6 +71,9 @@ void orc_sgm_f32(const orc_params* p, const uint8_t* ref, const float* cost, flo
  * (filter_cost.cu:3-55).  depth: W*H, idx: W*H WTA plane index. */
 void orc_filter_f64(const orc_params* p, const double* sgm, double* depth, int32_t* idx);
 void orc_filter_f32(const orc_params* p, const float* sgm, float* depth, int32_t* idx);
+/* The same with each pixel's outcome class: 0 depth, 1 non-overlap, 2 border plane, 3 flat,
+ * 4 ambiguous (the pm_stats winner-take-all classes). */
+void orc_filter_classes_f32(const orc_params* p, const float* sgm, float* depth, int32_t* idx, uint8_t* cls);
 
 /* Plane priority of the WTA reduction tree (filter_cost.cu:22-30): rank[d] (0 = wins ties)
  * and incl[d] (0 when the tree never compares plane d). */
@@ -87,6 +90,12 @@ void orc_fuse_gpu_f64(int W, int H, const float pose[12], const float cam[4], do
 void orc_fuse_gpu_f32(int W, int H, const float pose[12], const float cam[4], float* depth,
                       float* pa, float* pb, float* pm, float* ps,
                       float* ca, float* cb, float* cm, float* cs, int32_t* table);
+/* The same with the step's 13 pm_stats fusion counters: transform empty, outlier, behind,
+ * outside, moved (transformMap :26-48); prediction none, copied, filled (depth_predict
+ * :128-136, hole_filling); update empty, init, no measurement, output, hidden (:161-219). */
+void orc_fuse_gpu_counts_f32(int W, int H, const float pose[12], const float cam[4], float* depth,
+                             float* pa, float* pb, float* pm, float* ps,
+                             float* ca, float* cb, float* cm, float* cs, int32_t* table, uint32_t* counts);
 
 /* a13: CPU fusion variant (stereo_mapper.cpp:246-587) with the masking of
  * outputFusionCPU (stereo_mapper.cpp:743-784).  Sequential, as in the reference.
@@ -95,6 +104,11 @@ void orc_fuse_gpu_f32(int W, int H, const float pose[12], const float cam[4], fl
 void orc_fuse_cpu(int W, int H, const double pose[12], const float cam[4], int pre,
                   float* result, float* alpha, float* beta, float* mu, float* sigma,
                   uint32_t* table);
+/* The same with the 13 counters of orc_fuse_gpu_counts_f32, classified as transformMapCPU,
+ * depthPreditCPU and depthUpdateCPU count them (stereo_mapper.cpp:274-326, 405-421, 466-556). */
+void orc_fuse_cpu_counts(int W, int H, const double pose[12], const float cam[4], int pre,
+                         float* result, float* alpha, float* beta, float* mu, float* sigma,
+                         uint32_t* table, uint32_t* counts);
 
 /* a11: pitched <-> linear float copy (convert.cu:4-24), byte pitch. flag=1: linear->pitched. */
 void orc_convert(int W, int H, const void* in, void* out, int flag, uint64_t pitch_bytes);

@@ -65,6 +65,17 @@ class PmBuffers(ctypes.Structure):
                 ("wta_depth", ctypes.c_void_p), ("table", ctypes.c_void_p), ("cost_offset", ctypes.c_void_p)]
 
 
+# pm_stats, in the order of its fields (include/pm_stereo.h)
+STATS_FIELDS = ("wta_depth", "wta_no_overlap", "wta_border", "wta_flat", "wta_ambiguous",
+                "tf_empty", "tf_outlier", "tf_behind", "tf_outside", "tf_moved",
+                "pred_none", "pred_copied", "pred_filled",
+                "upd_empty", "upd_init", "upd_no_measurement", "upd_output", "upd_hidden")
+
+
+class PmStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in STATS_FIELDS]
+
+
 # Every exported entry point with its argument types; also the list the load test checks.
 _P, _VP, _SZ, _I, _F = ctypes.POINTER, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_float
 _D = _P(ctypes.c_double)
@@ -88,6 +99,8 @@ SIGNATURES = {
     "pm_get_homography": (_I, [_VP, _I, _P(ctypes.c_float)]),
     "pm_enable_stage_timing": (_I, [_VP, _I]),
     "pm_get_stage_times": (_I, [_VP, _P(ctypes.c_float), _I]),
+    "pm_enable_stats": (_I, [_VP, _I]),
+    "pm_get_stats": (_I, [_VP, _P(PmStats)]),
     "pm_synchronize": (_I, [_VP]),
     "pm_debug_check_arith": (_I, [_P(ctypes.c_uint64), _VP]),
     "pm_last_error": (ctypes.c_char_p, [_VP]),

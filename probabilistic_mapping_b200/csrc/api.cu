@@ -74,6 +74,10 @@ struct pm_mapper {
     bool ev_valid[PM_NUM_STAGES] = {};
     cudaEvent_t ev_cost_kernel = nullptr;   // end of the cost kernel alone (stage 0 minus the rebase)
     bool ev_cost_valid = false;
+
+    unsigned* d_stats = nullptr;   // pm_stats counters (kStatWords), allocated by pm_enable_stats
+    uint8_t* d_wta_class = nullptr;   // W*H winner-take-all class of each pixel (pm_stats)
+    bool stats = false;
 };
 
 namespace pm {
@@ -318,7 +322,17 @@ pm_status run_sgm_filter(pm_mapper* h) {
     a.depth = h->d_depth;
     a.depth_pitch = sizeof(float) * (size_t)c.width;
     a.index = h->d_idx;
+    a.wta_class = h->stats ? h->d_wta_class : nullptr;
     PM_CK(h, launch_sgm(a, kCombineFilter, h->stream, h->have_side ? &h->side : nullptr));
+    if (h->stats)
+        PM_CK(h, launch_count_classes(h->d_wta_class, (long)c.width * c.height, kWtaClasses, h->d_stats + kStatWta,
+                                      h->stream));
+    return PM_OK;
+}
+
+// pm_stats: every output call starts from zero counters
+pm_status clear_stats(pm_mapper* h) {
+    if (h->stats) PM_CK(h, cudaMemsetAsync(h->d_stats, 0, sizeof(unsigned) * kStatWords, h->stream));
     return PM_OK;
 }
 
@@ -374,6 +388,8 @@ void release(pm_mapper* h) {
     cudaFree(h->d_chead);
     cudaFree(h->d_cnext);
     cudaFree(h->d_ctab);
+    cudaFree(h->d_stats);
+    cudaFree(h->d_wta_class);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
     if (h->ev_cost_kernel) cudaEventDestroy(h->ev_cost_kernel);
@@ -558,8 +574,10 @@ pm_status pm_output(pm_mapper* h, float* depth, size_t pitch) {
     DeviceGuard g(h->cfg.device);
     for (bool& v : h->ev_valid) v = false;
     h->ev_cost_valid = false;
+    pm_status st = clear_stats(h);
+    if (st != PM_OK) return st;
     mark(h, 0);
-    pm_status st = evaluate_cost(h, false);
+    st = evaluate_cost(h, false);
     mark_done(h, 0);
     if (st == PM_OK) st = run_sgm_filter(h);
     mark_done(h, 1);
@@ -580,8 +598,10 @@ pm_status pm_output_case(pm_mapper* h, int output_case, float* result, size_t pi
     const pm_config& c = h->cfg;
     for (bool& v : h->ev_valid) v = false;
     h->ev_cost_valid = false;
+    pm_status st = clear_stats(h);
+    if (st != PM_OK) return st;
     mark(h, 0);
-    pm_status st = evaluate_cost(h, false);
+    st = evaluate_cost(h, false);
     mark_done(h, 0);
     if (st != PM_OK) return st;
     SgmLaunch a;
@@ -618,8 +638,10 @@ pm_status pm_output_fusion(pm_mapper* h, float* depth, size_t depth_pitch, float
     const size_t N = (size_t)W * H;
     for (bool& v : h->ev_valid) v = false;
     h->ev_cost_valid = false;
+    pm_status st = clear_stats(h);
+    if (st != PM_OK) return st;
     mark(h, 0);
-    pm_status st = evaluate_cost(h, false);
+    st = evaluate_cost(h, false);
     mark_done(h, 0);
     if (st == PM_OK) st = run_sgm_filter(h);
     mark_done(h, 1);
@@ -653,6 +675,7 @@ pm_status pm_output_fusion(pm_mapper* h, float* depth, size_t depth_pitch, float
         f.head = h->d_chead;
         f.next = h->d_cnext;
         f.tab0 = h->d_ctab;
+        f.stats = h->stats ? h->d_stats : nullptr;
         PM_CK(h, launch_fuse_cpu_variant(f, h->stream));
         std::memcpy(h->R_prev, R, sizeof h->R_prev);
         std::memcpy(h->t_prev, t, sizeof h->t_prev);
@@ -673,6 +696,7 @@ pm_status pm_output_fusion(pm_mapper* h, float* depth, size_t depth_pitch, float
         f.ztable = h->d_ztable;
         f.table = h->d_table;
         f.variance = h->d_var;
+        f.stats = h->stats ? h->d_stats : nullptr;
         PM_CK(h, launch_fuse_gpu(f, h->stream));
         std::memcpy(h->R_prev, R, sizeof h->R_prev);
         std::memcpy(h->t_prev, t, sizeof h->t_prev);
@@ -780,6 +804,30 @@ pm_status pm_get_stage_times(pm_mapper* h, float* ms, int n) {
         if (h->ev_valid[0] && h->ev_cost_valid)
             PM_CK(h, cudaEventElapsedTime(&ms[PM_NUM_STAGES], h->ev[0], h->ev_cost_kernel));
     }
+    return PM_OK;
+}
+
+static_assert(PM_STATS_WORDS == kStatWords && sizeof(pm_stats) == sizeof(unsigned) * kStatWords,
+              "pm_stats mirrors the device counter block");
+
+pm_status pm_enable_stats(pm_mapper* h, int enable) {
+    if (!h) return PM_ERR_INVALID_ARGUMENT;
+    DeviceGuard g(h->cfg.device);
+    if (enable && !h->d_stats) {
+        PM_CK(h, cudaMalloc(&h->d_wta_class, (size_t)h->cfg.width * h->cfg.height));
+        PM_CK(h, cudaMalloc(&h->d_stats, sizeof(unsigned) * kStatWords));
+        PM_CK(h, cudaMemsetAsync(h->d_stats, 0, sizeof(unsigned) * kStatWords, h->stream));
+    }
+    h->stats = enable != 0;
+    return PM_OK;
+}
+
+pm_status pm_get_stats(pm_mapper* h, pm_stats* out) {
+    if (!h || !out) return PM_ERR_INVALID_ARGUMENT;
+    if (!h->stats) return fail(h, PM_ERR_BAD_STATE, "pixel counters are not enabled");
+    DeviceGuard g(h->cfg.device);
+    PM_CK(h, cudaMemcpyAsync(out, h->d_stats, sizeof(pm_stats), cudaMemcpyDeviceToHost, h->stream));
+    PM_CK(h, cudaStreamSynchronize(h->stream));
     return PM_OK;
 }
 

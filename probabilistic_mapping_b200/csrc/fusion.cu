@@ -50,21 +50,18 @@ __device__ __forceinline__ FuseView view(const FuseLaunch& a) {
     return v;
 }
 
-__global__ void __launch_bounds__(256) fuse_transform_kernel(const FuseLaunch a) {
+// transformMap of one pixel; returns its pm_stats class (-1: not counted)
+__device__ __forceinline__ int transform_pixel(const FuseLaunch& a, const FuseView& v, int x, int y) {
     const int W = a.W, H = a.H;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
-    if (x >= W || y >= H) return;
     const int index = y * W + x;
-    const FuseView v = view(a);
     if (v.first) {   // first keyframe: both state sets start from zero (stereo_mapper.cpp:138-141)
         for (int k = 0; k < 4; ++k) a.state[0][k][index] = a.state[1][k][index] = 0.0f;
-        return;
+        return -1;
     }
     const float al = v.pre[0][index];
-    if ((double)al < kFloatEps) return;                                    // (:26)
+    if ((double)al < kFloatEps) return kTfEmpty;                           // (:26)
     const float be = v.pre[1][index];
-    if ((double)__fdiv_rn(al, __fadd_rn(al, be)) < 0.4) return;            // (:30)
+    if ((double)__fdiv_rn(al, __fadd_rn(al, be)) < 0.4) return kTfOutlier; // (:30)
     const float dep = v.pre[2][index];
     const float fx = v.cam[0], fy = v.cam[1], cx = v.cam[2], cy = v.cam[3];
     const float px = __fmul_rn(__fdiv_rn(__fsub_rn((float)x, cx), fx), dep);   // (:34)
@@ -76,15 +73,24 @@ __global__ void __launch_bounds__(256) fuse_transform_kernel(const FuseLaunch a)
     const float px2 = __fadd_rn(__fmaf_rn(p[2], pz, __fmaf_rn(p[1], py, __fmul_rn(p[0], px))), p[9]);
     const float py2 = __fadd_rn(__fmaf_rn(p[5], pz, __fmaf_rn(p[4], py, __fmul_rn(p[3], px))), p[10]);
     const float pz2 = __fadd_rn(__fmaf_rn(p[8], pz, __fmaf_rn(p[7], py, __fmul_rn(p[6], px))), p[11]);
-    if ((double)pz2 < kFloatEps) return;                                   // (:40)
+    if ((double)pz2 < kFloatEps) return kTfBehind;                         // (:40)
     const int x2 = __double2int_rz(__dadd_rn((double)__fmaf_rn(__fdiv_rn(px2, pz2), fx, cx), 0.5));   // (:43)
     const int y2 = __double2int_rz(__dadd_rn((double)__fmaf_rn(__fdiv_rn(py2, pz2), fy, cy), 0.5));
-    if (x2 < 0 || x2 >= W || y2 < 0 || y2 >= H) return;
+    if (x2 < 0 || x2 >= W || y2 < 0 || y2 >= H) return kTfOutside;
     v.pre[2][index] = pz2;                                                 // (:48)
     v.pre[3][index] = __double2float_rn(__dadd_rn((double)v.pre[3][index], __dmul_rn((double)pz2, 0.05)));
-    if (index == 0) return;   // index 0 encodes "empty" in the reference's table
+    if (index == 0) return kTfMoved;   // index 0 encodes "empty" in the reference's table
     const unsigned long long key = ((unsigned long long)__float_as_uint(pz2) << 32) | (unsigned)index;
     atomicMin(a.ztable + (size_t)y2 * W + x2, key);
+    return kTfMoved;
+}
+
+__global__ void __launch_bounds__(256) fuse_transform_kernel(const FuseLaunch a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const bool in = x < a.W && y < a.H;
+    const int cls = in ? transform_pixel(a, view(a), x, y) : -1;
+    if (a.stats) tally_block<kTfClasses>(a.stats + kStatTf, cls);
 }
 
 __device__ __forceinline__ float normpdf(float x, float mu, float sig) {   // (:3-6)
@@ -93,24 +99,23 @@ __device__ __forceinline__ float normpdf(float x, float mu, float sig) {   // (:
                      rsqrtf(__double2float_rn(__dmul_rn(2.0 * M_PI, (double)sig))));
 }
 
-__global__ void __launch_bounds__(256) fuse_update_kernel(const FuseLaunch a) {
+// Hole filling, depth_predict and depthUpdate of one cell; returns its pm_stats classes
+// (prediction: 0 none, 1 copied, 2 copied from hole filling; update: UpdateClass) or -1s.
+__device__ __forceinline__ int2 update_pixel(const FuseLaunch& a, const FuseView& v, int x, int y) {
     const int W = a.W, H = a.H;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
-    if (x >= W || y >= H) return;
     const int e = y * W + x;
-    const FuseView v = view(a);
     if (v.first) {   // first keyframe: the fused map and its variance are zero
         a.depth[e] = 0.0f;
         if (a.variance) a.variance[e] = 0.0f;
         if (a.table) a.table[e] = 0;
-        return;
+        return make_int2(-1, -1);
     }
 
     // hole filling (:80-105): an empty cell takes the last occupied interior neighbour in
     // raster order, the writer whose own 3x3 loop (:96-103) reaches it first
     const unsigned long long k0 = a.ztable[e];
     int t = k0 == kEmpty ? 0 : (int)(unsigned)(k0 & 0xffffffffu);
+    const bool direct = t != 0;
     if (t == 0) {
         for (int i = 1; i >= -1 && t == 0; --i)
             for (int j = 1; j >= -1; --j) {
@@ -135,15 +140,19 @@ __global__ void __launch_bounds__(256) fuse_update_kernel(const FuseLaunch a) {
     const float unc = __double2float_rn(__dmul_rn((double)__fmul_rn(d, d), 0.01));   // (:151)
     float out_d = d;
     bool write_all = (t != 0);   // predict copied the whole state
+    int ucls;
     if ((double)ca < kFloatEps) {                                           // (:161)
         if ((double)d < kFloatEps) {
             out_d = 0.0f;
+            ucls = kUpdEmpty;
         } else {
             ca = 10.0f; cb = 10.0f; cm = d; cs = 2500.0f;
             write_all = true;
+            ucls = kUpdInit;
         }
     } else if ((double)d < kFloatEps) {                                     // (:176)
         out_d = ((double)__fdiv_rn(ca, __fadd_rn(ca, cb)) > 0.6) ? cm : 0.0f;
+        ucls = kUpdNoMeasurement;
     } else {
         const float aa = ca, bb = cb, miu = cm, sq = cs;
         const float us = __fadd_rn(unc, sq);
@@ -171,12 +180,26 @@ __global__ void __launch_bounds__(256) fuse_update_kernel(const FuseLaunch a) {
         const float b_p = __fdiv_rn(__fmul_rn(a_p, __fsub_rn(1.0f, f)), f);
         ca = a_p; cb = b_p; cm = mu_p; cs = sig_p;
         write_all = true;
-        out_d = ((double)__fdiv_rn(aa, ab) > 0.6) ? mu_p : 0.0f;             // (:219)
+        const bool shown = (double)__fdiv_rn(aa, ab) > 0.6;                  // (:219)
+        out_d = shown ? mu_p : 0.0f;
+        ucls = shown ? kUpdOutput : kUpdHidden;
     }
     v.cur[0][e] = ca;
     if (write_all) { v.cur[1][e] = cb; v.cur[2][e] = cm; v.cur[3][e] = cs; }
     a.depth[e] = out_d;
     if (a.variance) a.variance[e] = write_all ? cs : v.cur[3][e];
+    return make_int2(t == 0 ? 0 : direct ? 1 : 2, ucls);
+}
+
+__global__ void __launch_bounds__(256) fuse_update_kernel(const FuseLaunch a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const bool in = x < a.W && y < a.H;
+    const int2 cls = in ? update_pixel(a, view(a), x, y) : make_int2(-1, -1);
+    // prediction words none, copied, filled, then the update classes (kStatUpd = kStatPred + 3)
+    if (a.stats)
+        tally_block<3 + kUpdClasses>(a.stats + kStatPred, cls.x < 0 ? -1 : cls.x == 0 ? 0 : 1,
+                                     cls.x == 2 ? 2 : -1, cls.y < 0 ? -1 : 3 + cls.y);
 }
 
 }  // namespace

@@ -25,10 +25,8 @@ constexpr int kExpand = 3;   // expand_sz of holeFillingCPU (:334)
 __device__ __forceinline__ uint32_t pack(int x, int y) { return ((uint32_t)y << 16) | (uint32_t)x; }
 
 // masks (:743-760) and transformMapCPU's per-pixel part (:246-312); pushes the pixel onto its
-// target cell's list
-__global__ void __launch_bounds__(256) cpu_transform_kernel(const FuseCpuLaunch a) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= a.W || y >= a.H) return;
+// target cell's list.  Returns the pixel's pm_stats class (transformMapCPU's cnt0..cnt4).
+__device__ __forceinline__ int cpu_transform_pixel(const FuseCpuLaunch& a, int x, int y) {
     const int i = y * a.W + x;
     float r = a.result[i];
     uint8_t m = 0;
@@ -37,8 +35,8 @@ __global__ void __launch_bounds__(256) cpu_transform_kernel(const FuseCpuLaunch 
     a.result[i] = r;
     a.mask[i] = m;
     const float al = a.pre[0][i], be = a.pre[1][i];
-    if ((double)al < kFloatEps) return;
-    if ((double)__fdiv_rn(al, __fadd_rn(al, be)) < 0.5) return;
+    if ((double)al < kFloatEps) return kTfEmpty;
+    if ((double)__fdiv_rn(al, __fadd_rn(al, be)) < 0.5) return kTfOutlier;
     const float depth = a.pre[2][i];
     const float fx = a.cam[0], fy = a.cam[1], cx = a.cam[2], cy = a.cam[3];
     const double p0 = (double)__fmul_rn(__fdiv_rn(__fsub_rn((float)x, cx), fx), depth);
@@ -49,15 +47,22 @@ __global__ void __launch_bounds__(256) cpu_transform_kernel(const FuseCpuLaunch 
         q[k] = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(a.pose[3 * k], p0), __dmul_rn(a.pose[3 * k + 1], p1)),
                                    __dmul_rn(a.pose[3 * k + 2], p2)),
                          a.pose[9 + k]);
-    if (q[2] < kFloatEps) return;
+    if (q[2] < kFloatEps) return kTfBehind;
     const int x2 = __double2int_rz(__dadd_rn(__dadd_rn(__dmul_rn(__ddiv_rn(q[0], q[2]), (double)fx), (double)cx), 0.5));
     const int y2 = __double2int_rz(__dadd_rn(__dadd_rn(__dmul_rn(__ddiv_rn(q[1], q[2]), (double)fy), (double)cy), 0.5));
-    if (x2 < 0 || x2 >= a.W || y2 < 0 || y2 >= a.H) return;
+    if (x2 < 0 || x2 >= a.W || y2 < 0 || y2 >= a.H) return kTfOutside;
     a.orig_mu[i] = depth;
     a.pre[2][i] = __double2float_rn(q[2]);
     a.pre[3][i] = __double2float_rn(__dadd_rn((double)a.pre[3][i], __dmul_rn(q[2], 0.05)));
     const int cell = y2 * a.W + x2;
     a.next[i] = atomicExch(a.head + cell, i);
+    return kTfMoved;
+}
+
+__global__ void __launch_bounds__(256) cpu_transform_kernel(const FuseCpuLaunch a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    const int cls = x < a.W && y < a.H ? cpu_transform_pixel(a, x, y) : -1;
+    if (a.stats) tally_block<kTfClasses>(a.stats + kStatTf, cls);
 }
 
 // The z-test of :313-328 replayed per cell in raster order of its hitters.
@@ -96,12 +101,12 @@ __device__ __forceinline__ float normpdf_cpu(float x, float mu, float var) {   /
     return __double2float_rn(__dmul_rn((double)expf(arg), __dsqrt_rn(__dmul_rn(2.0 * M_PI, (double)var))));
 }
 
-// holeFillingCPU (gather), depthPreditCPU, depthUpdateCPU and the re-mask, one pixel per thread.
-__global__ void __launch_bounds__(256) cpu_update_kernel(const FuseCpuLaunch a) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= a.W || y >= a.H) return;
+// holeFillingCPU (gather), depthPreditCPU, depthUpdateCPU and the re-mask of one pixel.  Returns
+// its pm_stats words relative to kStatPred: (none 0 / copied 1, filled 2 or -1, 3 + update class).
+__device__ __forceinline__ int3 cpu_update_pixel(const FuseCpuLaunch& a, int x, int y) {
     const int i = y * a.W + x;
     uint32_t t = a.tab0[i];
+    const bool direct = t != 0;
     if (t == 0) {
         for (int dy = -kExpand; dy <= kExpand && t == 0; ++dy)
             for (int dx = -kExpand; dx <= kExpand; ++dx) {
@@ -124,16 +129,20 @@ __global__ void __launch_bounds__(256) cpu_update_kernel(const FuseCpuLaunch a) 
     const float d = a.result[i];
     const float unc = 64.0f;
     float res;
+    int ucls;
     if ((double)ca < kFloatEps) {
         res = 0.0f;
         if ((double)d < kFloatEps) {
             cm = d;
+            ucls = kUpdEmpty;
         } else {
             ca = 10.0f; cb = 10.0f; cm = d; cs = 256.0f;
+            ucls = kUpdInit;
         }
     } else if ((double)d < kFloatEps) {
         cb = __double2float_rn(__dadd_rn((double)cb, 1.0));
         res = ((double)__fdiv_rn(ca, __fadd_rn(ca, cb)) > 0.51) ? cm : 0.0f;
+        ucls = kUpdNoMeasurement;
     } else {
         const float aa = ca, bb = cb, miu = cm, sq = cs;
         const float us = __fadd_rn(unc, sq);
@@ -158,7 +167,9 @@ __global__ void __launch_bounds__(256) cpu_update_kernel(const FuseCpuLaunch a) 
         const float a_p = __fdiv_rn(__fsub_rn(e, f), __fsub_rn(f, __fdiv_rn(e, f)));
         const float b_p = __fdiv_rn(__fmul_rn(a_p, __fsub_rn(1.0f, f)), f);
         ca = a_p; cb = b_p; cm = mu_p; cs = sig_p;
-        res = ((double)__fdiv_rn(a_p, __fadd_rn(a_p, b_p)) > 0.51) ? mu_p : 0.0f;
+        const bool shown = (double)__fdiv_rn(a_p, __fadd_rn(a_p, b_p)) > 0.51;
+        res = shown ? mu_p : 0.0f;
+        ucls = shown ? kUpdOutput : kUpdHidden;
     }
     a.cur[0][i] = ca;
     a.cur[1][i] = cb;
@@ -169,6 +180,13 @@ __global__ void __launch_bounds__(256) cpu_update_kernel(const FuseCpuLaunch a) 
     if ((double)res < 0.1) res = 0.0f;
     a.result[i] = res;
     if (a.variance) a.variance[i] = cs;
+    return make_int3(t == 0 ? 0 : 1, t != 0 && !direct ? 2 : -1, 3 + ucls);
+}
+
+__global__ void __launch_bounds__(256) cpu_update_kernel(const FuseCpuLaunch a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    const int3 c = x < a.W && y < a.H ? cpu_update_pixel(a, x, y) : make_int3(-1, -1, -1);
+    if (a.stats) tally_block<3 + kUpdClasses>(a.stats + kStatPred, c.x, c.y, c.z);
 }
 
 }  // namespace

@@ -19,6 +19,21 @@ constexpr unsigned kFull = 0xffffffffu;
 __device__ __forceinline__ float nan_f() { return __int_as_float(0x7fffffff); }
 __device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
 
+// pm_stats counters: adds one to each of a thread's words c0, c1, c2 (each in [0, N), or -1 for
+// none) of the N global counters at g.  The block's counts meet in shared memory first, then one
+// global add per word and block.  Every thread of the block calls it.
+template <int N>
+__device__ __forceinline__ void tally_block(unsigned* g, int c0, int c1 = -1, int c2 = -1) {
+    __shared__ unsigned s[N];
+    if (threadIdx.x < N) s[threadIdx.x] = 0u;
+    __syncthreads();
+    if (c0 >= 0) atomicAdd(&s[c0], 1u);
+    if (c1 >= 0) atomicAdd(&s[c1], 1u);
+    if (c2 >= 0) atomicAdd(&s[c2], 1u);
+    __syncthreads();
+    if (threadIdx.x < N && s[threadIdx.x]) atomicAdd(g + threadIdx.x, s[threadIdx.x]);
+}
+
 // Homography of one source frame as kernel arguments (the 12 floats of ad_calc_cost,
 // calc_cost.cu:212-219).
 struct Hom {

@@ -13,6 +13,16 @@ constexpr float kDepInf = 1000.0f;   // DEP_INF (parameters.h:29)
 constexpr double kFloatEps = 1e-5;   // FLOAT_EPS (parameters.h:6)
 constexpr float kCaseInf = 10000.0f; // no-overlap value of the CASE 0/1 debug outputs (stereo_mapper.cpp:651)
 
+// Per-map pixel counters (pm_stats): word offsets of the classes in the device counter block.
+enum WtaClass { kWtaDepth = 0, kWtaNoOverlap, kWtaBorder, kWtaFlat, kWtaAmbiguous, kWtaClasses };
+enum TransformClass { kTfEmpty = 0, kTfOutlier, kTfBehind, kTfOutside, kTfMoved, kTfClasses };
+enum UpdateClass { kUpdEmpty = 0, kUpdInit, kUpdNoMeasurement, kUpdOutput, kUpdHidden, kUpdClasses };
+constexpr int kStatWta = 0;
+constexpr int kStatTf = kStatWta + kWtaClasses;
+constexpr int kStatPred = kStatTf + kTfClasses;   // none, copied, filled
+constexpr int kStatUpd = kStatPred + 3;
+constexpr int kStatWords = kStatUpd + kUpdClasses;
+
 // ---- plane-sweep cost volume (calc_cost.cu) ----------------------------------------------
 struct CostLaunch {
     const float* ref;      // W*H scaled reference image
@@ -77,7 +87,10 @@ struct SgmLaunch {
     int pair_warps;        // scanlines per block of the path-pair kernel: 2, 4 or 8 (0: 2)
     int serial_pairs;      // 1: run the path pairs one after another on the caller's stream
     int priority;          // launch priority of the pair and combine kernels (0: the stream's)
+    uint8_t* wta_class;    // W*H winner-take-all class of each pixel (WtaClass, fused filter only), or nullptr
 };
+// pm_stats: adds the per-pixel classes (values below n) of npix pixels to the n counters at g.
+cudaError_t launch_count_classes(const uint8_t* cls, long npix, int n, unsigned* g, cudaStream_t s);
 // Side streams for the concurrent path pairs: pairs 0..2 fork from the caller's stream and join
 // back before the combine kernel.
 struct SgmStreams {
@@ -145,6 +158,7 @@ struct FuseLaunch {
     const float* params_dev;
     const int* flags_dev;
     float* state[2][4];
+    unsigned* stats;       // kStatWords counters (transform, predict and update classes added), or nullptr
 };
 cudaError_t launch_fuse_gpu(const FuseLaunch& a, cudaStream_t s);
 
@@ -164,6 +178,7 @@ struct FuseCpuLaunch {
     int* head;
     int* next;
     uint32_t* tab0;
+    unsigned* stats;       // kStatWords counters, or nullptr
 };
 cudaError_t launch_fuse_cpu_variant(const FuseCpuLaunch& a, cudaStream_t s);
 

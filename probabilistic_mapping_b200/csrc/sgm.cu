@@ -73,11 +73,36 @@ __global__ void __launch_bounds__(NW * 32) sgm_pair_kernel(const SgmLaunch a, in
     sgm_pair_block<PPL, HALF, NW, FULL, HOUT>(a, dx, dy, slot, blockIdx.x, ring);
 }
 
+// Blocks per SM that the combine kernel is held to (0: no bound): D = 192 in FP32 and D = 256 in FP16
+// with four paths, where the compiler's default register choice leaves one block per SM fewer.
+constexpr int combine_min_blocks(int ppl, int np, bool hin) {
+    return ppl == 6 && !hin ? (np == 2 ? 4 : 3) : ppl == 8 && hin && np == 2 ? 3 : 0;
+}
+
 // grid-stride over the image's pixels, one warp per pixel
 template <int PPL, int MODE, int NP, bool HIN>
-__global__ void __launch_bounds__(256) combine_kernel(const SgmLaunch a) {
+__global__ void __launch_bounds__(256, combine_min_blocks(PPL, NP, HIN)) combine_kernel(const SgmLaunch a) {
     combine_pixels<PPL, MODE, NP, HIN, false>(a, (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5),
                                               (long)gridDim.x * (blockDim.x >> 5), (long)a.W * a.H);
+}
+
+// pm_stats: the histogram of a per-pixel class array (classes below n <= 8), one ballot per class
+// and 32 pixels, summed per block in shared memory
+__global__ void __launch_bounds__(256) count_classes_kernel(const uint8_t* __restrict__ cls, long npix, int n,
+                                                            unsigned* g) {
+    __shared__ unsigned s[8];
+    if (threadIdx.x < 8) s[threadIdx.x] = 0u;
+    __syncthreads();
+    for (long base = (long)blockIdx.x * blockDim.x; base < npix; base += (long)gridDim.x * blockDim.x) {
+        const long i = base + threadIdx.x;
+        const int v = i < npix ? (int)cls[i] : -1;
+        for (int c = 0; c < n; ++c) {
+            const unsigned m = __ballot_sync(kFull, v == c);
+            if ((threadIdx.x & 31) == 0 && m) atomicAdd(&s[c], (unsigned)__popc(m));
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < n && s[threadIdx.x]) atomicAdd(g + threadIdx.x, s[threadIdx.x]);
 }
 
 template <int PPL>
@@ -93,8 +118,8 @@ __global__ void __launch_bounds__(128) filter_kernel(const float* __restrict__ s
     float s[PPL];
     load_planes<PPL>(s, sum + (size_t)pix * D + lane * PPL);
     float dep;
-    int idx;
-    wta_filter<PPL>(s, incl, rk, lane, D, fp, dep, idx);
+    int idx, cls;
+    wta_filter<PPL>(s, incl, rk, lane, D, fp, dep, idx, cls);
     if (lane == 0) {
         const int y = (int)(pix / W), x = (int)(pix - (long)y * W);
         *reinterpret_cast<float*>(reinterpret_cast<char*>(depth) + (size_t)y * pitch + (size_t)x * 4) = dep;
@@ -312,6 +337,14 @@ cudaError_t launch_case_argmin(const void* vol, int half, const float* offset, i
 #undef PM_CASE_PPL
         default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t launch_count_classes(const uint8_t* cls, long npix, int n, unsigned* g, cudaStream_t s) {
+    if (n < 1 || n > 8 || npix < 0) return cudaErrorInvalidValue;
+    if (npix == 0) return cudaSuccess;
+    const long blocks = (npix + 255) / 256;
+    count_classes_kernel<<<(unsigned)(blocks < 592 ? blocks : 592), 256, 0, s>>>(cls, npix, n, g);
+    return cudaGetLastError();
 }
 
 }  // namespace pm

@@ -76,7 +76,7 @@ __device__ __forceinline__ void lane_order(const PlaneOrder& o, int lane, uint32
 template <int PPL>
 __device__ __forceinline__ void wta_filter(const float (&s)[PPL], uint32_t incl, const uint16_t (&rk)[PPL],
                                            int lane, int D, const FilterParams& fp, float& depth_out,
-                                           int& idx_out) {
+                                           int& idx_out, int& cls_out) {
     float lmin = inf_f();
 #pragma unroll
     for (int j = 0; j < PPL; ++j)
@@ -92,14 +92,18 @@ __device__ __forceinline__ void wta_filter(const float (&s)[PPL], uint32_t incl,
     const int idx = __shfl_sync(kFull, lane * PPL + lj, __ffs(ball) - 1);
 
     float depth;
+    int cls = kWtaDepth;
     if ((double)mn < kFloatEps && (double)mn > -kFloatEps) {
         depth = kDepInf;                                   // non-overlap (:37-38)
+        cls = kWtaNoOverlap;
     } else if (idx == 0 || idx == D - 1) {
         depth = 0.0f;                                      // border plane (:39-40)
+        cls = kWtaBorder;
     } else {
         const float pre = plane_value(s, idx - 1), post = plane_value(s, idx + 1);
         if (__fadd_rn(pre, post) < __fmul_rn(__fmul_rn(2.0f, mn), fp.var_scale)) {
             depth = 0.0f;                                  // flat minimum (:41-42)
+            cls = kWtaFlat;
         } else {
             bool reject = false;
             if (fp.uniq > 0.0f && fp.uniq < 1.0f) {
@@ -114,6 +118,7 @@ __device__ __forceinline__ void wta_filter(const float (&s)[PPL], uint32_t incl,
             }
             if (reject) {
                 depth = 0.0f;
+                cls = kWtaAmbiguous;
             } else {                                       // parabola (:45-51)
                 const float a2 = __fadd_rn(__fsub_rn(pre, __fmul_rn(2.0f, mn)), post);
                 const float b = __fadd_rn(-pre, post);
@@ -124,6 +129,7 @@ __device__ __forceinline__ void wta_filter(const float (&s)[PPL], uint32_t incl,
     }
     depth_out = depth;
     idx_out = idx;
+    cls_out = cls;
 }
 
 // The debug winner-take-all of outputFusionCPU's CASE 0 and CASE 1 (stereo_mapper.cpp:636-660,
@@ -576,13 +582,15 @@ __device__ __forceinline__ void combine_pixels(const SgmLaunch& a, long first, l
         if constexpr (MODE != kCombineStore) {
             float depth;
             int idx;
-            if constexpr (MODE == kCombineFilter) wta_filter<PPL>(o, incl, rk, lane, D, a.fp, depth, idx);
+            int cls = 0;
+            if constexpr (MODE == kCombineFilter) wta_filter<PPL>(o, incl, rk, lane, D, a.fp, depth, idx, cls);
             else case_argmin<PPL>(o, lane, D, a.fp, depth, idx);
             if (lane == 0) {
                 const int y = (int)(pix / a.W), x = (int)(pix - (long)y * a.W);
                 *reinterpret_cast<float*>(reinterpret_cast<char*>(a.depth) + (size_t)y * a.depth_pitch +
                                           (size_t)x * 4) = depth;
                 if (a.index) a.index[pix] = idx;
+                if (a.wta_class) a.wta_class[pix] = (uint8_t)cls;
             }
         }
 #pragma unroll

@@ -157,6 +157,15 @@ class StereoMapper:
                     "pm_get_stage_times")
         return out
 
+    def enable_stats(self, enable=True):
+        self._check(self.lib.pm_enable_stats(self.h, int(enable)), "pm_enable_stats")
+
+    def stats(self) -> dict:
+        """Pixel counters of the last output call (pm_stats) as a dict of ints."""
+        st = _lib.PmStats()
+        self._check(self.lib.pm_get_stats(self.h, ctypes.byref(st)), "pm_get_stats")
+        return {n: int(getattr(st, n)) for n in _lib.STATS_FIELDS}
+
     def synchronize(self):
         self._check(self.lib.pm_synchronize(self.h), "pm_synchronize")
 

@@ -26,7 +26,7 @@ def pytest_collection_modifyitems(config, items):
         return
     skip = pytest.mark.skip(reason="no CUDA device in this container")
     for it in items:
-        if "gpu" in it.keywords:
+        if it.get_closest_marker("gpu") is not None:
             it.add_marker(skip)
 
 

@@ -1,7 +1,8 @@
 // Builds against include/pm_stereo_mapper.hpp and libpm_stereo.so the way a C++ host program
 // (the reference's evaluate.cc) would, and exercises the error path: a bad configuration must
 // raise pm::Error with PM_ERR_INVALID_ARGUMENT.  With a GPU present (argv[1] == "gpu") it also
-// maps one synthetic frame pair and checks that the depth map is finite.
+// maps one synthetic frame pair and checks that the depth map is finite and that the pixel
+// counters add up.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -34,10 +35,16 @@ int main(int argc, char** argv) {
                 src[y * W + x] = (uint8_t)(128 + 100 * std::sin(0.7 * (x + 2)) * std::cos(0.5 * y));
             }
         const double I[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, T0[3] = {0, 0, 0}, T1[3] = {0.1, 0, 0};
+        m.enableStats(true);
         m.initReference(ref.data(), W);
         m.update(src.data(), W, I, T0, I, T1);
         std::vector<float> depth(W * H);
         m.output(depth.data(), W * sizeof(float));
+        const pm_stats st = m.stats();   // every pixel in one winner-take-all class
+        if (st.wta_depth + st.wta_no_overlap + st.wta_border + st.wta_flat + st.wta_ambiguous != (uint32_t)(W * H)) {
+            std::printf("winner-take-all counters do not add up to the pixels\n");
+            return 1;
+        }
         for (float d : depth)
             if (!std::isfinite(d)) {
                 std::printf("non-finite depth\n");
