@@ -111,6 +111,9 @@ def lib():
         L.orc_diff_forward.restype = ctypes.c_double
         L.orc_diff_backward.argtypes = [dp, d, d, d, d, d, d, d, d]
         L.orc_diff_backward.restype = ctypes.c_double
+        L.orc_diff_source_validity.argtypes = [dp, d, d, d, d, d, u8]
+        L.orc_diff_forward_frozen.argtypes = [dp, d, d, d, d, d, d, u8]
+        L.orc_diff_forward_frozen.restype = ctypes.c_double
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -411,6 +414,26 @@ def diff_forward(p: DiffParams, ref, srcs, K, R, t, rho_gt):
     loss = lib().orc_diff_forward(ctypes.byref(cp), *[_ptr(x, ctypes.c_double) for x in a],
                                   _ptr(rho_hat, ctypes.c_double), _ptr(valid, ctypes.c_uint8))
     return loss, rho_hat.reshape(p.H, p.W), valid.reshape(p.H, p.W)
+
+
+def diff_source_validity(p: DiffParams, ref, srcs, K, R, t):
+    """(H, W, D, S) uint8: 1 where source s measures plane d of the pixel at this pose."""
+    a = _diff_args(p, ref, srcs, K, R, t, np.zeros(p.W * p.H))[:5]
+    ok = np.zeros(p.W * p.H * p.D * p.S, np.uint8)
+    cp = p.c()
+    lib().orc_diff_source_validity(ctypes.byref(cp), *[_ptr(x, ctypes.c_double) for x in a], _ptr(ok, ctypes.c_uint8))
+    return ok.reshape(p.H, p.W, p.D, p.S)
+
+
+def diff_forward_frozen(p: DiffParams, ref, srcs, K, R, t, rho_gt, frozen):
+    """FP64 loss with the source validity flags held at `frozen` (diff_source_validity of the base
+    pose): the loss as a function of the pose without border jumps."""
+    a = _diff_args(p, ref, srcs, K, R, t, rho_gt)
+    fz = np.ascontiguousarray(frozen, np.uint8).reshape(-1)
+    assert fz.size == p.W * p.H * p.D * p.S
+    cp = p.c()
+    return lib().orc_diff_forward_frozen(ctypes.byref(cp), *[_ptr(x, ctypes.c_double) for x in a],
+                                         _ptr(fz, ctypes.c_uint8))
 
 
 def diff_backward(p: DiffParams, ref, srcs, K, R, t, rho_gt):

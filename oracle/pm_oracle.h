@@ -130,6 +130,14 @@ double orc_diff_forward(const orc_diff_params* p, const double* ref, const doubl
                         const double* R, const double* t, const double* rho_gt, double* rho_hat, uint8_t* valid);
 double orc_diff_backward(const orc_diff_params* p, const double* ref, const double* srcs, const double* K,
                          const double* R, const double* t, const double* rho_gt, double* g_srcs, double* g_pose);
+/* The validity flag of each (pixel, plane, source) at a pose: ok[(pixel * D + d) * S + s] = 1
+ * when all nine samples of the patch land inside the image with w >= 0.  The frozen forward
+ * keeps those flags (the set of sources averaged into each voxel, and the pixel validity) while
+ * the pose moves, so that central differences over a pose step see no border jumps. */
+void orc_diff_source_validity(const orc_diff_params* p, const double* ref, const double* srcs, const double* K,
+                              const double* R, const double* t, uint8_t* ok);
+double orc_diff_forward_frozen(const orc_diff_params* p, const double* ref, const double* srcs, const double* K,
+                               const double* R, const double* t, const double* rho_gt, const uint8_t* frozen);
 
 #ifdef __cplusplus
 }

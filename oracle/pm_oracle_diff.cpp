@@ -37,6 +37,11 @@ struct Model {
     const orc_diff_params* p;
     const double* ref;
     const double* srcs;
+    // N*D*S source validity flags ((pixel * D + plane) * S + source) that replace the tests of
+    // the warped samples, or nullptr.  A frozen-valid source is evaluated even where one of its
+    // samples has moved out of [0, W-1] x [0, H-1]: the zero border keeps the bilinear value
+    // continuous, so the loss has no jumps under a small pose change.
+    const uint8_t* frozen = nullptr;
     double fx, fy, cx, cy;
     std::vector<double> H;   // S x 12: K R K^-1 row-major, then K t
     int W, H_, D, S;
@@ -81,7 +86,7 @@ struct Sample {
     double a, b;
 };
 
-inline Sample sample(const Model& m, int s, int qu, int qv, double rho) {
+inline Sample sample(const Model& m, int s, int qu, int qv, double rho, bool force = false) {
     const double* h = &m.H[12 * s];
     Sample r{};
     const double x = h[0] * qu + h[1] * qv + h[2] + h[9] * rho;
@@ -91,7 +96,7 @@ inline Sample sample(const Model& m, int s, int qu, int qv, double rho) {
     r.u = x / w;
     r.v = y / w;
     r.ok = w >= 0.0 && r.u >= 0.0 && r.u <= m.W - 1 && r.v >= 0.0 && r.v <= m.H_ - 1;
-    if (!r.ok) return r;
+    if (!r.ok && !force) return r;
     const double* img = m.srcs + m.N * s;
     r.i = (int)std::floor(r.u);
     r.j = (int)std::floor(r.v);
@@ -108,8 +113,8 @@ inline Sample sample(const Model& m, int s, int qu, int qv, double rho) {
 
 const int kPatch[9][2] = {{0, 0}, {0, -1}, {0, 1}, {-1, 0}, {1, 0}, {-1, -1}, {1, 1}, {-1, 1}, {1, -1}};
 
-// C (V), pixel validity (N)
-void cost_forward(const Model& m, std::vector<double>& C, std::vector<uint8_t>& valid) {
+// C (V), pixel validity (N); ok_out (optional): the N*D*S source validity flags of m.frozen
+void cost_forward(const Model& m, std::vector<double>& C, std::vector<uint8_t>& valid, uint8_t* ok_out = nullptr) {
     const int W = m.W, H = m.H_, D = m.D;
     C.assign(m.V, 0.0);
     valid.assign(m.N, 1);
@@ -123,13 +128,15 @@ void cost_forward(const Model& m, std::vector<double>& C, std::vector<uint8_t>& 
                 int n = 0;
                 for (int s = 0; s < m.S; ++s) {
                     double tmp = 0.0;
-                    bool ok = true;
+                    const size_t fi = (((size_t)v * W + u) * D + d) * m.S + s;
+                    bool ok = m.frozen ? m.frozen[fi] != 0 : true;
                     for (int k = 0; k < 9 && ok; ++k) {
                         const int qu = u + kPatch[k][0], qv = v + kPatch[k][1];
-                        const Sample smp = sample(m, s, qu, qv, rho);
-                        ok = smp.ok;
+                        const Sample smp = sample(m, s, qu, qv, rho, m.frozen != nullptr);
+                        if (!m.frozen) ok = smp.ok;
                         if (ok) tmp += std::fabs(at(m.ref, W, H, qu, qv) - smp.val);
                     }
+                    if (ok_out) ok_out[fi] = ok;
                     if (ok) {
                         sum += tmp / 9.0;
                         ++n;
@@ -374,6 +381,28 @@ double orc_diff_forward(const orc_diff_params* p, const double* ref, const doubl
     }
     if (valid_out) std::memcpy(valid_out, valid.data(), m.N);
     return soft_forward(m, Ssum, rho_gt, valid, rho_hat, nullptr);
+}
+
+void orc_diff_source_validity(const orc_diff_params* p, const double* ref, const double* srcs, const double* K,
+                              const double* R, const double* t, uint8_t* ok) {
+    const Model m = make_model(p, ref, srcs, K, R, t);
+    std::vector<double> C;
+    std::vector<uint8_t> valid;
+    cost_forward(m, C, valid, ok);
+}
+
+double orc_diff_forward_frozen(const orc_diff_params* p, const double* ref, const double* srcs, const double* K,
+                               const double* R, const double* t, const double* rho_gt, const uint8_t* frozen) {
+    Model m = make_model(p, ref, srcs, K, R, t);
+    m.frozen = frozen;
+    std::vector<double> C, L, Ssum(m.V, 0.0);
+    std::vector<uint8_t> valid;
+    cost_forward(m, C, valid);
+    for (int r = 0; r < p->num_paths; ++r) {
+        path_forward(m, C, r, L);
+        for (size_t i = 0; i < m.V; ++i) Ssum[i] += L[i];
+    }
+    return soft_forward(m, Ssum, rho_gt, valid, nullptr, nullptr);
 }
 
 double orc_diff_backward(const orc_diff_params* p, const double* ref, const double* srcs, const double* K,

@@ -7,9 +7,10 @@ Configuration: 320x240, 64 planes in [0.1, 2.0], 2 sources, f = 260, soft-argmin
 * gradients: GPU against the FP64 transcription's adjoint -- pose (12 values) within 2 % of the
   vector norm, source intensities within 5 % (relative L2) with correlation >= 0.99 (FP32
   sums and near-ties in the SGM minima move individual routes);
-* FP64 central differences: intensities with a step of 1e-5, poses with a step of 1e-7 (a pose
+* FP64 central differences: intensities with a step of 1e-5; poses with a step of 1e-7, and with
+  the step of 1e-5 on the loss whose per-voxel source validity is held at the base pose (a pose
   step moves every warped sample, and at 1e-5 samples crossing the image border switch sources
-  in and out of a voxel's mean -- jumps of the loss -- so the 1e-5 pose differences are
+  in and out of a voxel's mean -- jumps of the loss; the plain 1e-5 pose differences are
   reported, not asserted);
 * memory with and without per-path recomputation of the SGM states (same loss, same gradients
   up to the order of atomic sums), and the torch.autograd harness against the direct calls.
@@ -85,7 +86,9 @@ def test_diff_form(case):
     # FP64 central differences
     fd7 = np.zeros((S, 6))
     fd5 = np.zeros((S, 6))
-    for eps, fd in ((1e-7, fd7), (1e-5, fd5)):
+    fd5f = np.zeros((S, 6))
+    frozen = oracle.diff_source_validity(c["p"], c["ref"], c["srcs"], c["K"], c["R"], c["t"])
+    for eps, fd, fz in ((1e-7, fd7, None), (1e-5, fd5, None), (1e-5, fd5f, frozen)):
         for s in range(S):
             for i in range(6):
                 v = []
@@ -94,10 +97,14 @@ def test_diff_form(case):
                     xi[i] = sign * eps
                     Rq, tq = c["R"].copy(), c["t"].copy()
                     Rq[s], tq[s] = perturb_pose(c["R"][s], c["t"][s], xi)
-                    v.append(oracle_loss(c, R=Rq, t=tq))
+                    if fz is None:
+                        v.append(oracle_loss(c, R=Rq, t=tq))
+                    else:
+                        v.append(oracle.diff_forward_frozen(c["p"], c["ref"], c["srcs"], c["K"], Rq, tq, c["rgt"], fz))
                 fd[s, i] = (v[0] - v[1]) / (2 * eps)
     fd_err7 = np.linalg.norm(g0["gp"] - fd7) / np.linalg.norm(fd7)
     fd_err5 = np.linalg.norm(g0["gp"] - fd5) / np.linalg.norm(fd5)
+    fd_err5f = np.linalg.norm(g0["gp"] - fd5f) / np.linalg.norm(fd5f)
     pix = []
     for k in np.argsort(-np.abs(gs64.reshape(-1)))[:5]:
         s, rem = divmod(int(k), W * H)
@@ -112,7 +119,8 @@ def test_diff_form(case):
     report = {"config": f"{W}x{H}, {D} planes, {S} sources, T={T}", "loss_gpu": g0["loss"], "loss_fp64": loss64,
               "pose_grad_rel_err_vs_fp64_adjoint": pose_err, "image_grad_rel_err_vs_fp64_adjoint": img_err,
               "image_grad_correlation": corr, "pose_grad_rel_err_vs_fd_step_1e-7": fd_err7,
-              "pose_grad_rel_err_vs_fd_step_1e-5": fd_err5, "image_grad_vs_fd_step_1e-5": pix,
+              "pose_grad_rel_err_vs_fd_step_1e-5": fd_err5,
+              "pose_grad_rel_err_vs_fd_step_1e-5_frozen_validity": fd_err5f, "image_grad_vs_fd_step_1e-5": pix,
               "device_bytes_recompute": g0["mem"], "device_bytes_store_paths": g1["mem"],
               "pose_grad_gpu": g0["gp"].tolist(), "pose_grad_fd_1e-7": fd7.tolist()}
     print(json.dumps(report))
@@ -124,6 +132,7 @@ def test_diff_form(case):
     assert pose_err < 0.02
     assert img_err < 0.05 and corr > 0.99
     assert fd_err7 < 0.02
+    assert fd_err5f < 0.02
     for a, b in pix:
         assert a == pytest.approx(b, rel=0.02, abs=1e-7)
 
