@@ -258,6 +258,7 @@ typedef struct pm_batch pm_batch;
                                  PM_BATCH_AUTOTUNE and PM_BATCH_PRIORITY do not apply to it.
                                  pm_batch_synchronize reports PM_ERR_CUDA if a dependency wait
                                  of the last step ran out (its outputs are then invalid). */
+#define PM_BATCH_STATS 16 /* per-sequence pm_stats counters of each step (pm_batch_get_stats) */
 PM_API pm_status pm_batch_create(const pm_config* cfgs, int num_sequences, int num_sources, int lanes, int flags,
                                  pm_batch** out);
 PM_API void pm_batch_destroy(pm_batch* b);
@@ -288,6 +289,9 @@ PM_API pm_status pm_batch_copy_wta_depth(pm_batch* b, int seq, float* depth, siz
 /* SGM schedule of sequence seq: scanlines per block of the path-pair kernel, serial (1) or
  * concurrent (0) path pairs, and the stage time the autotuner measured (ms; 0 if untuned). */
 PM_API pm_status pm_batch_tuning(pm_batch* b, int seq, int* pair_warps, int* serial_pairs, float* ms);
+/* The pm_stats counters of sequence seq's last step (a batch created with PM_BATCH_STATS), after
+ * waiting for the batch's stream; PM_ERR_BAD_STATE without the flag. */
+PM_API pm_status pm_batch_get_stats(pm_batch* b, int seq, pm_stats* out);
 PM_API void* pm_batch_stream(pm_batch* b);
 PM_API const char* pm_batch_last_error(const pm_batch* b);
 

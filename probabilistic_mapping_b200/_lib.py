@@ -29,6 +29,7 @@ PM_BATCH_HOST_IO = 1
 PM_BATCH_AUTOTUNE = 2
 PM_BATCH_PRIORITY = 4
 PM_BATCH_PERSISTENT = 8
+PM_BATCH_STATS = 16
 PM_FUSION_GPU = 0
 PM_FUSION_CPU_PATH = 1
 PM_CASE_RAW_ARGMIN = 0
@@ -131,6 +132,7 @@ SIGNATURES = {
     "pm_stage_depth_fuse_cpu_path": (_I, [_I, _I, _P(ctypes.c_double), _P(ctypes.c_float), _VP, _P(_VP), _P(_VP),
                                           _VP, _VP, _VP]),
     "pm_batch_tuning": (_I, [_VP, _I, _P(_I), _P(_I), _P(_F)]),
+    "pm_batch_get_stats": (_I, [_VP, _I, _P(PmStats)]),
     "pm_batch_stream": (_VP, [_VP]),
     "pm_batch_last_error": (ctypes.c_char_p, [_VP]),
     "pm_diff_config_default": (None, [_P(PmDiffConfig), _I, _I, _I, _I]),

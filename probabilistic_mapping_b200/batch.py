@@ -23,7 +23,7 @@ class StereoBatch:
     """configs: list of dicts of pm_config fields, each with width, height and num_planes."""
 
     def __init__(self, configs, num_sources: int, lanes: int = 0, host_io: bool = True, autotune: bool = False,
-                 priority: bool = False, persistent: bool = False):
+                 priority: bool = False, persistent: bool = False, stats: bool = False):
         self.lib = load()
         n = len(configs)
         arr = (_lib.PmConfig * n)()
@@ -40,7 +40,8 @@ class StereoBatch:
         self.S = num_sources
         self.host_io = host_io
         flags = ((_lib.PM_BATCH_HOST_IO if host_io else 0) | (_lib.PM_BATCH_AUTOTUNE if autotune else 0) |
-                 (_lib.PM_BATCH_PRIORITY if priority else 0) | (_lib.PM_BATCH_PERSISTENT if persistent else 0))
+                 (_lib.PM_BATCH_PRIORITY if priority else 0) | (_lib.PM_BATCH_PERSISTENT if persistent else 0) |
+                 (_lib.PM_BATCH_STATS if stats else 0))
         b = ctypes.c_void_p()
         check(self.lib.pm_batch_create(arr, n, num_sources, lanes, flags, ctypes.byref(b)), None, "pm_batch_create")
         self.b = b
@@ -132,6 +133,12 @@ class StereoBatch:
         self._check(self.lib.pm_batch_tuning(self.b, seq, ctypes.byref(w), ctypes.byref(s), ctypes.byref(ms)),
                     "pm_batch_tuning")
         return w.value, s.value, ms.value
+
+    def stats(self, seq: int) -> dict:
+        """pm_stats counters of sequence seq's last step (a batch made with stats=True)."""
+        st = _lib.PmStats()
+        self._check(self.lib.pm_batch_get_stats(self.b, seq, ctypes.byref(st)), "pm_batch_get_stats")
+        return {n: int(getattr(st, n)) for n in _lib.STATS_FIELDS}
 
     def stream(self) -> int:
         return self.lib.pm_batch_stream(self.b)

@@ -76,6 +76,8 @@ struct Seq {
     int32_t* d_table = nullptr;
     float* d_fused = nullptr;
     float* d_var = nullptr;
+    unsigned* d_stats = nullptr;   // PM_BATCH_STATS: the step's pm_stats counters
+    uint8_t* d_cls = nullptr;      // PM_BATCH_STATS: W*H winner-take-all class of each pixel
     PlaneOrder order{};
     int lane = -1;               // index into the batch's lane sets
     // host step state (stereo_mapper.cpp:128-156)
@@ -192,6 +194,8 @@ void free_batch(pm_batch* b) {
         cudaFree(q.d_table);
         cudaFree(q.d_fused);
         cudaFree(q.d_var);
+        cudaFree(q.d_stats);
+        cudaFree(q.d_cls);
         for (auto& s : q.st)
             if (s) cudaStreamDestroy(s);
         if (q.side.fork) cudaEventDestroy(q.side.fork);
@@ -230,6 +234,7 @@ SgmLaunch sgm_launch(const Seq& q, const LaneBufs& l, int priority) {
     a.depth = q.d_depth;
     a.depth_pitch = sizeof(float) * (size_t)c.width;
     a.index = q.d_idx;
+    a.wta_class = q.d_cls;
     a.order = q.order;
     a.pair_warps = q.pair_warps;
     a.serial_pairs = q.serial_pairs;
@@ -314,12 +319,22 @@ cudaError_t enqueue_fusion(pm_batch* b, int i, int k, cudaStream_t m) {
     f.flags_dev = reinterpret_cast<const int*>(q.d_par[k] + 12 * q.S + 16);
     for (int s = 0; s < 2; ++s)
         for (int j = 0; j < 4; ++j) f.state[s][j] = q.d_state[s][j];
+    f.stats = q.d_stats;
     if ((e = launch_fuse_gpu(f, m))) return e;
     if (b->flags & PM_BATCH_HOST_IO) {
         if ((e = cudaMemcpyAsync(q.h_out[k], q.d_fused, 4 * N, cudaMemcpyDeviceToHost, m))) return e;
         if ((e = cudaMemcpyAsync(q.h_out[k] + N, q.d_var, 4 * N, cudaMemcpyDeviceToHost, m))) return e;
     }
     return cudaSuccess;
+}
+
+// PM_BATCH_STATS: the step's counters start from zero; the winner-take-all classes are counted
+// once the combine kernel has written them.
+cudaError_t clear_stats(const Seq& q, cudaStream_t m) {
+    return q.d_stats ? cudaMemsetAsync(q.d_stats, 0, sizeof(unsigned) * kStatWords, m) : cudaSuccess;
+}
+cudaError_t count_wta_classes(const Seq& q, cudaStream_t m) {
+    return q.d_stats ? launch_count_classes(q.d_cls, (long)q.N, kWtaClasses, q.d_stats + kStatWta, m) : cudaSuccess;
 }
 
 // The work of one sequence for buffer set k, on its own streams (captured into the graph).
@@ -329,6 +344,7 @@ cudaError_t enqueue_seq(pm_batch* b, int i, int k) {
     cudaStream_t m = q.st[0];
     cudaError_t e;
     if ((e = enqueue_inputs(b, i, k, m))) return e;
+    if ((e = clear_stats(q, m))) return e;
     // the lane's volumes are free once the previous sequence in this lane has finished its SGM
     if (l.last_user >= 0 && (e = cudaStreamWaitEvent(m, b->seqs[l.last_user].lane_free, 0))) return e;
     l.last_user = i;
@@ -336,6 +352,7 @@ cudaError_t enqueue_seq(pm_batch* b, int i, int k) {
     const SgmLaunch g = sgm_launch(q, l, b->sgm_priority);
     if ((e = launch_sgm(g, kCombineFilter, m, &q.side))) return e;
     if ((e = cudaEventRecord(q.lane_free, m))) return e;
+    if ((e = count_wta_classes(q, m))) return e;
     return enqueue_fusion(b, i, k, m);
 }
 
@@ -459,6 +476,7 @@ cudaError_t enqueue_persist(pm_batch* b, int k) {
         Seq& q = b->seqs[i];
         if ((e = cudaStreamWaitEvent(q.st[0], b->root, 0))) return e;
         if ((e = enqueue_inputs(b, i, k, q.st[0]))) return e;
+        if ((e = clear_stats(q, q.st[0]))) return e;
         if ((e = cudaEventRecord(q.side.fork, q.st[0]))) return e;
         if ((e = cudaStreamWaitEvent(b->run, q.side.fork, 0))) return e;
     }
@@ -470,6 +488,7 @@ cudaError_t enqueue_persist(pm_batch* b, int k) {
     for (int i = 0; i < (int)b->seqs.size(); ++i) {
         Seq& q = b->seqs[i];
         if ((e = cudaStreamWaitEvent(q.st[0], b->persist_done, 0))) return e;
+        if ((e = count_wta_classes(q, q.st[0]))) return e;
         if ((e = enqueue_fusion(b, i, k, q.st[0]))) return e;
         if ((e = cudaEventRecord(q.done, q.st[0]))) return e;
         if ((e = cudaStreamWaitEvent(b->run, q.done, 0))) return e;
@@ -652,7 +671,10 @@ pm_status pm_batch_create(const pm_config* cfgs, int n, int num_sources, int lan
              (q.cfg.sampler != PM_SAMPLER_EXACT || alloc((void**)&q.d_srcq, 16 * N * q.S)) &&
              alloc((void**)&q.d_depth, 4 * N) && alloc((void**)&q.d_idx, 4 * N) &&
              alloc((void**)&q.d_ztable, 8 * N) && alloc((void**)&q.d_table, 4 * N) &&
-             alloc((void**)&q.d_fused, 4 * N) && alloc((void**)&q.d_var, 4 * N);
+             alloc((void**)&q.d_fused, 4 * N) && alloc((void**)&q.d_var, 4 * N) &&
+             (!(flags & PM_BATCH_STATS) ||
+              (alloc((void**)&q.d_stats, sizeof(unsigned) * kStatWords) && alloc((void**)&q.d_cls, N) &&
+               note(cudaMemset(q.d_stats, 0, sizeof(unsigned) * kStatWords))));
         for (int s = 0; s < 2 && ok; ++s)
             for (int k = 0; k < 4 && ok; ++k) ok = alloc((void**)&q.d_state[s][k], 4 * N);
         for (int s = 0; q.cfg.sampler != PM_SAMPLER_EXACT && s < q.S && ok; ++s)
@@ -877,6 +899,17 @@ pm_status pm_batch_copy_wta_depth(pm_batch* b, int seq, float* depth, size_t pit
     DevGuard dg(b->device);
     PB_CK(b, cudaStreamSynchronize(b->run));
     PB_CK(b, cudaMemcpy2D(depth, pitch, d, row, row, (size_t)q.cfg.height, cudaMemcpyDefault));
+    return PM_OK;
+}
+
+pm_status pm_batch_get_stats(pm_batch* b, int seq, pm_stats* out) {
+    if (!b || !out) return PM_ERR_INVALID_ARGUMENT;
+    if (seq < 0 || seq >= (int)b->seqs.size()) return bfail(b, PM_ERR_INVALID_ARGUMENT, "no sequence %d", seq);
+    const Seq& q = b->seqs[seq];
+    if (!q.d_stats) return bfail(b, PM_ERR_BAD_STATE, "the batch was created without PM_BATCH_STATS");
+    DevGuard dg(b->device);
+    PB_CK(b, cudaStreamSynchronize(b->run));
+    PB_CK(b, cudaMemcpy(out, q.d_stats, sizeof(pm_stats), cudaMemcpyDeviceToHost));
     return PM_OK;
 }
 

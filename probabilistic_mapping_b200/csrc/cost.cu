@@ -57,11 +57,12 @@ __global__ void __launch_bounds__(256) invalid_kernel(const void* cost, long npi
 template <int MODE, bool HALF, int SAMP>
 cudaError_t launch_t(const CostLaunch& a, dim3 grid, cudaStream_t s) {
     auto kern = a.incremental ? cost_kernel<MODE, HALF, SAMP, true> : cost_kernel<MODE, HALF, SAMP, false>;
-    if (Smem::BYTES > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Smem::BYTES);
+    const size_t smem = (HALF && !a.incremental) ? SmemL<true>::BYTES : SmemL<false>::BYTES;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    kern<<<grid, NT, Smem::BYTES, s>>>(a);
+    kern<<<grid, NT, smem, s>>>(a);
     return cudaGetLastError();
 }
 

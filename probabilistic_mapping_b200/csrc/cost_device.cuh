@@ -3,6 +3,8 @@
 // cost.cu (the stand-alone kernels) and persist.cu (the batched form's persistent kernel).
 #pragma once
 
+#include <type_traits>
+
 #include "pm_device.cuh"
 
 namespace pm {
@@ -17,13 +19,17 @@ constexpr int NT = 32 * WARPS;
 constexpr int SP = PCB + 2;              // state pitch: even (8-byte pairs), conflict-free pairs
 constexpr int NPIX = TXU * TY;
 
-struct Smem {
-    static constexpr size_t REF = 0;                                        // float2 [TY+2][32]
-    static constexpr size_t ACC = REF + sizeof(float2) * (TY + 2) * 32;     // float [NPIX][SP]
-    static constexpr size_t CNT = ACC + sizeof(float) * NPIX * SP;          // float [NPIX][SP]
-    static constexpr size_t OFF = CNT + sizeof(float) * NPIX * SP;         // float [NPIX] (FP16 form)
+// Shared layout of a tile.  HC: the counts as FP16 (the FP16 form's first pass, whose counts are
+// small integers, exact in FP16): fewer shared bytes per CTA leave more of the SM's L1 to the
+// texture cache, which the texture samplers' speed depends on.
+template <bool HC> struct SmemL {
+    static constexpr size_t REF = 0;                                              // float2 [TY+2][32]
+    static constexpr size_t ACC = REF + sizeof(float2) * (TY + 2) * 32;           // float [NPIX][SP]
+    static constexpr size_t CNT = ACC + sizeof(float) * NPIX * SP;                // float or half [NPIX][SP]
+    static constexpr size_t OFF = CNT + (HC ? sizeof(__half) : sizeof(float)) * NPIX * SP;   // float [NPIX] (FP16 form)
     static constexpr size_t BYTES = OFF + sizeof(float) * NPIX;
 };
+using Smem = SmemL<false>;   // the larger layout
 
 __device__ __forceinline__ float ref_at(const float* __restrict__ ref, int W, int H, int x, int y) {
     return (x < 0 || y < 0 || x >= W || y >= H) ? 0.0f : __ldg(ref + (size_t)y * W + x);
@@ -214,13 +220,15 @@ __device__ __forceinline__ void fold2(float2& acc, float2& cn, float2 tmp, float
 }
 
 // The FP16 form's first pass (from initReference): the state holds the SUM of the sources'
-// tmp/9 terms and their count, and the mean is formed once when the tile is stored (sum_to_mean);
-// a rejected sum (NaN) adds nothing.  The reference's running mean (calc_cost.cu:200-207) and this
-// mean differ only by FP32 rounding, far below the FP16 volume's step.
-__device__ __forceinline__ void fold2_sum(float2& acc, float2& cn, float2 tmp, float r9) {
+// tmp/9 terms and their count (FP16, exact for counts up to 2048), and the mean is formed once
+// when the tile is stored (sum_to_mean); a rejected sum (NaN) adds nothing.  The reference's
+// running mean (calc_cost.cu:200-207) and this mean differ only by FP32 rounding, far below the
+// FP16 volume's step.
+__device__ __forceinline__ void fold2_sum(float2& acc, __half2& cn, float2 tmp, float r9) {
     const bool v0 = tmp.x == tmp.x, v1 = tmp.y == tmp.y;
     acc = __ffma2_rn(make_float2(v0 ? tmp.x : 0.0f, v1 ? tmp.y : 0.0f), make_float2(r9, r9), acc);
-    cn = __fadd2_rn(cn, make_float2(v0 ? 1.0f : 0.0f, v1 ? 1.0f : 0.0f));
+    const unsigned one = (v0 ? 0x3C00u : 0u) | (v1 ? 0x3C000000u : 0u);   // (v0, v1) as FP16 ones
+    cn = __hadd2(cn, *reinterpret_cast<const __half2*>(&one));
 }
 __device__ __forceinline__ float sum_to_mean(float sum, float cnt) {
     if (cnt == 0.0f) return -1.0f;   // never measured (initReference's -1, stereo_mapper.cpp:69)
@@ -233,9 +241,12 @@ __device__ __forceinline__ float sum_to_mean(float sum, float cnt) {
 // One CTA's tile (bx, by) and 16-plane block bz of the volume; smem_raw holds Smem::BYTES.
 template <int MODE, bool HALF, int SAMP, bool INC>
 __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, int bz, unsigned char* smem_raw) {
-    float2* const refp = reinterpret_cast<float2*>(smem_raw + Smem::REF);
-    float* const accs = reinterpret_cast<float*>(smem_raw + Smem::ACC);
-    float* const cnts = reinterpret_cast<float*>(smem_raw + Smem::CNT);
+    constexpr bool HC = HALF && !INC;   // sums and FP16 counts
+    using SM = SmemL<HC>;
+    using CntT = typename std::conditional<HC, __half, float>::type;
+    float2* const refp = reinterpret_cast<float2*>(smem_raw + SM::REF);
+    float* const accs = reinterpret_cast<float*>(smem_raw + SM::ACC);
+    CntT* const cnts = reinterpret_cast<CntT*>(smem_raw + SM::CNT);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int W = a.W, H = a.H, D = a.D;
@@ -267,7 +278,7 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
             }
         }
         accs[p * SP + k] = c0;
-        cnts[p * SP + k] = n0;
+        cnts[p * SP + k] = (CntT)n0;
     }
     __syncthreads();
 
@@ -277,7 +288,8 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
     // this lane's state slots (one 8-byte pair per row); lanes outside the output columns never
     // touch them
     float2* const accp = reinterpret_cast<float2*>(accs + (out_col ? lane - 1 : 0) * SP + 2 * warp);
-    float2* const cntp = reinterpret_cast<float2*>(cnts + (out_col ? lane - 1 : 0) * SP + 2 * warp);
+    using CntPair = typename std::conditional<HC, __half2, float2>::type;
+    CntPair* const cntp = reinterpret_cast<CntPair*>(cnts + (out_col ? lane - 1 : 0) * SP + 2 * warp);
 
     for (int s = 0; s < a.nsrc; ++s) {
         Src<SAMP> src;
@@ -348,9 +360,10 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
                 for (int k = 1; k < 9; ++k) t2 = __fadd2_rn(t2, f2(fabsf(d[k].x), fabsf(d[k].y)));
                 const float tx = t2.x, ty = t2.y;
                 float2* const ap = accp + o * (TXU * SP / 2);
-                float2* const cp = cntp + o * (TXU * SP / 2);
-                float2 av = *ap, nv = *cp;
-                if constexpr (HALF && !INC) fold2_sum(av, nv, f2(tx, ty), r9);
+                CntPair* const cp = cntp + o * (TXU * SP / 2);
+                float2 av = *ap;
+                CntPair nv = *cp;
+                if constexpr (HC) fold2_sum(av, nv, f2(tx, ty), r9);
                 else fold2<INC, HALF>(av, nv, f2(tx, ty), r9);
                 *ap = av;
                 *cp = nv;
@@ -368,13 +381,13 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
         if constexpr (!INC) {   // sums and counts to means
             for (int e = tid; e < NPIX * PCB; e += NT) {
                 const int p = e / PCB, k = e - p * PCB;
-                accs[p * SP + k] = sum_to_mean(accs[p * SP + k], cnts[p * SP + k]);
+                accs[p * SP + k] = sum_to_mean(accs[p * SP + k], (float)cnts[p * SP + k]);
             }
             __syncthreads();
         }
         // per pixel and 16-plane block: the smallest measured cost of the block (0 when none is
         // measured) is stored beside the block, and the half volume holds the differences
-        float* const s_off = reinterpret_cast<float*>(smem_raw + Smem::OFF);
+        float* const s_off = reinterpret_cast<float*>(smem_raw + SM::OFF);
         for (int p = tid; p < NPIX; p += NT) {
             float m = inf_f();
 #pragma unroll
@@ -396,7 +409,7 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
             if (gx < W && gy < H) {
                 const size_t g = ((size_t)gy * W + gx) * D + d0 + k;
                 store_cost<true>(a.cost, g, __fsub_rn(accs[p * SP + k], s_off[p]));
-                if (a.cnt) a.cnt[g] = cnts[p * SP + k];
+                if (a.cnt) a.cnt[g] = (float)cnts[p * SP + k];
             }
         }
     } else {

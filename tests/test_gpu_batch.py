@@ -4,7 +4,8 @@ A batch of sequences with different shapes, precisions, samplers, path counts an
 of them sharing one lane of cost/path volumes) is stepped over several keyframes; after every step each
 sequence's fused depth and variance must equal, bit for bit, what a StereoMapper fed the same
 frames and poses returns: the batch runs the same kernels, with the per-step values read from
-device memory instead of kernel parameters.
+device memory instead of kernel parameters.  With PM_BATCH_STATS, each sequence's pixel
+counters must also equal the separate mapper's.
 """
 import numpy as np
 import pytest
@@ -37,12 +38,12 @@ def make_configs():
     return out
 
 
-@pytest.mark.parametrize("host_io,autotune,priority", [(True, False, False), (False, True, True)])
-def test_batch_matches_separate_mappers(host_io, autotune, priority):
+@pytest.mark.parametrize("host_io,autotune,priority,stats", [(True, False, False, False), (False, True, True, True)])
+def test_batch_matches_separate_mappers(host_io, autotune, priority, stats):
     cfgs = make_configs()
     seqs = [scene.make_sequence(c["width"], c["height"], 0.8 * c["width"], S, 3, seed=50 + i)
             for i, c in enumerate(cfgs)]
-    b = StereoBatch(cfgs, S, lanes=1, host_io=host_io, autotune=autotune, priority=priority)
+    b = StereoBatch(cfgs, S, lanes=1, host_io=host_io, autotune=autotune, priority=priority, stats=stats)
     mappers = []
     for i, c in enumerate(cfgs):
         W, H, D = c["width"], c["height"], c["num_planes"]
@@ -51,6 +52,8 @@ def test_batch_matches_separate_mappers(host_io, autotune, priority):
         _, drho = scene.plane_range(D)
         K = seqs[i][0].K
         m.initIntrinsic(K, 0.0, drho)
+        if stats:
+            m.enable_stats(True)
         b.init_intrinsic(i, K, drho)
         mappers.append(m)
     if autotune:
@@ -82,6 +85,8 @@ def test_batch_matches_separate_mappers(host_io, autotune, priority):
             assert (got_d.view(np.uint32) == want_d.view(np.uint32)).all(), (step, i)
             assert (got_v.view(np.uint32) == want_v.view(np.uint32)).all(), (step, i)
             nonzero += int((got_d != 0).sum() + (got_v != 0).sum())
+            if stats:
+                assert b.stats(i) == m.stats(), (step, i)
     assert nonzero > 0   # the fusion steps after the first keyframe produce depths and variances
     for m in mappers:
         m.close()
@@ -97,10 +102,11 @@ PERSIST_SEQS = [
 ]
 
 
-@pytest.mark.parametrize("precision,sampler,mode", [(1, 2, 0), (0, 0, 0), (0, 2, 1), (1, 0, 1)],
-                         ids=["fp16-texture_f32-ref", "fp32-exact-ref", "fp32-texture_f32-corrected",
+@pytest.mark.parametrize("precision,sampler,mode,stats", [(1, 2, 0, True), (0, 0, 0, True), (0, 2, 1, False),
+                                                          (1, 0, 1, False)],
+                         ids=["fp16-texture_f32-ref-stats", "fp32-exact-ref-stats", "fp32-texture_f32-corrected",
                               "fp16-exact-corrected"])
-def test_persistent_batch_matches_separate_mappers(precision, sampler, mode):
+def test_persistent_batch_matches_separate_mappers(precision, sampler, mode, stats):
     """PM_BATCH_PERSISTENT: the cost tiles, rebases, SGM scanlines and combines of all sequences in
     one persistent launch give, bit for bit, what separate StereoMappers give (shapes, plane counts
     and path counts mixed; one precision, sampler and cost mode per batch)."""
@@ -112,13 +118,15 @@ def test_persistent_batch_matches_separate_mappers(precision, sampler, mode):
         cfgs.append(dict(c, rho0=rho0, precision=precision, sampler=sampler, cost_mode=mode, **COMMON))
     seqs = [scene.make_sequence(c["width"], c["height"], 0.8 * c["width"], S, 3, seed=80 + i)
             for i, c in enumerate(cfgs)]
-    b = StereoBatch(cfgs, S, lanes=0, host_io=True, persistent=True)
+    b = StereoBatch(cfgs, S, lanes=0, host_io=True, persistent=True, stats=stats)
     mappers = []
     for i, c in enumerate(cfgs):
         params = {k: v for k, v in c.items() if k not in ("width", "height", "num_planes")}
         m = StereoMapper(c["width"], c["height"], c["num_planes"], **params)
         _, drho = scene.plane_range(c["num_planes"])
         m.initIntrinsic(seqs[i][0].K, 0.0, drho)
+        if stats:
+            m.enable_stats(True)
         b.init_intrinsic(i, seqs[i][0].K, drho)
         mappers.append(m)
     nonzero = 0
@@ -144,6 +152,8 @@ def test_persistent_batch_matches_separate_mappers(precision, sampler, mode):
             assert (got_d.view(np.uint32) == want_d.view(np.uint32)).all(), (step, i)
             assert (got_v.view(np.uint32) == want_v.view(np.uint32)).all(), (step, i)
             nonzero += int((got_d != 0).sum())
+            if stats:
+                assert b.stats(i) == m.stats(), (step, i)
     assert nonzero > 0
     for m in mappers:
         m.close()
@@ -158,3 +168,7 @@ def test_persistent_batch_rejects_what_it_cannot_schedule():
         StereoBatch([a, dict(a, precision=1)], S, persistent=True)
     with pytest.raises(PmError):   # every sequence with its own volumes
         StereoBatch([a, a], S, lanes=1, persistent=True)
+    b = StereoBatch([a], S)
+    with pytest.raises(PmError):   # counters only in a batch created with them
+        b.stats(0)
+    b.close()
