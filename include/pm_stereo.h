@@ -230,6 +230,13 @@ PM_API pm_status pm_synchronize(pm_mapper* h);
  * definition (RN(1/w) for 2^-126 <= |w| <= 2^126, NaN for zero, subnormal, infinite or NaN w,
  * +-0 above).  All four are 0 on a correct device.  Allocates 32 bytes of device memory. */
 PM_API pm_status pm_debug_check_arith(uint64_t out[4], void* stream);
+/* The bounds-checked library (libpm_stereo_checked.so, built from the same sources with
+ * PM_BOUNDS_CHECK; no counterpart in the reference, which has no checks): the kernels test the
+ * element index of their global accesses against the buffer and skip an access that is out of
+ * range instead of faulting.  out[0] = accesses skipped since the last reset, out[1..3] = site,
+ * index and extent of the first one.  Synchronises the device; reset = 1 clears the record.
+ * The product library returns PM_ERR_UNSUPPORTED (and zeros). */
+PM_API pm_status pm_debug_bounds(uint64_t out[4], int reset);
 PM_API const char* pm_last_error(const pm_mapper* h);
 PM_API const char* pm_status_string(pm_status s);
 

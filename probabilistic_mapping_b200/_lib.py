@@ -9,7 +9,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libpm_stereo.so")
+# PM_STEREO_LIB selects another build of the library (the bounds-checked libpm_stereo_checked.so)
+LIB_PATH = os.environ.get("PM_STEREO_LIB") or os.path.join(HERE, "libpm_stereo.so")
 
 PM_OK = 0
 PM_ERR_INVALID_ARGUMENT = 1
@@ -104,6 +105,7 @@ SIGNATURES = {
     "pm_get_stats": (_I, [_VP, _P(PmStats)]),
     "pm_synchronize": (_I, [_VP]),
     "pm_debug_check_arith": (_I, [_P(ctypes.c_uint64), _VP]),
+    "pm_debug_bounds": (_I, [_P(ctypes.c_uint64), _I]),
     "pm_last_error": (ctypes.c_char_p, [_VP]),
     "pm_status_string": (ctypes.c_char_p, [_I]),
     "pm_stage_to_float": (_I, [_I, _I, _VP, _SZ, _VP, _F, _VP]),

@@ -4,6 +4,11 @@ Compiles every .cu under csrc/ with nvcc for sm_100a (and the host-only .cpp fil
 g++) and links one shared library next to this file.  -fmad=false: FP32 expressions are written with explicit fused/unfused
 intrinsics, so the compiler must not contract multiply-adds on its own (the CPU oracle replays
 the same operation order).
+
+The same sources also build libpm_stereo_checked.so: -DPM_BOUNDS_CHECK turns on the element-index
+tests of the kernels' global accesses (a failing access is skipped and recorded, read back with
+pm_debug_bounds), and relocatable device code lets all kernels share one record.  It is a test
+build; the product library is libpm_stereo.so.
 """
 from __future__ import annotations
 
@@ -19,6 +24,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libpm_stereo.so")
+LIB_CHECKED = os.path.join(HERE, "libpm_stereo_checked.so")
+BUILD_CHECKED = os.path.join(HERE, "_build_checked")
+CHECKED_FLAGS = ["-DPM_BOUNDS_CHECK", "-rdc=true"]
 CLI_SRC = os.path.join(HERE, "cli", "pm_sequence.cpp")
 CLI = os.path.join(HERE, "pm_sequence")
 
@@ -76,8 +84,8 @@ def build_cli(force: bool = False) -> str:
     return CLI
 
 
-def _compile(src: str, extra: list[str]) -> str:
-    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+def _compile(src: str, extra: list[str], outdir: str = BUILD) -> str:
+    obj = os.path.join(outdir, os.path.basename(src) + ".o")
     cmd = [nvcc()] + NVCC_FLAGS + extra + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -96,23 +104,38 @@ def _compile_host(src: str) -> str:
     return obj
 
 
-def build(force: bool = False, verbose_ptxas: bool = False) -> str:
-    """Compile csrc/*.cu for sm_100a into libpm_stereo.so (skipped when up to date)."""
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _deps_mtime():
-        build_cli()
-        return LIB
-    os.makedirs(BUILD, exist_ok=True)
-    extra = ["-Xptxas", "-v"] if verbose_ptxas else []
-    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, extra), _sources()))
-        objs += list(ex.map(_compile_host, _host_sources()))
-    tmp = LIB + ".tmp"
-    cmd = [nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcuda", "-lz"]
+def _link(objs: list[str], lib: str, extra: list[str]) -> None:
+    tmp = lib + ".tmp"
+    cmd = [nvcc()] + ARCH + extra + ["-shared", "-o", tmp] + objs + ["-lcuda", "-lz"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    os.replace(tmp, LIB)
-    build_cli(force=True)
+    os.replace(tmp, lib)
+
+
+def build(force: bool = False, verbose_ptxas: bool = False, checked: bool = True) -> str:
+    """Compile csrc/*.cu for sm_100a into libpm_stereo.so and, with `checked`, the bounds-checked
+    libpm_stereo_checked.so (each skipped when up to date)."""
+    deps = _deps_mtime()
+    need = force or not os.path.exists(LIB) or os.path.getmtime(LIB) < deps
+    need_checked = checked and (force or not os.path.exists(LIB_CHECKED) or os.path.getmtime(LIB_CHECKED) < deps)
+    if not need and not need_checked:
+        build_cli()
+        return LIB
+    os.makedirs(BUILD, exist_ok=True)
+    os.makedirs(BUILD_CHECKED, exist_ok=True)
+    extra = ["-Xptxas", "-v"] if verbose_ptxas else []
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        jobs = [ex.submit(_compile, s, extra) for s in _sources()] if need else []
+        cjobs = [ex.submit(_compile, s, CHECKED_FLAGS, BUILD_CHECKED) for s in _sources()] if need_checked else []
+        host = list(ex.map(_compile_host, _host_sources()))
+        objs = [j.result() for j in jobs]
+        cobjs = [j.result() for j in cjobs]
+    if need:
+        _link(objs + host, LIB, [])
+    if need_checked:
+        _link(cobjs + host, LIB_CHECKED, ["-rdc=true"])
+    build_cli(force=need)
     return LIB
 
 

@@ -137,8 +137,11 @@ __device__ __forceinline__ float2 sample2(const Src<SAMP>& src, const WarpConst&
         const unsigned i1 = __float_as_uint(tv.y) * (unsigned)src.W + __float_as_uint(tu.y) - src.off;
         float2 lo0, hi0, lo1, hi1;
         {
-            const float4 t0 = __ldg(src.q + (ok0 ? i0 : 0u));
-            const float4 t1 = __ldg(src.q + (ok1 ? i1 : 0u));
+            [[maybe_unused]] const long long nq = (long long)src.W * src.H;
+            const bool in0 = !ok0 || PM_IN_BOUNDS(i0, nq, kSiteCostSource);
+            const bool in1 = !ok1 || PM_IN_BOUNDS(i1, nq, kSiteCostSource);
+            const float4 t0 = __ldg(src.q + (ok0 && in0 ? i0 : 0u));
+            const float4 t1 = __ldg(src.q + (ok1 && in1 ? i1 : 0u));
             lo0 = f2(t0.x, t0.y); hi0 = f2(t0.z, t0.w);
             lo1 = f2(t1.x, t1.y); hi1 = f2(t1.z, t1.w);
         }
@@ -270,8 +273,8 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
         if (INC) {
             const int o = p / TXU, i = p - o * TXU;
             const int gx = x0 + i, gy = y0 + o;
-            if (gx < W && gy < H) {
-                const size_t g = ((size_t)gy * W + gx) * D + d0 + k;
+            const size_t g = ((size_t)gy * W + gx) * D + d0 + k;
+            if (gx < W && gy < H && PM_IN_BOUNDS(g, (long long)W * H * D, kSiteCostState)) {
                 c0 = load_cost<HALF>(a.cost, g);
                 if constexpr (HALF) c0 = __fadd_rn(c0, a.offset[(size_t)gy * W + gx]);
                 n0 = a.cnt[g];
@@ -399,15 +402,17 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
             s_off[p] = m;
             const int o = p / TXU, i = p - o * TXU;
             const int gx = x0 + i, gy = y0 + o;
-            if (gx < W && gy < H) a.block_offset[((size_t)gy * W + gx) * (D / PCB) + bz] = m;
+            const size_t bo = ((size_t)gy * W + gx) * (D / PCB) + bz;
+            if (gx < W && gy < H && PM_IN_BOUNDS(bo, (long long)W * H * (D / PCB), kSiteCostOffset))
+                a.block_offset[bo] = m;
         }
         __syncthreads();
         for (int e = tid; e < NPIX * PCB; e += NT) {
             const int p = e / PCB, k = e - p * PCB;
             const int o = p / TXU, i = p - o * TXU;
             const int gx = x0 + i, gy = y0 + o;
-            if (gx < W && gy < H) {
-                const size_t g = ((size_t)gy * W + gx) * D + d0 + k;
+            const size_t g = ((size_t)gy * W + gx) * D + d0 + k;
+            if (gx < W && gy < H && PM_IN_BOUNDS(g, (long long)W * H * D, kSiteCostState)) {
                 store_cost<true>(a.cost, g, __fsub_rn(accs[p * SP + k], s_off[p]));
                 if (a.cnt) a.cnt[g] = (float)cnts[p * SP + k];
             }
@@ -417,8 +422,8 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
             const int p = e / PCB, k = e - p * PCB;
             const int o = p / TXU, i = p - o * TXU;
             const int gx = x0 + i, gy = y0 + o;
-            if (gx < W && gy < H) {
-                const size_t g = ((size_t)gy * W + gx) * D + d0 + k;
+            const size_t g = ((size_t)gy * W + gx) * D + d0 + k;
+            if (gx < W && gy < H && PM_IN_BOUNDS(g, (long long)W * H * D, kSiteCostState)) {
                 store_cost<false>(a.cost, g, accs[p * SP + k]);
                 if (a.cnt) a.cnt[g] = cnts[p * SP + k];
             }
@@ -444,10 +449,12 @@ __device__ __forceinline__ void rebase_pixels(__half2* __restrict__ cost, const 
     for (int r = 0; r < RB; ++r) {
         const long pix = pix0 + r < npix ? pix0 + r : npix - 1;   // a repeated last pixel is rewritten identically
         const __half2* c = cost + ((size_t)pix * D + lane * PPL) / 2;
+        const bool in = PM_RANGE_IN_BOUNDS((long long)pix * D + lane * PPL, PPL, (long long)npix * D, kSiteRebase) &&
+                        (lane >= nb || PM_IN_BOUNDS((long long)pix * nb + lane, (long long)npix * nb, kSiteRebase));
 #pragma unroll
-        for (int j = 0; j < PPL / 2; ++j) h[r][j] = LDCG ? __ldcg(c + j) : c[j];
-        bl[r] = lane < nb ? (LDCG ? __ldcg(boff + (size_t)pix * nb + lane) : __ldg(boff + (size_t)pix * nb + lane))
-                          : inf_f();
+        for (int j = 0; j < PPL / 2; ++j) h[r][j] = !in ? __half2() : LDCG ? __ldcg(c + j) : c[j];
+        bl[r] = lane < nb && in ? (LDCG ? __ldcg(boff + (size_t)pix * nb + lane) : __ldg(boff + (size_t)pix * nb + lane))
+                                : inf_f();
     }
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
@@ -461,12 +468,13 @@ __device__ __forceinline__ void rebase_pixels(__half2* __restrict__ cost, const 
         }
         const float g = __any_sync(kFull, neg) ? 0.0f : warp_min_f32(bl[r]);
         __half2* c = cost + ((size_t)pix * D + lane * PPL) / 2;
+        const bool in = PM_RANGE_IN_BOUNDS((long long)pix * D + lane * PPL, PPL, (long long)npix * D, kSiteRebase);
 #pragma unroll
         for (int j = 0; j < PPL / 2; ++j) {
             const float2 v = __half22float2(h[r][j]);
             const float s0 = __fsub_rn(__shfl_sync(kFull, bl[r], (lane * PPL + 2 * j) >> 4), g);
             const float s1 = __fsub_rn(__shfl_sync(kFull, bl[r], (lane * PPL + 2 * j + 1) >> 4), g);
-            c[j] = __floats2half2_rn(__fadd_rn(v.x, s0), __fadd_rn(v.y, s1));
+            if (in) c[j] = __floats2half2_rn(__fadd_rn(v.x, s0), __fadd_rn(v.y, s1));
         }
         if (lane == 0) off[pix] = g;
     }

@@ -9,6 +9,19 @@
 #include "pm_stereo.h"
 
 namespace pm {
+
+#ifdef PM_BOUNDS_CHECK
+__device__ unsigned long long g_bounds_log[4];
+__device__ bool bounds_fail(int site, long long idx, long long n) {
+    if (atomicAdd(&g_bounds_log[0], 1ull) == 0) {
+        g_bounds_log[1] = (unsigned long long)site;
+        g_bounds_log[2] = (unsigned long long)idx;
+        g_bounds_log[3] = (unsigned long long)n;
+    }
+    return false;
+}
+#endif
+
 namespace {
 
 // definition of rcp_warp2 (see pm_device.cuh)
@@ -73,4 +86,24 @@ extern "C" pm_status pm_debug_check_arith(uint64_t out[4], void* stream) {
     cudaFree(bad);
     for (int k = 0; k < 4; ++k) out[k] = host[k];
     return st;
+}
+
+extern "C" pm_status pm_debug_bounds(uint64_t out[4], int reset) {
+    if (!out) return PM_ERR_INVALID_ARGUMENT;
+#ifdef PM_BOUNDS_CHECK
+    unsigned long long host[4] = {0, 0, 0, 0};
+    if (cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpyFromSymbol(host, pm::g_bounds_log, sizeof host) != cudaSuccess)
+        return PM_ERR_CUDA;
+    for (int k = 0; k < 4; ++k) out[k] = host[k];
+    if (reset) {
+        const unsigned long long zero[4] = {0, 0, 0, 0};
+        if (cudaMemcpyToSymbol(pm::g_bounds_log, zero, sizeof zero) != cudaSuccess) return PM_ERR_CUDA;
+    }
+    return PM_OK;
+#else
+    (void)reset;
+    for (int k = 0; k < 4; ++k) out[k] = 0;
+    return PM_ERR_UNSUPPORTED;   // the product library has no checks
+#endif
 }

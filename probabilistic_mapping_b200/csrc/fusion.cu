@@ -81,7 +81,8 @@ __device__ __forceinline__ int transform_pixel(const FuseLaunch& a, const FuseVi
     v.pre[3][index] = __double2float_rn(__dadd_rn((double)v.pre[3][index], __dmul_rn((double)pz2, 0.05)));
     if (index == 0) return kTfMoved;   // index 0 encodes "empty" in the reference's table
     const unsigned long long key = ((unsigned long long)__float_as_uint(pz2) << 32) | (unsigned)index;
-    atomicMin(a.ztable + (size_t)y2 * W + x2, key);
+    if (PM_IN_BOUNDS((long long)y2 * W + x2, (long long)W * H, kSiteFuseTransform))
+        atomicMin(a.ztable + (size_t)y2 * W + x2, key);
     return kTfMoved;
 }
 
@@ -121,6 +122,7 @@ __device__ __forceinline__ int2 update_pixel(const FuseLaunch& a, const FuseView
             for (int j = 1; j >= -1; --j) {
                 const int ny = y + i, nx = x + j;
                 if (nx <= 0 || nx >= W - 1 || ny <= 0 || ny >= H - 1) continue;
+                if (!PM_IN_BOUNDS((long long)ny * W + nx, (long long)W * H, kSiteFuseGather)) continue;
                 const unsigned long long kk = a.ztable[ny * W + nx];
                 if (kk != kEmpty) { t = (int)(unsigned)(kk & 0xffffffffu); break; }
             }
@@ -129,7 +131,7 @@ __device__ __forceinline__ int2 update_pixel(const FuseLaunch& a, const FuseView
 
     // depth_predict (:107-137)
     float ca, cb = 0.0f, cm = 0.0f, cs = 0.0f;
-    if (t == 0) {
+    if (t == 0 || !PM_IN_BOUNDS(t, (long long)W * H, kSiteFuseGather)) {
         ca = -1.0f;
     } else {
         ca = v.pre[0][t]; cb = v.pre[1][t]; cm = v.pre[2][t]; cs = v.pre[3][t];

@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(256) cpu_ztest_kernel(const FuseCpuLaunch a) {
         int last = -1;
         for (;;) {   // next hitter in index order: the smallest index above the last one
             int j = -1;
-            for (int k = first; k >= 0; k = a.next[k])
+            for (int k = first; k >= 0 && PM_IN_BOUNDS(k, (long long)a.W * a.H, kSiteCpuList); k = a.next[k])
                 if (k > last && (j < 0 || k < j)) j = k;
             if (j < 0) break;
             last = j;
@@ -112,6 +112,7 @@ __device__ __forceinline__ int3 cpu_update_pixel(const FuseCpuLaunch& a, int x, 
             for (int dx = -kExpand; dx <= kExpand; ++dx) {
                 const int sx = x + dx, sy = y + dy;
                 if (sx < kExpand || sx >= a.W - kExpand || sy < kExpand || sy >= a.H - kExpand) continue;
+                if (!PM_IN_BOUNDS((long long)sy * a.W + sx, (long long)a.W * a.H, kSiteCpuGather)) continue;
                 const uint32_t v = a.tab0[sy * a.W + sx];
                 if (v != 0) { t = v; break; }
             }
@@ -119,10 +120,10 @@ __device__ __forceinline__ int3 cpu_update_pixel(const FuseCpuLaunch& a, int x, 
     if (a.table) a.table[i] = t;
     // depthPreditCPU (:391-432)
     float ca, cb = a.cur[1][i], cm = a.cur[2][i], cs = a.cur[3][i];
-    if (t == 0) {
+    const int ts = (int)(t >> 16) * a.W + (int)(t & 0xffff);
+    if (t == 0 || !PM_IN_BOUNDS(ts, (long long)a.W * a.H, kSiteCpuGather)) {
         ca = 0.0f;
     } else {
-        const int ts = (int)(t >> 16) * a.W + (int)(t & 0xffff);
         ca = a.pre[0][ts]; cb = a.pre[1][ts]; cm = a.pre[2][ts]; cs = a.pre[3][ts];
     }
     // depthUpdateCPU (:439-566)

@@ -16,6 +16,25 @@ namespace pm {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+// ---- bounds-checked build ---------------------------------------------------------------
+// libpm_stereo_checked.so is compiled with -DPM_BOUNDS_CHECK (and relocatable device code, so
+// that every kernel shares one record).  In it each checked global access first tests its element
+// index against the buffer's extent; a failing index is not accessed.  Every failure is counted,
+// and the first failure's site (BoundsSite), index and extent are kept (pm_debug_bounds), so a
+// wrong index shows up as a record instead of a fault.  In the product library the test is the
+// constant true and compiles away.
+#ifdef PM_BOUNDS_CHECK
+extern __device__ unsigned long long g_bounds_log[4];   // failures, first site, its index, its extent
+__device__ bool bounds_fail(int site, long long idx, long long n);
+#define PM_IN_BOUNDS(idx, n, site)                                                        \
+    (((unsigned long long)(long long)(idx) < (unsigned long long)(long long)(n)) ||       \
+     ::pm::bounds_fail((site), (long long)(idx), (long long)(n)))
+#else
+#define PM_IN_BOUNDS(idx, n, site) true
+#endif
+// the elements [e, e + len) lie in [0, n)
+#define PM_RANGE_IN_BOUNDS(e, len, n, site) PM_IN_BOUNDS((e), (long long)(n) - (long long)(len) + 1, (site))
+
 __device__ __forceinline__ float nan_f() { return __int_as_float(0x7fffffff); }
 __device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
 

@@ -23,6 +23,24 @@ constexpr int kStatPred = kStatTf + kTfClasses;   // none, copied, filled
 constexpr int kStatUpd = kStatPred + 3;
 constexpr int kStatWords = kStatUpd + kUpdClasses;
 
+// Access sites of the bounds-checked build (PM_BOUNDS_CHECK): the site of a recorded failure.
+enum BoundsSite {
+    kSiteCostSource = 1,   // cost kernel: a source quad
+    kSiteCostState,        // cost kernel: a voxel of the running state (load or store)
+    kSiteCostOffset,       // cost kernel: a block offset or pixel offset of the FP16 form
+    kSiteRebase,           // rebase of the FP16 volume
+    kSitePairLoad,         // SGM pair kernel: a cost slice
+    kSitePairRef,          // SGM pair kernel: a reference pixel
+    kSitePairOut,          // SGM pair kernel: a pair-volume slice (store or reduction)
+    kSiteCombineLoad,      // combine kernel: a pair-volume slice or a pixel offset
+    kSiteCombineOut,       // combine kernel: depth, index or class of a pixel
+    kSiteFuseTransform,    // fusion: the z-buffer cell of a moved pixel
+    kSiteFuseGather,       // fusion: a neighbour or predecessor cell
+    kSiteCpuList,          // CPU-variant fusion: a hitter list entry or the occupant of a cell
+    kSiteCpuGather,        // CPU-variant fusion: a neighbour or predecessor cell
+    kSiteClassCount,       // pm_stats class counting
+};
+
 // ---- plane-sweep cost volume (calc_cost.cu) ----------------------------------------------
 struct CostLaunch {
     const float* ref;      // W*H scaled reference image

@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(256) count_classes_kernel(const uint8_t* __res
     __syncthreads();
     for (long base = (long)blockIdx.x * blockDim.x; base < npix; base += (long)gridDim.x * blockDim.x) {
         const long i = base + threadIdx.x;
-        const int v = i < npix ? (int)cls[i] : -1;
+        const int v = i < npix && PM_IN_BOUNDS(i, npix, kSiteClassCount) ? (int)cls[i] : -1;
         for (int c = 0; c < n; ++c) {
             const unsigned m = __ballot_sync(kFull, v == c);
             if ((threadIdx.x & 31) == 0 && m) atomicAdd(&s[c], (unsigned)__popc(m));

@@ -341,18 +341,20 @@ __device__ __forceinline__ void path_step(const SgmLaunch& a, PathState<PPL>& s,
 }
 
 // Reference intensity of step k of a chain starting at pixel p0 (0 past its end).
-__device__ __forceinline__ float chain_ref(const float* __restrict__ ref, long p0, long step, int k, int n) {
-    return k < n ? __ldg(ref + p0 + (long)k * step) : 0.0f;
+__device__ __forceinline__ float chain_ref(const float* __restrict__ ref, long p0, long step, int k, int n,
+                                           long npix) {
+    return k < n && PM_IN_BOUNDS(p0 + (long)k * step, npix, kSitePairRef) ? __ldg(ref + p0 + (long)k * step) : 0.0f;
 }
 
 // The flags |I(k) - I(k-1)| < tau of the 32 steps k0 .. k0+31 of one chain as a ballot (bit i:
 // step k0 + i).  Lane i holds I(k0 + i) in `cur` (read one batch ahead into `nxt`, which is
 // then refilled with I(k0 + 64 + i)); `last` carries I(k0 - 1).
 __device__ __forceinline__ unsigned penalty_flags(float& cur, float& nxt, const float* __restrict__ ref, long p0,
-                                                  long step, int k0, int n, int lane, float tau, float& last) {
+                                                  long step, int k0, int n, int lane, float tau, float& last,
+                                                  long npix) {
     const float I = cur;
     cur = nxt;
-    nxt = chain_ref(ref, p0, step, k0 + 64 + lane, n);
+    nxt = chain_ref(ref, p0, step, k0 + 64 + lane, n, npix);
     float prev = __shfl_up_sync(kFull, I, 1);
     if (lane == 0) prev = last;
     last = __shfl_sync(kFull, I, 31);
@@ -393,11 +395,15 @@ __device__ __forceinline__ void sgm_pair_block(const SgmLaunch& a, int dx, int d
     OT* const out = static_cast<OT*>(a.part[slot >> 1]);
     OT* qf = out + (size_t)pf0 * D + lane * PPL;        // the current step's output slices
     OT* qb = out + (size_t)pb0 * D + lane * PPL;
-    auto put = [](OT* q, const float (&v)[PPL]) {
+    const long npix = (long)W * H;
+    [[maybe_unused]] const long long nvox = (long long)npix * D;
+    auto put = [&](OT* q, const float (&v)[PPL]) {
+        if (!PM_RANGE_IN_BOUNDS(q - out, PPL, nvox, kSitePairOut)) return;
         if constexpr (HOUT) store_planes_h<PPL>(q, v);
         else store_planes<PPL>(q, v);
     };
-    auto add = [](OT* q, const float (&v)[PPL]) {
+    auto add = [&](OT* q, const float (&v)[PPL]) {
+        if (!PM_RANGE_IN_BOUNDS(q - out, PPL, nvox, kSitePairOut)) return;
         if constexpr (HOUT) red_planes_h<PPL>(q, v);
         else red_planes<PPL>(q, v);
     };
@@ -411,8 +417,11 @@ __device__ __forceinline__ void sgm_pair_block(const SgmLaunch& a, int dx, int d
     };
 
     auto issue = [&](unsigned char* sb, int k) {
-        cp_async_bytes<CB>(sb + lane * CB, cf0 + (long)k * gstep);
-        cp_async_bytes<CB>(sb + CHAIN_B + lane * CB, cb0 - (long)k * gstep);
+        [[maybe_unused]] const CT* const base = reinterpret_cast<const CT*>(a.cost);
+        if (PM_RANGE_IN_BOUNDS(cf0 + (long)k * gstep - base, PPL, nvox, kSitePairLoad))
+            cp_async_bytes<CB>(sb + lane * CB, cf0 + (long)k * gstep);
+        if (PM_RANGE_IN_BOUNDS(cb0 - (long)k * gstep - base, PPL, nvox, kSitePairLoad))
+            cp_async_bytes<CB>(sb + CHAIN_B + lane * CB, cb0 - (long)k * gstep);
     };
 #pragma unroll 1
     for (int k = 0; k < PF; ++k) {
@@ -426,10 +435,10 @@ __device__ __forceinline__ void sgm_pair_block(const SgmLaunch& a, int dx, int d
     PathState<PPL> fs, bs;
     float lastf = 0.0f, lastb = 0.0f;
     // intensities of steps lane and 32 + lane of both chains; then the flags of steps 0..31
-    float If = chain_ref(a.ref, pf0, step, lane, n), Ifn = chain_ref(a.ref, pf0, step, 32 + lane, n);
-    float Ib = chain_ref(a.ref, pb0, -step, lane, n), Ibn = chain_ref(a.ref, pb0, -step, 32 + lane, n);
-    fs.qmask = penalty_flags(If, Ifn, a.ref, pf0, step, 0, n, lane, a.tau, lastf);
-    bs.qmask = penalty_flags(Ib, Ibn, a.ref, pb0, -step, 0, n, lane, a.tau, lastb);
+    float If = chain_ref(a.ref, pf0, step, lane, n, npix), Ifn = chain_ref(a.ref, pf0, step, 32 + lane, n, npix);
+    float Ib = chain_ref(a.ref, pb0, -step, lane, n, npix), Ibn = chain_ref(a.ref, pb0, -step, 32 + lane, n, npix);
+    fs.qmask = penalty_flags(If, Ifn, a.ref, pf0, step, 0, n, lane, a.tau, lastf, npix);
+    bs.qmask = penalty_flags(Ib, Ibn, a.ref, pb0, -step, 0, n, lane, a.tau, lastb, npix);
 
     // step 0: the first pixel of both paths
     cp_async_wait<PF - 1>();
@@ -457,8 +466,8 @@ __device__ __forceinline__ void sgm_pair_block(const SgmLaunch& a, int dx, int d
         qf += gstep;
         qb -= gstep;
         if ((k & 31) == 0) {
-            fs.qmask = penalty_flags(If, Ifn, a.ref, pf0, step, k, n, lane, a.tau, lastf);
-            bs.qmask = penalty_flags(Ib, Ibn, a.ref, pb0, -step, k, n, lane, a.tau, lastb);
+            fs.qmask = penalty_flags(If, Ifn, a.ref, pf0, step, k, n, lane, a.tau, lastf, npix);
+            bs.qmask = penalty_flags(Ib, Ibn, a.ref, pb0, -step, k, n, lane, a.tau, lastb, npix);
         }
         cp_async_wait<PF - 1>();
         unsigned char* sb = wbase + st * STAGE_B;
@@ -517,8 +526,17 @@ __device__ __forceinline__ void combine_pixels(const SgmLaunch& a, long first, l
     // the FP16 volumes are half the bytes per pixel, so PD pixels are kept in flight instead of one
     constexpr int WPP = HIN ? PPL / 2 : PPL;
     constexpr int PD = HIN ? 3 : 1;
+    [[maybe_unused]] const long long nvox = (long long)a.W * a.H * D;
     auto loadw = [&](long pix, uint32_t (&w)[NP][WPP], float& off) {
         const size_t e = (size_t)pix * D + lane * PPL;
+        if (!PM_RANGE_IN_BOUNDS(e, PPL, nvox, kSiteCombineLoad)) {
+#pragma unroll
+            for (int g = 0; g < NP; ++g)
+#pragma unroll
+                for (int j = 0; j < WPP; ++j) w[g][j] = 0u;
+            off = 0.0f;
+            return;
+        }
 #pragma unroll
         for (int g = 0; g < NP; ++g) {
             const uint32_t* src = HIN ? reinterpret_cast<const uint32_t*>(static_cast<const __half*>(a.part[g]) + e)
@@ -578,14 +596,15 @@ __device__ __forceinline__ void combine_pixels(const SgmLaunch& a, long first, l
             for (int j = 0; j < PPL; ++j) o[j] = __fadd_rn(o[j], sh);
         }
 
-        if (a.total) store_planes<PPL>(a.total + (size_t)pix * D + lane * PPL, o);
+        if (a.total && PM_RANGE_IN_BOUNDS((size_t)pix * D + lane * PPL, PPL, nvox, kSiteCombineOut))
+            store_planes<PPL>(a.total + (size_t)pix * D + lane * PPL, o);
         if constexpr (MODE != kCombineStore) {
             float depth;
             int idx;
             int cls = 0;
             if constexpr (MODE == kCombineFilter) wta_filter<PPL>(o, incl, rk, lane, D, a.fp, depth, idx, cls);
             else case_argmin<PPL>(o, lane, D, a.fp, depth, idx);
-            if (lane == 0) {
+            if (lane == 0 && PM_IN_BOUNDS(pix, (long long)a.W * a.H, kSiteCombineOut)) {
                 const int y = (int)(pix / a.W), x = (int)(pix - (long)y * a.W);
                 *reinterpret_cast<float*>(reinterpret_cast<char*>(a.depth) + (size_t)y * a.depth_pitch +
                                           (size_t)x * 4) = depth;

@@ -106,3 +106,16 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "libpm_stereo.so"))
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         _lib.load()
+
+
+def test_checked_build_exports_the_same_entry_points(pm_lib):
+    """libpm_stereo_checked.so (PM_BOUNDS_CHECK) is built beside the product library and exports
+    the same C ABI; only the product library answers pm_debug_bounds with PM_ERR_UNSUPPORTED, and
+    it does so without touching the GPU."""
+    from probabilistic_mapping_b200 import _lib, build
+    assert os.path.exists(build.LIB_CHECKED)
+    checked = ctypes.CDLL(build.LIB_CHECKED)
+    for n in declared():
+        assert hasattr(checked, n), f"{n} missing from the checked build"
+    out = (ctypes.c_uint64 * 4)(1, 2, 3, 4)
+    assert pm_lib.pm_debug_bounds(out, 0) == _lib.PM_ERR_UNSUPPORTED and list(out) == [0, 0, 0, 0]
