@@ -652,7 +652,8 @@ pm_status pm_batch_create(const pm_config* cfgs, int n, int num_sources, int lan
             if (ok && esz == 2)
                 ok = alloc((void**)&l.off, 4 * q.N) && note(cudaMemset(l.off, 0, 4 * q.N)) &&
                      alloc((void**)&l.boff, 4 * q.N * (q.cfg.num_planes / 16));
-            for (int r = 0; r < q.cfg.num_paths / 2 && ok; ++r) ok = alloc((void**)&l.part[r], 4 * q.V);
+            // the FP16 form keeps its pair volumes in FP16 (SgmLaunch::part_half)
+            for (int r = 0; r < q.cfg.num_paths / 2 && ok; ++r) ok = alloc((void**)&l.part[r], esz * q.V);
             b->lanes.push_back(l);
             if (!ok) break;
         }

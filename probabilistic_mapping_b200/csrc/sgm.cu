@@ -73,10 +73,11 @@ __global__ void __launch_bounds__(NW * 32) sgm_pair_kernel(const SgmLaunch a, in
     sgm_pair_block<PPL, HALF, NW, FULL, HOUT>(a, dx, dy, slot, blockIdx.x, ring);
 }
 
-// Blocks per SM that the combine kernel is held to (0: no bound): D = 192 in FP32 and D = 256 in FP16
-// with four paths, where the compiler's default register choice leaves one block per SM fewer.
+// Blocks per SM that the combine kernel is held to (0: no bound): D = 192 in FP32, D = 256 in FP16
+// with four paths and D = 128 in FP16 with eight, where the compiler's default register choice
+// leaves one block per SM fewer.
 constexpr int combine_min_blocks(int ppl, int np, bool hin) {
-    return ppl == 6 && !hin ? (np == 2 ? 4 : 3) : ppl == 8 && hin && np == 2 ? 3 : 0;
+    return ppl == 6 && !hin ? (np == 2 ? 4 : 3) : ppl == 8 && hin && np == 2 ? 3 : ppl == 4 && hin && np == 4 ? 4 : 0;
 }
 
 // grid-stride over the image's pixels, one warp per pixel

@@ -574,14 +574,14 @@ __device__ __forceinline__ void combine_pixels(const SgmLaunch& a, long first, l
     };
     uint32_t ring[PD + 1][NP][WPP];
     float offr[PD + 1];
-#pragma unroll
-    for (int i = 0; i < PD; ++i)
-        if (first + i * nw < npix) loadw(first + i * nw, ring[i], offr[i]);
-    for (long pix = first; pix < npix; pix += nw) {
-        if (pix + PD * nw < npix) loadw(pix + PD * nw, ring[PD], offr[PD]);
+    // up to four planes per lane, the pixel of the warp's step t sits in ring slot t % (PD + 1) and
+    // the pixel loop is unrolled by PD + 1, so that every slot index is a constant and the ring
+    // rotates without register moves
+    const bool contiguous = a.depth_pitch == (size_t)a.W * sizeof(float);
+    auto process = [&](long pix, const uint32_t (&w)[NP][WPP], float off) {
         float cur[NP][PPL];
 #pragma unroll
-        for (int g = 0; g < NP; ++g) unpack(ring[0][g], cur[g]);
+        for (int g = 0; g < NP; ++g) unpack(w[g], cur[g]);
         float o[PPL];
 #pragma unroll
         for (int j = 0; j < PPL; ++j) {
@@ -591,7 +591,7 @@ __device__ __forceinline__ void combine_pixels(const SgmLaunch& a, long first, l
                 o[j] = __fadd_rn(cur[0][j], cur[1][j]);
         }
         if (a.offset) {   // every path carries the FP16 volume's per-pixel shift once
-            const float sh = __fmul_rn((float)(2 * NP), offr[0]);
+            const float sh = __fmul_rn((float)(2 * NP), off);
 #pragma unroll
             for (int j = 0; j < PPL; ++j) o[j] = __fadd_rn(o[j], sh);
         }
@@ -605,20 +605,44 @@ __device__ __forceinline__ void combine_pixels(const SgmLaunch& a, long first, l
             if constexpr (MODE == kCombineFilter) wta_filter<PPL>(o, incl, rk, lane, D, a.fp, depth, idx, cls);
             else case_argmin<PPL>(o, lane, D, a.fp, depth, idx);
             if (lane == 0 && PM_IN_BOUNDS(pix, (long long)a.W * a.H, kSiteCombineOut)) {
-                const int y = (int)(pix / a.W), x = (int)(pix - (long)y * a.W);
-                *reinterpret_cast<float*>(reinterpret_cast<char*>(a.depth) + (size_t)y * a.depth_pitch +
-                                          (size_t)x * 4) = depth;
+                float* dp = a.depth + pix;
+                if (!contiguous) {   // W * H < 2^32: 32-bit division
+                    const unsigned up = (unsigned)pix, uw = (unsigned)a.W;
+                    const unsigned y = up / uw, x = up - y * uw;
+                    dp = reinterpret_cast<float*>(reinterpret_cast<char*>(a.depth) + (size_t)y * a.depth_pitch) + x;
+                }
+                *dp = depth;
                 if (a.index) a.index[pix] = idx;
                 if (a.wta_class) a.wta_class[pix] = (uint8_t)cls;
             }
         }
+    };
 #pragma unroll
-        for (int i = 0; i < PD; ++i) {
-            offr[i] = offr[i + 1];
+    for (int i = 0; i < PD; ++i)
+        if (first + i * nw < npix) loadw(first + i * nw, ring[i], offr[i]);
+    if constexpr (PPL <= 4) {
+        for (long pix = first; pix < npix;) {
 #pragma unroll
-            for (int g = 0; g < NP; ++g)
+            for (int u = 0; u <= PD; ++u) {   // slot u holds pix; slot (u + PD) % (PD + 1) takes pix + PD * nw
+                if (pix >= npix) break;
+                const int ld = (u + PD) % (PD + 1);
+                if (pix + PD * nw < npix) loadw(pix + PD * nw, ring[ld], offr[ld]);
+                process(pix, ring[u], offr[u]);
+                pix += nw;
+            }
+        }
+    } else {   // more planes per lane: one copy of the body, the ring shifted by register moves
+        for (long pix = first; pix < npix; pix += nw) {
+            if (pix + PD * nw < npix) loadw(pix + PD * nw, ring[PD], offr[PD]);
+            process(pix, ring[0], offr[0]);
 #pragma unroll
-                for (int j = 0; j < WPP; ++j) ring[i][g][j] = ring[i + 1][g][j];
+            for (int i = 0; i < PD; ++i) {
+                offr[i] = offr[i + 1];
+#pragma unroll
+                for (int g = 0; g < NP; ++g)
+#pragma unroll
+                    for (int j = 0; j < WPP; ++j) ring[i][g][j] = ring[i + 1][g][j];
+            }
         }
     }
 }
