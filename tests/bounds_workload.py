@@ -24,6 +24,8 @@ MAPPERS = [   # width, height, planes, precision, sampler, cost mode, paths, fus
     (64, 33, 64, 1, 0, 0, 8, 0, 2),
     (101, 47, 96, 0, 2, 0, 8, 1, 8),
     (70, 90, 64, 1, 1, 0, 8, 0, 8),
+    (45, 37, 192, 0, 0, 1, 8, 0, 8),    # six planes per lane, planes left out of the reduction tree
+    (52, 29, 256, 1, 2, 0, 4, 1, 2),    # eight planes per lane, FP16, incremental passes
 ]
 
 

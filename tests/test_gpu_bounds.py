@@ -1,4 +1,5 @@
-"""The bounds-checked build (libpm_stereo_checked.so, PM_BOUNDS_CHECK) on odd image shapes: every
+"""The bounds-checked build (libpm_stereo_checked.so, PM_BOUNDS_CHECK) on odd image shapes and
+64 to 256 planes: every
 checked global access of the cost, rebase, SGM pair, combine, counting and fusion kernels stays
 inside its buffer (the record of skipped accesses is empty), and the checked build's outputs are
 bit-identical to the product library's on the same inputs.  Both libraries run the same workload
