@@ -112,8 +112,11 @@ __device__ __forceinline__ float2 sample2(const Src<SAMP>& src, const WarpConst&
     }
     const float2 u = __fmul2_rn(nx, r), v = __fmul2_rn(ny, r);
     // u + 0 turns -0 into +0 (which the reference's u < 0 accepts); then 0 <= u <= W-1 is one
-    // unsigned compare of the bit patterns: negative values and NaN have patterns above W-1's
-    const float2 uz = __fadd2_rn(u, f2(0.0f, 0.0f)), vz = __fadd2_rn(v, f2(0.0f, 0.0f));
+    // unsigned compare of the bit patterns: negative values and NaN have patterns above W-1's.
+    // The FP16 form's warps already use the reciprocal estimate, so it leaves out the +0: a
+    // coordinate of exactly -0 (a numerator of -0, which needs rho = 0) is then rejected.
+    constexpr bool EXACT = !(SAMP == kTex || SAMP == kQuadH);
+    const float2 uz = EXACT ? __fadd2_rn(u, f2(0.0f, 0.0f)) : u, vz = EXACT ? __fadd2_rn(v, f2(0.0f, 0.0f)) : v;
     const unsigned Wb = __float_as_uint(c.W1), Hb = __float_as_uint(c.H1);
     const bool ok0 = (w.x >= 0.0f) && (__float_as_uint(uz.x) <= Wb) && (__float_as_uint(vz.x) <= Hb);
     const bool ok1 = (w.y >= 0.0f) && (__float_as_uint(uz.y) <= Wb) && (__float_as_uint(vz.y) <= Hb);
