@@ -71,6 +71,13 @@ __device__ __forceinline__ void lane_order(const PlaneOrder& o, int lane, uint32
     for (int j = 0; j < PPL; ++j) rk[j] = s_rank[lane * PPL + j];
 }
 
+// |x| < FLOAT_EPS evaluated in double, as the reference's float-against-double compares
+// (filter_cost.cu:37, stereo_mapper.cpp:651): RN_float(1e-5) = 9.99999974737875e-06 lies below
+// 1e-5 and the next float above it, so (double)x < 1e-5 holds exactly when x <= that float.
+constexpr float kFloatEpsBelow = 9.99999974737875e-06f;
+__device__ __forceinline__ bool below_eps(float x) { return x <= kFloatEpsBelow; }
+__device__ __forceinline__ bool within_eps(float x) { return x <= kFloatEpsBelow && x >= -kFloatEpsBelow; }
+
 // Winner-take-all with the reference tree's tie-break, then the three rejection rules and
 // the parabola subpixel refinement (filter_cost.cu:22-52), plus the optional uniqueness test.
 template <int PPL>
@@ -93,7 +100,7 @@ __device__ __forceinline__ void wta_filter(const float (&s)[PPL], uint32_t incl,
 
     float depth;
     int cls = kWtaDepth;
-    if ((double)mn < kFloatEps && (double)mn > -kFloatEps) {
+    if (within_eps(mn)) {
         depth = kDepInf;                                   // non-overlap (:37-38)
         cls = kWtaNoOverlap;
     } else if (idx == 0 || idx == D - 1) {
@@ -123,7 +130,7 @@ __device__ __forceinline__ void wta_filter(const float (&s)[PPL], uint32_t incl,
                 const float a2 = __fadd_rn(__fsub_rn(pre, __fmul_rn(2.0f, mn)), post);
                 const float b = __fadd_rn(-pre, post);
                 const float sub = __fsub_rn((float)idx, __fdiv_rn(b, __fmul_rn(2.0f, a2)));
-                depth = __frcp_rn(__fmaf_rn(sub, fp.drho, fp.rho0));
+                depth = rcp_rn(__fmaf_rn(sub, fp.drho, fp.rho0));
             }
         }
     }
@@ -150,9 +157,9 @@ __device__ __forceinline__ void case_argmin(const float (&s)[PPL], int lane, int
     const unsigned r = __reduce_min_sync(kFull, m == mn ? mi : 0xffffffffu);
     const int idx = r < (unsigned)D ? (int)r : 0;
     float v;
-    if ((double)mn < kFloatEps) v = kCaseInf;
+    if (below_eps(mn)) v = kCaseInf;
     else if (idx == 0 || idx == D - 1) v = 0.0f;
-    else v = __frcp_rn(__fmaf_rn((float)idx, fp.drho, fp.rho0));
+    else v = rcp_rn(__fmaf_rn((float)idx, fp.drho, fp.rho0));
     out = v;
     idx_out = idx;
 }
@@ -582,18 +589,17 @@ __device__ __forceinline__ void combine_pixels(const SgmLaunch& a, long first, l
         float cur[NP][PPL];
 #pragma unroll
         for (int g = 0; g < NP; ++g) unpack(w[g], cur[g]);
-        float o[PPL];
-#pragma unroll
-        for (int j = 0; j < PPL; ++j) {
-            if constexpr (NP == 4)
-                o[j] = __fadd_rn(__fadd_rn(cur[0][j], cur[1][j]), __fadd_rn(cur[2][j], cur[3][j]));
-            else
-                o[j] = __fadd_rn(cur[0][j], cur[1][j]);
+        float o[PPL];   // (P0 + P1) + (P2 + P3), two planes per packed add
+        if constexpr (NP == 4) {
+            float s01[PPL], s23[PPL];
+            add_planes<PPL>(s01, cur[0], cur[1]);
+            add_planes<PPL>(s23, cur[2], cur[3]);
+            add_planes<PPL>(o, s01, s23);
+        } else {
+            add_planes<PPL>(o, cur[0], cur[1]);
         }
         if (a.offset) {   // every path carries the FP16 volume's per-pixel shift once
-            const float sh = __fmul_rn((float)(2 * NP), off);
-#pragma unroll
-            for (int j = 0; j < PPL; ++j) o[j] = __fadd_rn(o[j], sh);
+            add_planes<PPL>(o, o, __fmul_rn((float)(2 * NP), off));
         }
 
         if (a.total && PM_RANGE_IN_BOUNDS((size_t)pix * D + lane * PPL, PPL, nvox, kSiteCombineOut))
