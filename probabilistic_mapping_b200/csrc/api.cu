@@ -687,8 +687,8 @@ pm_status pm_output_fusion(pm_mapper* h, float* depth, size_t depth_pitch, float
         f.H = H;
         fusion_pose(R, t, h->R_prev, h->t_prev, f.pose);
         f.cam[0] = fx; f.cam[1] = fy; f.cam[2] = cx; f.cam[3] = cy;
-        PM_CK(h, cudaMemcpyAsync(h->d_fused, h->d_depth, 4 * N, cudaMemcpyDeviceToDevice, h->stream));
-        f.depth = h->d_fused;
+        f.depth = h->d_fused;   // written from the WTA depth by the update kernel
+        f.depth_in = h->d_depth;
         for (int k = 0; k < 4; ++k) {
             f.pre[k] = h->d_state[h->pre_index][k];
             f.cur[k] = h->d_state[h->pre_index ^ 1][k];

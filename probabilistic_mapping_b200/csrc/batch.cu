@@ -306,12 +306,12 @@ cudaError_t enqueue_fusion(pm_batch* b, int i, int k, cudaStream_t m) {
     Seq& q = b->seqs[i];
     const size_t N = q.N;
     cudaError_t e;
-    if ((e = cudaMemcpyAsync(q.d_fused, q.d_depth, 4 * N, cudaMemcpyDeviceToDevice, m))) return e;
     FuseLaunch f;
     std::memset(&f, 0, sizeof f);
     f.W = q.cfg.width;
     f.H = q.cfg.height;
-    f.depth = q.d_fused;
+    f.depth = q.d_fused;      // written from the WTA depth by the update kernel
+    f.depth_in = q.d_depth;
     f.ztable = q.d_ztable;
     f.table = q.d_table;
     f.variance = q.d_var;

@@ -231,10 +231,11 @@ __device__ __forceinline__ void fold2(float2& acc, float2& cn, float2 tmp, float
 // running mean (calc_cost.cu:200-207) and this mean differ only by FP32 rounding, far below the
 // FP16 volume's step.
 __device__ __forceinline__ void fold2_sum(float2& acc, __half2& cn, float2 tmp, float r9) {
-    const bool v0 = tmp.x == tmp.x, v1 = tmp.y == tmp.y;
-    acc = __ffma2_rn(make_float2(v0 ? tmp.x : 0.0f, v1 ? tmp.y : 0.0f), make_float2(r9, r9), acc);
-    const unsigned one = (v0 ? 0x3C00u : 0u) | (v1 ? 0x3C000000u : 0u);   // (v0, v1) as FP16 ones
-    cn = __hadd2(cn, *reinterpret_cast<const __half2*>(&one));
+    // a measured sum is >= +0 and a rejected one NaN, so fmaxf(tmp, 0) is the sum or 0 (the
+    // maximum drops a NaN operand); 1 + 0 * tmp is 1 or NaN, and its maximum with 0 the count step
+    acc = __ffma2_rn(make_float2(fmaxf(tmp.x, 0.0f), fmaxf(tmp.y, 0.0f)), make_float2(r9, r9), acc);
+    const float2 one = __ffma2_rn(tmp, make_float2(0.0f, 0.0f), make_float2(1.0f, 1.0f));
+    cn = __hadd2(cn, __floats2half2_rn(fmaxf(one.x, 0.0f), fmaxf(one.y, 0.0f)));
 }
 __device__ __forceinline__ float sum_to_mean(float sum, float cnt) {
     if (cnt == 0.0f) return -1.0f;   // never measured (initReference's -1, stereo_mapper.cpp:69)

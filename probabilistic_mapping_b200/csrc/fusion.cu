@@ -138,7 +138,7 @@ __device__ __forceinline__ int2 update_pixel(const FuseLaunch& a, const FuseView
     }
 
     // depthUpdate (:139-225)
-    const float d = a.depth[e];
+    const float d = a.depth_in ? a.depth_in[e] : a.depth[e];
     const float unc = __double2float_rn(__dmul_rn((double)__fmul_rn(d, d), 0.01));   // (:151)
     float out_d = d;
     bool write_all = (t != 0);   // predict copied the whole state

@@ -163,7 +163,8 @@ struct FuseLaunch {
     int W, H;
     float pose[12];        // R_p2c row-major, t_p2c
     float cam[4];          // fx, fy, cx, cy
-    float* depth;          // in: WTA depth, out: fused depth (W*H)
+    float* depth;          // in: WTA depth (unless depth_in is given), out: fused depth (W*H)
+    const float* depth_in; // W*H WTA depth read instead of depth (nullptr: depth in place)
     float* pre[4];         // alpha, beta, mu, sigma of the previous keyframe (modified)
     float* cur[4];         // state of the current keyframe (written)
     unsigned long long* ztable;  // W*H scratch z-buffer
