@@ -98,11 +98,18 @@ struct WarpConst {
 // the hardware reciprocal estimate); rejected (NaN) when w < 0 or (u, v) lies outside
 // [0, W-1] x [0, H-1] (NaN coordinates included).
 template <int SAMP>
+__device__ __forceinline__ float2 sample2_core(const Src<SAMP>& src, const WarpConst& c, float2 w, float2 nx,
+                                               float2 ny);
+template <int SAMP>
 __device__ __forceinline__ float2 sample2(const Src<SAMP>& src, const WarpConst& c, float x, float y, float z,
                                           float2 rho) {
-    const float2 w = __ffma2_rn(c.t3, rho, f2(z, z));
-    const float2 nx = __ffma2_rn(c.t1, rho, f2(x, x));
-    const float2 ny = __ffma2_rn(c.t2, rho, f2(y, y));
+    return sample2_core<SAMP>(src, c, __ffma2_rn(c.t3, rho, f2(z, z)), __ffma2_rn(c.t1, rho, f2(x, x)),
+                              __ffma2_rn(c.t2, rho, f2(y, y)));
+}
+// The same from the denominator w and the numerators (nx, ny) of the plane pair.
+template <int SAMP>
+__device__ __forceinline__ float2 sample2_core(const Src<SAMP>& src, const WarpConst& c, float2 w, float2 nx,
+                                               float2 ny) {
     float2 r;
     if constexpr (SAMP == kTex || SAMP == kQuadH) {
         asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r.x) : "f"(w.x));
@@ -249,6 +256,7 @@ __device__ __forceinline__ float sum_to_mean(float sum, float cnt) {
 template <int MODE, bool HALF, int SAMP, bool INC>
 __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, int bz, unsigned char* smem_raw) {
     constexpr bool HC = HALF && !INC;   // sums and FP16 counts
+    constexpr bool PM = HALF;           // packed-pair warp coordinates (see the source loop)
     using SM = SmemL<HC>;
     using CntT = typename std::conditional<HC, __half, float>::type;
     float2* const refp = reinterpret_cast<float2*>(smem_raw + SM::REF);
@@ -317,6 +325,35 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
         c.t3 = f2(h.t3, h.t3);
         c.W1 = (float)(W - 1);
         c.H1 = (float)(H - 1);
+        // FP16 form (PM): the warped coordinates of the plane pair as packed pairs straight from
+        // per-source constants.  At row y the denominator and numerators are R*y + A (one packed
+        // FMA each: A holds the column's terms and t*rho), and MODE 0's corrupted neighbours 4
+        // and 8 are the centre row's x plus constant pairs B and C (one packed add each).  The
+        // association differs from the reference's expressions by rounding only, inside the FP16
+        // form's tolerance; the FP32 forms keep the reference's expressions bit for bit.
+        [[maybe_unused]] float Xc = 0.0f;
+        [[maybe_unused]] float2 A1, A2, A3, R12, R22, R32, B1, B2, B3, C1, C2, C3;
+        if constexpr (PM) {
+            const float fx = (float)x;
+            const float2 T1 = __fmul2_rn(c.t1, rho), T2 = __fmul2_rn(c.t2, rho), T3 = __fmul2_rn(c.t3, rho);
+            Xc = __fmaf_rn(h.r11, fx, h.r13);
+            const float Yc = __fmaf_rn(h.r21, fx, h.r23), Zc = __fmaf_rn(h.r31, fx, h.r33);
+            A1 = __fadd2_rn(f2(Xc, Xc), T1);
+            A2 = __fadd2_rn(f2(Yc, Yc), T2);
+            A3 = __fadd2_rn(f2(Zc, Zc), T3);
+            R12 = f2(h.r12, h.r12);
+            R22 = f2(h.r22, h.r22);
+            R32 = f2(h.r32, h.r32);
+            if constexpr (MODE == 0) {
+                B1 = __fadd2_rn(f2(h.r11, h.r11), T1);
+                B2 = __fadd2_rn(f2(h.r21, h.r21), T2);
+                B3 = __fadd2_rn(f2(h.r31, h.r31), T3);
+                const float e1 = __fsub_rn(h.r11, h.r12), e2 = __fsub_rn(h.r11, h.r22), e3 = __fsub_rn(h.r11, h.r32);
+                C1 = __fadd2_rn(f2(e1, e1), T1);
+                C2 = __fadd2_rn(f2(e2, e2), T2);
+                C3 = __fadd2_rn(f2(e3, e3), T3);
+            }
+        }
 
         // rows r-2 (up) and r-1 (centre) of this column (S) and of its left / right neighbour
         // columns (L / R); row r (down) is computed in the iteration
@@ -324,9 +361,19 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
         float hxc = 0.0f;
 #pragma unroll   // unrolled, the rolling row registers are renamed instead of copied
         for (int r = 0; r < TY + 2; ++r) {
-            float hx, hy, hz;
-            homog(h, x, y0 - 1 + r, hx, hy, hz);
-            const float2 Sd = sample2<SAMP>(src, c, hx, hy, hz, rho);
+            float hx = 0.0f;   // the row's homogeneous x: MODE 0's neighbours of the next output row
+            float2 Sd;
+            if constexpr (PM) {
+                const float fy = (float)(y0 - 1 + r);
+                const float2 yy = f2(fy, fy);
+                Sd = sample2_core<SAMP>(src, c, __ffma2_rn(R32, yy, A3), __ffma2_rn(R12, yy, A1),
+                                        __ffma2_rn(R22, yy, A2));
+                if constexpr (MODE == 0) hx = __fmaf_rn(h.r12, fy, Xc);
+            } else {
+                float hy, hz;
+                homog(h, x, y0 - 1 + r, hx, hy, hz);
+                Sd = sample2<SAMP>(src, c, hx, hy, hz, rho);
+            }
             const float2 Ld = shfl_up2(Sd), Rd_ = shfl_down2(Sd);
             const int o = r - 2;   // output row y0 + o
             if (o >= 0 && out_col && y0 + o < H) {
@@ -337,10 +384,17 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
                 float2 d[9];
                 if constexpr (MODE == 0) {
                     // the corrupted neighbours (calc_cost.cu:49-51, 69-71) from the centre's x
-                    const float xr = __fadd_rn(hxc, h.r11), yr = __fadd_rn(hxc, h.r21), zr = __fadd_rn(hxc, h.r31);
-                    const float xru = __fsub_rn(xr, h.r12), yru = __fsub_rn(xr, h.r22), zru = __fsub_rn(xr, h.r32);
-                    const float2 B4 = sample2<SAMP>(src, c, xr, yr, zr, rho);
-                    const float2 B8 = sample2<SAMP>(src, c, xru, yru, zru, rho);
+                    float2 B4, B8;
+                    if constexpr (PM) {
+                        const float2 xc = f2(hxc, hxc);
+                        B4 = sample2_core<SAMP>(src, c, __fadd2_rn(xc, B3), __fadd2_rn(xc, B1), __fadd2_rn(xc, B2));
+                        B8 = sample2_core<SAMP>(src, c, __fadd2_rn(xc, C3), __fadd2_rn(xc, C1), __fadd2_rn(xc, C2));
+                    } else {
+                        const float xr = __fadd_rn(hxc, h.r11), yr = __fadd_rn(hxc, h.r21), zr = __fadd_rn(hxc, h.r31);
+                        const float xru = __fsub_rn(xr, h.r12), yru = __fsub_rn(xr, h.r22), zru = __fsub_rn(xr, h.r32);
+                        B4 = sample2<SAMP>(src, c, xr, yr, zr, rho);
+                        B8 = sample2<SAMP>(src, c, xru, yru, zru, rho);
+                    }
                     d[0] = sub2(Rc_, Sc);    // 0  (:93)
                     d[1] = sub2(Rd, Su);     // 1  warps (u, v-1), reads ref (u, v+1) (:106)
                     d[2] = sub2(Ru_, Sd);    // 2  warps (u, v+1), reads ref (u, v-1) (:119)
