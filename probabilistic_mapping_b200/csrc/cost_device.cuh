@@ -26,8 +26,7 @@ template <bool HC> struct SmemL {
     static constexpr size_t REF = 0;                                              // float2 [TY+2][32]
     static constexpr size_t ACC = REF + sizeof(float2) * (TY + 2) * 32;           // float [NPIX][SP]
     static constexpr size_t CNT = ACC + sizeof(float) * NPIX * SP;                // float or half [NPIX][SP]
-    static constexpr size_t OFF = CNT + (HC ? sizeof(__half) : sizeof(float)) * NPIX * SP;   // float [NPIX] (FP16 form)
-    static constexpr size_t BYTES = OFF + sizeof(float) * NPIX;
+    static constexpr size_t BYTES = CNT + (HC ? sizeof(__half) : sizeof(float)) * NPIX * SP;
 };
 using Smem = SmemL<false>;   // the larger layout
 
@@ -279,10 +278,10 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
 
     // running state of the tile's voxels, [pixel][plane] with pitch SP: from memory (the
     // state of earlier calls), or the initReference state cost = -1, count = 0
-    for (int e = tid; e < NPIX * PCB; e += NT) {
-        const int p = e / PCB, k = e - p * PCB;
-        float c0 = (HALF && !INC) ? 0.0f : -1.0f, n0 = 0.0f;   // sum or running mean, count
-        if (INC) {
+    if constexpr (INC) {
+        for (int e = tid; e < NPIX * PCB; e += NT) {
+            const int p = e / PCB, k = e - p * PCB;
+            float c0 = -1.0f, n0 = 0.0f;   // running mean, count
             const int o = p / TXU, i = p - o * TXU;
             const int gx = x0 + i, gy = y0 + o;
             const size_t g = ((size_t)gy * W + gx) * D + d0 + k;
@@ -291,9 +290,19 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
                 if constexpr (HALF) c0 = __fadd_rn(c0, a.offset[(size_t)gy * W + gx]);
                 n0 = a.cnt[g];
             }
+            accs[p * SP + k] = c0;
+            cnts[p * SP + k] = (CntT)n0;
         }
-        accs[p * SP + k] = c0;
-        cnts[p * SP + k] = (CntT)n0;
+    } else {
+        // the whole arrays, pitch padding included, in 16-byte stores: -1 (FP16 form: a sum of
+        // 0) and a count of 0, whose FP32 and FP16 bit patterns are both zero
+        static_assert((NPIX * SP * sizeof(float)) % 16 == 0 && (NPIX * SP * sizeof(CntT)) % 16 == 0 &&
+                          SM::ACC % 16 == 0 && SM::CNT % 16 == 0, "16-byte state stores");
+        const float c0 = HC ? 0.0f : -1.0f;
+        float4* const av = reinterpret_cast<float4*>(accs);
+        for (int i = tid; i < NPIX * SP / 4; i += NT) av[i] = make_float4(c0, c0, c0, c0);
+        float4* const cv = reinterpret_cast<float4*>(cnts);
+        for (int i = tid; i < (int)(NPIX * SP * sizeof(CntT) / 16); i += NT) cv[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
     __syncthreads();
 
@@ -436,55 +445,73 @@ __device__ __forceinline__ void cost_tile(const CostLaunch& a, int bx, int by, i
         }
     }
 
-    // store contiguous plane runs of the volume (plane-innermost layout)
+    // store contiguous plane runs of the volume (plane-innermost layout): one thread per pixel
+    // and 4 consecutive planes, the 4 threads of a pixel in consecutive lanes of one warp
     __syncthreads();
-    if constexpr (HALF) {
-        if constexpr (!INC) {   // sums and counts to means
-            for (int e = tid; e < NPIX * PCB; e += NT) {
-                const int p = e / PCB, k = e - p * PCB;
-                accs[p * SP + k] = sum_to_mean(accs[p * SP + k], (float)cnts[p * SP + k]);
-            }
-            __syncthreads();
+    constexpr int NQ = NPIX * (PCB / 4);
+    static_assert(PCB % 4 == 0 && SP % 2 == 0 && NQ % 32 == 0, "whole warps per pass, 8-byte state pairs");
+    // vector stores where the caller's buffers allow them (stage entry points take any pointer)
+    const bool vcost = (reinterpret_cast<uintptr_t>(a.cost) & (HALF ? 7 : 15)) == 0;
+    const bool vcnt = (reinterpret_cast<uintptr_t>(a.cnt) & 15) == 0;
+    for (int e = tid; e < NQ; e += NT) {   // warp-uniform trip count
+        const int p = e >> 2, k = (e & 3) * 4;
+        const int o = p / TXU, i = p - o * TXU;
+        const int gx = x0 + i, gy = y0 + o;
+        const size_t g = ((size_t)gy * W + gx) * D + d0 + k;
+        const float2 s01 = *reinterpret_cast<const float2*>(accs + p * SP + k);
+        const float2 s23 = *reinterpret_cast<const float2*>(accs + p * SP + k + 2);
+        float n[4];
+        if constexpr (HC) {
+            const float2 n01 = __half22float2(*reinterpret_cast<const __half2*>(cnts + p * SP + k));
+            const float2 n23 = __half22float2(*reinterpret_cast<const __half2*>(cnts + p * SP + k + 2));
+            n[0] = n01.x; n[1] = n01.y; n[2] = n23.x; n[3] = n23.y;
+        } else {
+            const float2 n01 = *reinterpret_cast<const float2*>(cnts + p * SP + k);
+            const float2 n23 = *reinterpret_cast<const float2*>(cnts + p * SP + k + 2);
+            n[0] = n01.x; n[1] = n01.y; n[2] = n23.x; n[3] = n23.y;
         }
-        // per pixel and 16-plane block: the smallest measured cost of the block (0 when none is
-        // measured) is stored beside the block, and the half volume holds the differences
-        float* const s_off = reinterpret_cast<float*>(smem_raw + SM::OFF);
-        for (int p = tid; p < NPIX; p += NT) {
+        float v[4] = {s01.x, s01.y, s23.x, s23.y};
+        if constexpr (HC) {   // sums and counts to means
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = sum_to_mean(v[j], n[j]);
+        }
+        const bool in = gx < W && gy < H && PM_RANGE_IN_BOUNDS(g, 4, (long long)W * H * D, kSiteCostState);
+        if constexpr (HALF) {
+            // per pixel and 16-plane block: the smallest measured cost of the block (0 when none
+            // is measured) is stored beside the block, and the half volume holds the differences
             float m = inf_f();
 #pragma unroll
-            for (int k = 0; k < PCB; ++k) {
-                const float v = accs[p * SP + k];
-                m = v >= 0.0f ? fminf(m, v) : m;
-            }
+            for (int j = 0; j < 4; ++j) m = v[j] >= 0.0f ? fminf(m, v[j]) : m;
+            m = fminf(m, __shfl_xor_sync(kFull, m, 1));
+            m = fminf(m, __shfl_xor_sync(kFull, m, 2));
             m = m == inf_f() ? 0.0f : m;
-            s_off[p] = m;
-            const int o = p / TXU, i = p - o * TXU;
-            const int gx = x0 + i, gy = y0 + o;
             const size_t bo = ((size_t)gy * W + gx) * (D / PCB) + bz;
-            if (gx < W && gy < H && PM_IN_BOUNDS(bo, (long long)W * H * (D / PCB), kSiteCostOffset))
+            if (k == 0 && gx < W && gy < H && PM_IN_BOUNDS(bo, (long long)W * H * (D / PCB), kSiteCostOffset))
                 a.block_offset[bo] = m;
-        }
-        __syncthreads();
-        for (int e = tid; e < NPIX * PCB; e += NT) {
-            const int p = e / PCB, k = e - p * PCB;
-            const int o = p / TXU, i = p - o * TXU;
-            const int gx = x0 + i, gy = y0 + o;
-            const size_t g = ((size_t)gy * W + gx) * D + d0 + k;
-            if (gx < W && gy < H && PM_IN_BOUNDS(g, (long long)W * H * D, kSiteCostState)) {
-                store_cost<true>(a.cost, g, __fsub_rn(accs[p * SP + k], s_off[p]));
-                if (a.cnt) a.cnt[g] = (float)cnts[p * SP + k];
+            if (in) {
+                const __half2 h01 = __floats2half2_rn(__fsub_rn(v[0], m), __fsub_rn(v[1], m));
+                const __half2 h23 = __floats2half2_rn(__fsub_rn(v[2], m), __fsub_rn(v[3], m));
+                __half2* const dst = reinterpret_cast<__half2*>(reinterpret_cast<__half*>(a.cost) + g);
+                if (vcost) {
+                    uint2 u;
+                    u.x = *reinterpret_cast<const unsigned*>(&h01);
+                    u.y = *reinterpret_cast<const unsigned*>(&h23);
+                    *reinterpret_cast<uint2*>(dst) = u;
+                } else {
+                    __half* const hd = reinterpret_cast<__half*>(dst);
+                    hd[0] = __low2half(h01); hd[1] = __high2half(h01);
+                    hd[2] = __low2half(h23); hd[3] = __high2half(h23);
+                }
             }
+        } else if (in) {
+            float* const dst = reinterpret_cast<float*>(a.cost) + g;
+            if (vcost) *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+            else { dst[0] = v[0]; dst[1] = v[1]; dst[2] = v[2]; dst[3] = v[3]; }
         }
-    } else {
-        for (int e = tid; e < NPIX * PCB; e += NT) {
-            const int p = e / PCB, k = e - p * PCB;
-            const int o = p / TXU, i = p - o * TXU;
-            const int gx = x0 + i, gy = y0 + o;
-            const size_t g = ((size_t)gy * W + gx) * D + d0 + k;
-            if (gx < W && gy < H && PM_IN_BOUNDS(g, (long long)W * H * D, kSiteCostState)) {
-                store_cost<false>(a.cost, g, accs[p * SP + k]);
-                if (a.cnt) a.cnt[g] = cnts[p * SP + k];
-            }
+        if (in && a.cnt) {
+            float* const cd = a.cnt + g;
+            if (vcnt) *reinterpret_cast<float4*>(cd) = make_float4(n[0], n[1], n[2], n[3]);
+            else { cd[0] = n[0]; cd[1] = n[1]; cd[2] = n[2]; cd[3] = n[3]; }
         }
     }
 }

@@ -95,6 +95,41 @@ def test_calc_cost_incremental_matches_single_pass(pm_lib):
     assert (cnt.cpu().numpy() == want_cnt).all()
 
 
+@pytest.mark.parametrize("offset", [1, 2])
+def test_calc_cost_unaligned_buffers(pm_lib, offset):
+    """Volume and count buffers that start 4 or 8 bytes past a 16-byte boundary (the kernel's
+    vector stores need 16): the same values as the oracle, through element stores."""
+    fs, p = small_case(S=3)
+    homs = homographies(fs)
+    want_cost, want_cnt = oracle.calc_cost(p, fs.ref, fs.srcs, homs, "f32")
+    rf, sf = upload_images(pm_lib, fs, p.intensity_scale)
+    V = p.H * p.W * p.D
+    cbuf = torch.full((V + 4,), 7.0, dtype=torch.float32, device="cuda")
+    nbuf = torch.full((V + 4,), 7.0, dtype=torch.float32, device="cuda")
+    cost, cnt = cbuf[offset:offset + V], nbuf[offset:offset + V]
+    assert cost.data_ptr() % 16 and cnt.data_ptr() % 16
+    hf = np.ascontiguousarray(homs, np.float32).reshape(-1)
+    cfg = config(p)
+    # a first pass without counts, then the rest folded into it with counts
+    st = pm_lib.pm_stage_calc_cost(ctypes.byref(cfg), vp(rf), vp(sf), 3, fptr(hf), vp(cost), None, None, None)
+    assert st == 0
+    torch.cuda.synchronize()
+    assert (bits(cost.cpu().numpy()) == bits(want_cost.reshape(-1))).all()
+    cost.fill_(-1.0)
+    cnt.zero_()
+    for a, b in ((0, 2), (2, 3)):
+        st = pm_lib.pm_stage_calc_cost(ctypes.byref(cfg), vp(rf), vp(sf[a]), b - a, fptr(hf[12 * a:]),
+                                       vp(cost), vp(cnt), None, None)
+        assert st == 0
+    torch.cuda.synchronize()
+    assert (bits(cost.cpu().numpy()) == bits(want_cost.reshape(-1))).all()
+    assert (cnt.cpu().numpy() == want_cnt.reshape(-1)).all()
+    # nothing outside the views was written
+    for buf in (cbuf, nbuf):
+        h = buf.cpu().numpy()
+        assert (h[:offset] == 7.0).all() and (h[offset + V:] == 7.0).all()
+
+
 @pytest.mark.parametrize("D,paths,compat,uniq", [(64, 8, 1, 0.95), (64, 4, 1, 0.0), (96, 8, 1, 0.95),
                                                  (96, 4, 0, 0.0), (128, 8, 1, 0.95), (192, 4, 1, 0.0)])
 def test_sgm_and_filter_bit_exact(pm_lib, D, paths, compat, uniq):
