@@ -180,6 +180,24 @@ def cost_kernel_work(e: int, texels: bool = False):
     return FLOP_PER_VOXEL_SOURCE * V * S - tex_flop, tex_flop, e * V + 4 * N + (4 if texels else 16) * N * S
 
 
+# The texture samplers' binding unit: ncu counts at most one texture output wavefront per SM and
+# cycle, and eight per 32-lane bilinear fetch instruction, so an SM filters 4 fetches per clock.
+TEX_FETCHES_PER_SM_CLK = 4
+
+
+def cost_kernel_fetches(reference_mode: bool):
+    """Filtered texture fetches of one cost-kernel launch with a texture sampler.  Algorithmic: one
+    per warped position, plane and source (the row sample the 3x3 window shares) plus, in reference
+    mode, the two corrupted-neighbour samples per voxel and source.  Issued: the tile design's
+    fetch instructions x 32 lanes -- 30x8-pixel tiles of 16 planes, one plane pair per warp, each
+    warp sampling 10 rows for its 8 output rows (+ 2 samples per output row in reference mode)."""
+    V = W * H * D
+    alg = V * S * (3 if reference_mode else 1)
+    tiles = -(-W // 30) * -(-H // 8) * (D // 16)
+    per_warp_source = 10 * 2 + (8 * 2 * 2 if reference_mode else 0)
+    return alg, tiles * 8 * S * per_warp_source * 32
+
+
 def sgm_alg_bytes(e: int):
     """The SGM + winner-take-all + fusion share of B_alg per map: two sweeps over the cost volume
     (2 e V), the forward sweep's path sum written and read back once (8 V), the reference image
@@ -750,6 +768,18 @@ def main():
     cost_tflops = simt_flop / (cost_ms / 1000.0) / 1e12 if cost_ms > 0 else None
     cost_tflops_all = (simt_flop + tex_flop) / (cost_ms / 1000.0) / 1e12 if cost_ms > 0 else None
     cost_gbs = cost_bytes / (cost_ms / 1000.0) / 1e9 if cost_ms > 0 else None
+    tex_roof = None
+    if texels and cost_ms > 0:
+        f_alg, f_issued = cost_kernel_fetches(args.cost_mode != "corrected")
+        peak_tex = 148 * TEX_FETCHES_PER_SM_CLK * sm_mhz * 1e6 / 1e9   # G fetches/s
+        got = f_issued / (cost_ms / 1000.0) / 1e9
+        tex_roof = {"bound": "texture filtering", "achieved": got, "peak": peak_tex, "unit": "G fetches/s",
+                    "frac": got / peak_tex, "fetches_issued_per_launch": f_issued,
+                    "fetches_algorithmic_per_launch": f_alg,
+                    "frac_algorithmic": f_alg / (cost_ms / 1000.0) / 1e9 / peak_tex,
+                    "peak_kind": f"derived: 148 SM x {TEX_FETCHES_PER_SM_CLK} filtered fetches per clock x "
+                                 f"{sm_mhz:.0f} MHz (ncu: one texture output wavefront per SM and cycle at "
+                                 "peak, eight per 32-lane fetch instruction)"}
     sgm_gbs = sgm_bytes / (sgm_ms / 1000.0) / 1e9 if sgm_ms > 0 else None
     sgm_alg_gbs = b_sgm_alg / ((sgm_ms + fuse_ms) / 1000.0) / 1e9 if sgm_ms > 0 else None
     map_s = 1.0 / (value / world)   # seconds per map per GPU
@@ -806,6 +836,8 @@ def main():
                          "algorithmic_bytes_per_launch": cost_bytes,
                          "hbm_achieved_gbs": cost_gbs, "hbm_frac": (cost_gbs / peak_hbm) if cost_gbs else None,
                          "precision": args.precision,
+                         # texture samplers: the texture unit's filtering rate, the kernel's binding roof
+                         "texture": tex_roof,
                          "peak_kind": f"derived FP32 peak: 148 SM x 128 lanes x 2 flop x {sm_mhz:.0f} MHz "
                                       f"({peak_kind} clock); no measured FP32 SIMT peak exists"},
             # the SGM stage against the bytes this implementation moves, and the SGM + winner-take-

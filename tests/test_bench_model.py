@@ -51,3 +51,19 @@ def test_cost_and_sgm_work_at_the_headline_shape(shape):
     # read once by the combine; depth and index written
     assert sgm == 8 * (4 * V + 4 * N) + 4 * (4 * V + 8 * V) + 4 * 4 * V + 8 * N
     assert abs(sgm / V - 96) < 0.5                        # ~96 bytes per voxel for FP32
+
+
+def test_texture_fetch_model(shape):
+    """Fetches of one cost launch with a texture sampler: the tile design issues 52 fetch
+    instructions per warp and source in reference mode (10 row samples + 16 corrupted-neighbour
+    samples per plane pair), 20 with corrected samples; the algorithmic count is 3 (1) per voxel
+    and source.  At 640x480x128x5 that is 21,964,800 warp fetch instructions, the figure the ncu
+    capture of the FP16 texture kernel shows as 8 texture requests each (172.6 M requests; the
+    partly idle last tile column issues a little less)."""
+    shape(640, 480, 128, 5)
+    V = 640 * 480 * 128
+    alg, issued = bench.cost_kernel_fetches(True)
+    assert alg == 3 * V * 5 and issued == 22 * 60 * 8 * 8 * 5 * 52 * 32 == 21_964_800 * 32
+    alg1, issued1 = bench.cost_kernel_fetches(False)
+    assert alg1 == V * 5 and issued1 * 52 == issued * 20
+    assert 8 * issued / 32 >= 172_646_400   # no more requests than instructions allow
