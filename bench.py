@@ -198,6 +198,44 @@ def cost_kernel_fetches(reference_mode: bool):
     return alg, tiles * 8 * S * per_warp_source * 32
 
 
+def cost_roofline(cost_ms, cost_stage_ms, e, texels, reference_mode, sm_mhz, peak_hbm, peak_kind, precision,
+                  traffic):
+    """The cost kernel against its binding roof.  It is not HBM-bound: with exact bilinear the FP32
+    SIMT pipes bind (algorithmic flop on the SIMT pipes against the derived FP32 peak); with a
+    texture sampler the texture unit's filtering rate binds (ncu: the texture pipe near its peak),
+    so `achieved` is the algorithmic fetch count per launch over the kernel's time, against the
+    derived 4 fetches per SM and clock, with the FP32 figures under `fp32_simt`.  cost_ms is the
+    kernel alone (CUDA events on the mapper's stream, the FP16 form's rebase pass excluded)."""
+    simt_flop, tex_flop, cost_bytes = cost_kernel_work(e, texels)
+    peak_fp32 = fp32_peak_tflops(sm_mhz)
+    sec = cost_ms / 1000.0 if cost_ms and cost_ms > 0 else None
+    tflops = simt_flop / sec / 1e12 if sec else None
+    gbs = cost_bytes / sec / 1e9 if sec else None
+    fp32 = {"bound": "fp32", "kernel": "cost_kernel", "achieved": tflops, "peak": peak_fp32, "unit": "TFLOP/s",
+            "frac": tflops / peak_fp32 if tflops else None,
+            "algorithmic_flop_per_launch": simt_flop, "texture_unit_flop_per_launch": tex_flop,
+            "frac_counting_texture_interpolation": (simt_flop + tex_flop) / sec / 1e12 / peak_fp32 if sec else None,
+            "algorithmic_bytes_per_launch": cost_bytes, "hbm_achieved_gbs": gbs,
+            "hbm_frac": gbs / peak_hbm if gbs else None,
+            "peak_kind": f"derived FP32 peak: 148 SM x 128 lanes x 2 flop x {sm_mhz:.0f} MHz ({peak_kind} clock); "
+                         "no measured FP32 SIMT peak exists"}
+    common = {"traffic": traffic, "ms_per_launch": cost_ms, "stage_ms_with_rebase": cost_stage_ms,
+              "precision": precision}
+    if not texels:
+        return {**fp32, **common}
+    f_alg, f_issued = cost_kernel_fetches(reference_mode)
+    peak_tex = 148 * TEX_FETCHES_PER_SM_CLK * sm_mhz * 1e6 / 1e9   # G fetches/s
+    got = f_alg / sec / 1e9 if sec else None
+    return {"bound": "texture", "kernel": "cost_kernel", "achieved": got, "peak": peak_tex, "unit": "G fetches/s",
+            "frac": got / peak_tex if got else None, **common,
+            "fetches_algorithmic_per_launch": f_alg, "fetches_issued_per_launch": f_issued,
+            "frac_issued": f_issued / sec / 1e9 / peak_tex if sec else None,
+            "peak_kind": f"derived: 148 SM x {TEX_FETCHES_PER_SM_CLK} filtered fetches per clock x {sm_mhz:.0f} MHz "
+                         "(ncu: one texture output wavefront per SM and cycle at peak, eight per 32-lane fetch "
+                         "instruction); no measured texture peak exists",
+            "fp32_simt": fp32}
+
+
 def sgm_alg_bytes(e: int):
     """The SGM + winner-take-all + fusion share of B_alg per map: two sweeps over the cost volume
     (2 e V), the forward sweep's path sum written and read back once (8 V), the reference image
@@ -764,22 +802,7 @@ def main():
     cost_stage_ms, sgm_ms, fuse_ms = float(stage_ms[0]), float(stage_ms[1]), float(stage_ms[2])
     cost_ms = float(stage_ms[4]) if stage_ms[4] > 0 else cost_stage_ms   # the cost kernel alone
     texels = sampler_name(args, args.precision) != "exact"
-    simt_flop, tex_flop, cost_bytes = cost_kernel_work(e, texels)
-    cost_tflops = simt_flop / (cost_ms / 1000.0) / 1e12 if cost_ms > 0 else None
-    cost_tflops_all = (simt_flop + tex_flop) / (cost_ms / 1000.0) / 1e12 if cost_ms > 0 else None
-    cost_gbs = cost_bytes / (cost_ms / 1000.0) / 1e9 if cost_ms > 0 else None
-    tex_roof = None
-    if texels and cost_ms > 0:
-        f_alg, f_issued = cost_kernel_fetches(args.cost_mode != "corrected")
-        peak_tex = 148 * TEX_FETCHES_PER_SM_CLK * sm_mhz * 1e6 / 1e9   # G fetches/s
-        got = f_issued / (cost_ms / 1000.0) / 1e9
-        tex_roof = {"bound": "texture filtering", "achieved": got, "peak": peak_tex, "unit": "G fetches/s",
-                    "frac": got / peak_tex, "fetches_issued_per_launch": f_issued,
-                    "fetches_algorithmic_per_launch": f_alg,
-                    "frac_algorithmic": f_alg / (cost_ms / 1000.0) / 1e9 / peak_tex,
-                    "peak_kind": f"derived: 148 SM x {TEX_FETCHES_PER_SM_CLK} filtered fetches per clock x "
-                                 f"{sm_mhz:.0f} MHz (ncu: one texture output wavefront per SM and cycle at "
-                                 "peak, eight per 32-lane fetch instruction)"}
+    simt_flop, tex_flop, _ = cost_kernel_work(e, texels)
     sgm_gbs = sgm_bytes / (sgm_ms / 1000.0) / 1e9 if sgm_ms > 0 else None
     sgm_alg_gbs = b_sgm_alg / ((sgm_ms + fuse_ms) / 1000.0) / 1e9 if sgm_ms > 0 else None
     map_s = 1.0 / (value / world)   # seconds per map per GPU
@@ -820,26 +843,11 @@ def main():
             "plain_fp32": {"value": plain_value, "e2e": plain_e2e, "ms_per_map": t_plain / args.steps,
                            "unit": "depth maps/s"},
             "speedup_vs_plain_fp32": value / plain_value,
-            # the dominant kernel (cost_kernel, more than half of a map) is FP32-ALU-bound, not
-            # HBM-bound; its time is the kernel alone (CUDA events on the mapper's stream, the FP16
-            # form's rebase pass excluded), its flop the algorithmic count on the SIMT pipes
-            "roofline": {"bound": "fp32", "kernel": "cost_kernel",
-                         "achieved": cost_tflops, "peak": peak_fp32,
-                         "unit": "TFLOP/s", "frac": (cost_tflops / peak_fp32) if cost_tflops else None,
-                         "traffic": ncu_traffic("cost_kernel" if e == 4 and args.fp32_sampler == "exact"
-                                                else "cost_kernel_fp16" if e == 2 else None),
-                         "ms_per_launch": cost_ms, "stage_ms_with_rebase": cost_stage_ms,
-                         "algorithmic_flop_per_launch": simt_flop,
-                         "texture_unit_flop_per_launch": tex_flop,
-                         "frac_counting_texture_interpolation": (cost_tflops_all / peak_fp32) if cost_tflops_all
-                         else None,
-                         "algorithmic_bytes_per_launch": cost_bytes,
-                         "hbm_achieved_gbs": cost_gbs, "hbm_frac": (cost_gbs / peak_hbm) if cost_gbs else None,
-                         "precision": args.precision,
-                         # texture samplers: the texture unit's filtering rate, the kernel's binding roof
-                         "texture": tex_roof,
-                         "peak_kind": f"derived FP32 peak: 148 SM x 128 lanes x 2 flop x {sm_mhz:.0f} MHz "
-                                      f"({peak_kind} clock); no measured FP32 SIMT peak exists"},
+            # the dominant kernel (cost_kernel, more than half of a map), against the roof that binds it
+            "roofline": cost_roofline(cost_ms, cost_stage_ms, e, texels, args.cost_mode != "corrected", sm_mhz,
+                                      peak_hbm, peak_kind, args.precision,
+                                      ncu_traffic("cost_kernel" if e == 4 and args.fp32_sampler == "exact"
+                                                  else "cost_kernel_fp16" if e == 2 else None)),
             # the SGM stage against the bytes this implementation moves, and the SGM + winner-take-
             # all + fusion stages against their share of the path-grouped lower bound B_alg
             "roofline_sgm": {"bound": "hbm", "kernel": "sgm_pair_kernel x 4 + combine_kernel (winner-take-all)",

@@ -67,3 +67,20 @@ def test_texture_fetch_model(shape):
     alg1, issued1 = bench.cost_kernel_fetches(False)
     assert alg1 == V * 5 and issued1 * 52 == issued * 20
     assert 8 * issued / 32 >= 172_646_400   # no more requests than instructions allow
+
+
+def test_cost_roofline_binding_roof(shape):
+    """The bench line's `roofline`: the texture unit for a texture sampler (algorithmic fetches over
+    the kernel time against 148 x 4 fetches per clock), the FP32 SIMT pipes for exact bilinear."""
+    shape(640, 480, 128, 5)
+    r = bench.cost_roofline(0.6865, 0.7185, 2, True, True, 1965.0, 6441.6, "measured", "fp16", 55183104)
+    assert r["bound"] == "texture" and r["unit"] == "G fetches/s" and r["traffic"] == 55183104
+    assert abs(r["peak"] - 148 * 4 * 1.965) < 1e-6
+    assert abs(r["frac"] - 589_824_000 / 0.6865e-3 / 1e9 / r["peak"]) < 1e-9 and 0.73 < r["frac"] < 0.74
+    assert 0.87 < r["frac_issued"] < 0.89
+    f = r["fp32_simt"]
+    assert f["bound"] == "fp32" and abs(f["frac"] - 17_694_720_000 / 0.6865e-3 / 1e12 / f["peak"]) < 1e-9
+    r32 = bench.cost_roofline(1.112, 1.114, 4, False, True, 1965.0, 6441.6, "measured", "fp32", 161212928)
+    assert r32["bound"] == "fp32" and "fp32_simt" not in r32 and 0.34 < r32["frac"] < 0.35
+    assert r32["ms_per_launch"] == 1.112 and r32["traffic"] == 161212928
+    assert bench.cost_roofline(0.0, 0.0, 2, True, True, 1965.0, 6441.6, "measured", "fp16", None)["frac"] is None
